@@ -1,0 +1,215 @@
+"""celeris_b200: B200-native Celeris Boussinesq timestep path (host-side Python mirror).
+
+The computation lives in the CUDA/C++ library ``_build/libceleris_b200.so`` behind the C ABI of
+``include/celeris_b200.h``; this module only marshals arguments.  :class:`Engine` mirrors the
+reference's ``ShallowWaterEngine`` (remesh, resetTimestep, timestep, state access) and
+:class:`Batch` advances many domains together.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .abi import (CEL_BC_IRREGULAR, CEL_BC_SINEWAVE, CEL_BC_SOLID, CEL_BC_SPONGE, CEL_BC_UTS,  # noqa: F401
+                  CEL_FORM_FUSED, CEL_FORM_MIXED, CEL_FORM_PLAIN, CelError, Params, Stats, check,
+                  default_params, lib)
+
+FORMS = {"plain": CEL_FORM_PLAIN, "fused": CEL_FORM_FUSED, "mixed": CEL_FORM_MIXED}
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def params_from_cml(path: str) -> Params:
+    p = Params()
+    check(lib().cel_params_from_cml(path.encode(), C.byref(p)))
+    return p
+
+
+def read_cbf(path: str) -> np.ndarray:
+    bnx, bny = C.c_int(), C.c_int()
+    check(lib().cel_read_cbf(path.encode(), None, 0, C.byref(bnx), C.byref(bny)))
+    z = np.zeros((bny.value, bnx.value), dtype=np.float32)
+    check(lib().cel_read_cbf(path.encode(), _fp(z), z.size, C.byref(bnx), C.byref(bny)))
+    return z
+
+
+class Engine:
+    """One domain (``cel_engine``)."""
+
+    def __init__(self, params: Params, z: np.ndarray | None = None, form: str | int = "plain"):
+        self._params = params
+        f = FORMS[form] if isinstance(form, str) else int(form)
+        self.form = f
+        h = C.c_void_p()
+        if z is None:
+            check(lib().cel_create(C.byref(params), None, 0, 0, f, C.byref(h)))
+        else:
+            self._z = np.ascontiguousarray(z, dtype=np.float32)
+            check(lib().cel_create(C.byref(params), _fp(self._z), self._z.shape[1], self._z.shape[0], f, C.byref(h)))
+        self.h = h
+        nx, ny = C.c_int(), C.c_int()
+        check(lib().cel_get_dims(self.h, C.byref(nx), C.byref(ny)))
+        self.nx, self.ny = nx.value, ny.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cel_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return (self.ny + 4, self.nx + 4)
+
+    def remesh(self):
+        check(lib().cel_remesh(self.h))
+
+    def set_stream(self, stream_ptr: int | None):
+        check(lib().cel_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def state(self) -> np.ndarray:
+        out = np.zeros(self.shape + (4,), dtype=np.float32)
+        check(lib().cel_get_state(self.h, _fp(out)))
+        return out
+
+    def set_state(self, rgba: np.ndarray):
+        a = np.ascontiguousarray(rgba, dtype=np.float32)
+        assert a.shape == self.shape + (4,)
+        check(lib().cel_set_state(self.h, _fp(a)))
+
+    def bottom(self) -> np.ndarray:
+        out = np.zeros(self.shape + (3,), dtype=np.float32)
+        check(lib().cel_get_bottom(self.h, _fp(out)))
+        return out
+
+    def aux(self) -> np.ndarray:
+        out = np.zeros(self.shape + (4,), dtype=np.float32)
+        check(lib().cel_get_aux(self.h, _fp(out)))
+        return out
+
+    def reset_timestep(self, realworld_dt: float = 0.0, elapsed: float = 0.0) -> dict:
+        s = Stats()
+        check(lib().cel_reset_timestep(self.h, realworld_dt, elapsed, C.byref(s)))
+        return s.as_dict()
+
+    def timestep(self):
+        check(lib().cel_timestep(self.h))
+
+    def timesteps(self, n: int):
+        check(lib().cel_timesteps(self.h, n))
+
+    def physical_steps(self, n: int):
+        check(lib().cel_physical_steps(self.h, n))
+
+    def stats(self) -> dict:
+        s = Stats()
+        check(lib().cel_get_stats(self.h, C.byref(s)))
+        return s.as_dict()
+
+    def add_solitary_wave(self, H: float, theta_deg: float, xc: float, yc: float):
+        check(lib().cel_add_solitary_wave(self.h, H, theta_deg, xc, yc))
+
+    def synchronize(self):
+        check(lib().cel_synchronize(self.h))
+
+    def kernel_timing(self, enable: bool = True):
+        check(lib().cel_engine_kernel_timing(self.h, int(enable)))
+
+    def kernel_times(self) -> dict:
+        return _kernel_times(self.h, 0)
+
+
+def _kernel_times(handle, is_batch: int) -> dict:
+    cap = 64
+    names = (C.c_char * 64 * cap)()
+    ms = (C.c_double * cap)()
+    n_l = (C.c_longlong * cap)()
+    n = C.c_int()
+    check(lib().cel_kernel_times(handle, is_batch, C.cast(names, C.POINTER(C.c_char * 64)), ms, n_l, cap, C.byref(n)))
+    return {names[i].value.decode(): (ms[i], n_l[i]) for i in range(n.value)}
+
+
+class Batch:
+    """Many domains advanced together (``cel_batch``)."""
+
+    def __init__(self, members, form: str | int = "mixed"):
+        f = FORMS[form] if isinstance(form, str) else int(form)
+        self.form = f
+        self.members = list(members)
+        n = len(self.members)
+        self._params = [m[0] for m in self.members]
+        self._z = [np.ascontiguousarray(m[1], dtype=np.float32) for m in self.members]
+        pp = (C.POINTER(Params) * n)(*[C.pointer(p) for p in self._params])
+        zz = (C.POINTER(C.c_float) * n)(*[_fp(z) for z in self._z])
+        bnx = (C.c_int * n)(*[z.shape[1] for z in self._z])
+        bny = (C.c_int * n)(*[z.shape[0] for z in self._z])
+        h = C.c_void_p()
+        check(lib().cel_batch_create(n, pp, zz, bnx, bny, f, C.byref(h)))
+        self.h = h
+        self.n = n
+        self.shapes = [(p.ny + 4, p.nx + 4) for p in self._params]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().cel_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def cells(self) -> int:
+        return int(lib().cel_batch_cells(self.h))
+
+    def set_stream(self, stream_ptr: int | None):
+        check(lib().cel_batch_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def use_graph(self, enable: bool = True):
+        check(lib().cel_batch_use_graph(self.h, int(enable)))
+
+    def step(self, n: int = 1):
+        check(lib().cel_batch_step(self.h, n))
+
+    def stats(self) -> list:
+        arr = (Stats * self.n)()
+        check(lib().cel_batch_stats(self.h, arr))
+        return [arr[i].as_dict() for i in range(self.n)]
+
+    def state(self, i: int) -> np.ndarray:
+        out = np.zeros(self.shapes[i] + (4,), dtype=np.float32)
+        check(lib().cel_batch_get_state(self.h, i, _fp(out)))
+        return out
+
+    def set_state(self, i: int, rgba: np.ndarray):
+        a = np.ascontiguousarray(rgba, dtype=np.float32)
+        check(lib().cel_batch_set_state(self.h, i, _fp(a)))
+
+    def aux(self, i: int) -> np.ndarray:
+        out = np.zeros(self.shapes[i] + (4,), dtype=np.float32)
+        check(lib().cel_batch_get_aux(self.h, i, _fp(out)))
+        return out
+
+    def kernel_timing(self, enable: bool = True):
+        check(lib().cel_batch_kernel_timing(self.h, int(enable)))
+
+    def kernel_times(self) -> dict:
+        return _kernel_times(self.h, 1)
+
+
+def byte_model(form: str | int, correction_steps: int):
+    f = FORMS[form] if isinstance(form, str) else int(form)
+    a, b = C.c_double(), C.c_double()
+    check(lib().cel_byte_model(f, correction_steps, C.byref(a), C.byref(b)))
+    return a.value, b.value

@@ -1,0 +1,100 @@
+// Device restatements of the per-cell shader helpers of compute.hlsl (lines cited per
+// function).  Operation order follows the shader expressions, so a translation unit compiled
+// with -fmad=false reproduces IEEE single-precision results of the same expressions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "celeris_internal.hpp"
+
+namespace cel {
+
+#define CEL_MIN_DEPTH 0.0001f  // compute.hlsl:1062
+#define CEL_PI_F 3.14159274101257324f  // 4*atan(1.0f) in float (engine.cpp:89)
+
+// MinMod (compute.hlsl:292-296)
+__device__ __forceinline__ float minmod3(float a, float b, float c) {
+    return (a > 0.f && b > 0.f && c > 0.f) ? fminf(fminf(a, b), c)
+         : (a < 0.f && b < 0.f && c < 0.f) ? fmaxf(fmaxf(a, b), c) : 0.f;
+}
+
+// Reconstruct (compute.hlsl:298-315); sd is the breaking-indicator standard deviation.
+__device__ __forceinline__ void reconstruct(float tt, float w, float c, float e, float& ow, float& oe) {
+    const float z1 = tt * (c - w), z2 = e - w, z3 = tt * (e - c);
+    const float g2 = 0.25f * minmod3(z1, z2, z3);
+    oe = c + g2;
+    ow = c - g2;
+}
+__device__ __forceinline__ void reconstruct_sd(float tt, float w, float c, float e, float& ow, float& oe, float& sd) {
+    const float z1 = tt * (c - w), z2 = e - w, z3 = tt * (e - c);
+    const float g2 = 0.25f * minmod3(z1, z2, z3);
+    const float mu = 0.5f * (z1 + z2 + z3) / 3.0f;
+    sd = sqrtf(((z1 - mu) * (z1 - mu) + (z2 - mu) * (z2 - mu) + (z3 - mu) * (z3 - mu)) / 3.0f);
+    oe = c + g2;
+    ow = c - g2;
+}
+
+// CorrectW (compute.hlsl:317-328)
+__device__ __forceinline__ void correct_w(float Bw, float Be, float wbar, float& ww, float& we) {
+    if (we < Be) { we = Be; ww = fmaxf(Bw, 2.f * wbar - Be); }
+    else if (ww < Bw) { we = fmaxf(Be, 2.f * wbar - Bw); ww = Bw; }
+}
+
+// divide_by_h of CalcUV / CalcUV_Scalar (compute.hlsl:330-352)
+__device__ __forceinline__ float div_by_h(float h, float eps) {
+    const float h2 = h * h, h4 = h2 * h2;
+    return 1.41421354f * h / sqrtf(h4 + fmaxf(h4, eps));
+}
+
+// NumericalFlux (compute.hlsl:363-370)
+__device__ __forceinline__ float numflux(float ap, float am, float Fp, float Fm, float dU) {
+    if (ap - am != 0.f) return (ap * Fm - am * Fp + ap * am * dU) / (ap - am);
+    return 0.f;
+}
+
+// FrictionCalc (compute.hlsl:544-553)
+__device__ __forceinline__ float friction_calc(float hu, float hv, float h, float friction, int manning, float g,
+                                               float eps) {
+    float f = friction;
+    const float h4 = powf(h, 4.0f);
+    const float dbh = 1.41421354f * h / sqrtf(h4 + fmaxf(h4, eps));
+    if (manning == 1) f = g * friction * friction * powf(fabsf(dbh), 0.3333f);
+    return f * sqrtf(hu * hu + hv * hv) * dbh * dbh;
+}
+
+// SpongeFunction (compute.hlsl:1056-1059)
+__device__ __forceinline__ float sponge_fn(float L, float x) {
+    return 0.5f + 0.5f * cosf(CEL_PI_F * fmaxf(L - x, 0.f) / L);
+}
+
+// sineWave with Eckart's wavenumber (compute.hlsl:1080-1101); t is float as in the reference.
+__device__ __forceinline__ void sine_wave(float x, float y, float t, float d, float amp, float period,
+                                          float th, float phase, float g, float& e, float& hu, float& hv) {
+    const float omega = 2.f * CEL_PI_F / period;
+    const float k = omega * omega / (g * sqrtf(tanhf(omega * omega * d / g)));
+    const float c = omega / k;
+    const float kx = cosf(th) * x * k;
+    const float ky = sinf(th) * y * k;
+    e = amp * sinf(omega * t - kx - ky + phase);
+    hu = c * cosf(th) * e;
+    hv = c * sinf(th) * e;
+}
+
+// The same with the phase omega*t evaluated in FP64 and reduced modulo 2*pi before the FP32
+// sine (the mixed form's wave-maker phase).
+__device__ __forceinline__ void sine_wave_t64(float x, float y, double t, float d, float amp, float period,
+                                              float th, float phase, float g, float& e, float& hu, float& hv) {
+    const double omega_d = 2.0 * 3.14159265358979323846 / double(period);
+    const float omega = float(omega_d);
+    const float k = omega * omega / (g * sqrtf(tanhf(omega * omega * d / g)));
+    const float c = omega / k;
+    const float kx = cosf(th) * x * k;
+    const float ky = sinf(th) * y * k;
+    double ph = omega_d * t;
+    ph -= 6.283185307179586476925 * floor(ph / 6.283185307179586476925);
+    e = amp * sinf(float(ph) - kx - ky + phase);
+    hu = c * cosf(th) * e;
+    hv = c * sinf(th) * e;
+}
+
+}  // namespace cel

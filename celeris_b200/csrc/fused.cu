@@ -1,0 +1,1453 @@
+// Fused, batched B200 form of the Celeris timestep path.
+//
+// One pass (predictor, corrector or Euler) of every domain in a batch is three kernels plus the
+// boundary kernels, each launched once for all domains over a cross-domain work list:
+//   k_stencil  : Pass1 (minmod reconstruction, positivity fix, desingularised velocities) +
+//                Pass2 (Kurganov-Petrova central-upwind fluxes) + Pass3Predictor (flux
+//                divergence, bed slope, friction, Madsen-Sorensen dispersion, F*/G*, AB3/AM4
+//                combination) + white-water/inundation aux + the GetStats reduction, over a
+//                32x16 tile staged in shared memory with a 2-cell halo.  It writes the new w
+//                and, for hu and hv, the right-hand side of the implicit dispersive system in
+//                increment form: M dhu = r, hu_new = hu_base + dhu.
+//   k_rows / k_cols : the tridiagonal solves along x (one CTA per row) and y (one CTA per band
+//                of 16 columns), a chunked Thomas elimination whose forward and backward sweeps
+//                are first-order linear recurrences combined across chunks by a scan; the
+//                time-invariant LU factors are precomputed per domain.
+//   k_boundary : East, North, West, South strips in the reference's order (one launch each).
+// The whole physical step (predictor + correctors) is captured once per buffer-rotation phase
+// into CUDA graphs and replayed.
+//
+// CEL_FORM_MIXED additionally keeps a compensation (low) word for w, hu and hv and adds every
+// increment with a two-sum, evaluates the wave-maker phase omega*t in FP64 from an FP64 clock,
+// and reduces mass/energy in FP64.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "batch.hpp"
+#include "device_math.cuh"
+#include "engine_iface.hpp"
+#include "scheme.hpp"
+
+namespace cel {
+
+namespace {
+
+constexpr int TX = 32, TY = 16;
+constexpr int SW = TX + 4, SH = TY + 4;      // state tile with a 2-cell halo
+constexpr int FW = TX + 2, FH = TY + 2;      // face tile (1-cell halo)
+constexpr int NT1 = TX * TY;                 // stencil threads (one output cell each)
+constexpr int NTR = 256;                     // row-solver threads
+constexpr int NTC = 512;                     // column solver threads: CWT columns x (512/CWT) chunks
+constexpr int STATS_N = 12;
+
+// stats accumulator layout
+// [0] sum h  [1] sum h(B+h/2)  [2] sum hu  [3] sum hv  [4] sum (hu u + hv v)  [5] sum h (every cell)
+// [6] max u^2+v^2  [7] max h  [8] max cfl rate  [9] max (u^2+v^2)/h  [10] health flag
+struct MemberDev {
+    SimConsts c;
+    int P;                  // plane pitch in floats
+    float dt;
+    float* S[3][3];         // state buffers [buffer][w, hu, hv]
+    float* L[3][3];         // compensation words (mixed form)
+    const float* BY;
+    const float* BX;
+    const float* BA;
+    float* R[2];            // increment right-hand sides for hu, hv
+    float* G[4][3];         // dU/dt history buffers
+    float* F[4][2];         // F*, G* history buffers
+    float* AUX[2];          // max inundated depth, breaking indicator
+    const float* FX[3];     // x-systems: c', inv_den, m
+    const float* FYF[3];    // y-systems: c', inv_den, m
+    BoundaryDesc bd[4];     // N, E, S, W
+    const float4* waves;
+    const float* uts[4];    // (t, eta, hu, hv) tables, float
+    int nuts[4];
+    float* strip;
+    double* stats;
+    double* stats_now;
+    double* time64;
+    float* time32;
+};
+
+struct PassArgs {
+    int in, out, cur;
+    int og, oog, scr, pred;
+    int scheme;
+};
+
+__device__ __forceinline__ void two_sum_add(float& hi, float& lo, float d) {
+    // (hi + lo) + d with the rounding error of hi + d carried in lo (Knuth two-sum)
+    const float s = hi + d;
+    const float bp = s - hi;
+    const float err = (hi - (s - bp)) + (d - bp);
+    const float lo2 = lo + err;
+    const float h2 = s + lo2;
+    lo = lo2 - (h2 - s);
+    hi = h2;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+// Block reduction of the GetStats quantities of one cell per thread into the member's
+// accumulators (FP64 sums, maxima via the ordering of non-negative doubles).
+__device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h, float B, float hu, float hv,
+                             float u, float v, float q, float cc, float odx, float ody, bool bad,
+                             double (*red)[STATS_N]) {
+    double s[STATS_N];
+    for (int k = 0; k < STATS_N; ++k) s[k] = 0.0;
+    if (cnt_block) {
+        s[0] = h; s[1] = double(h * (B + 0.5f * h)); s[2] = hu; s[3] = hv; s[4] = double(hu * u + hv * v);
+        const float u2v2 = u * u + v * v;
+        s[6] = u2v2; s[7] = h;
+        s[8] = fmaxf((fabsf(u) + cc) * odx, (fabsf(v) + cc) * ody);
+        s[9] = u2v2 * q;
+    }
+    if (cnt_all) s[5] = h;
+    s[10] = bad ? 1.0 : 0.0;
+    for (int off = 16; off; off >>= 1)
+        for (int k = 0; k < 11; ++k) {
+            const double o = __shfl_down_sync(0xffffffffu, s[k], off);
+            s[k] = (k >= 6) ? fmax(s[k], o) : s[k] + o;
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < 11; ++k) red[wid][k] = s[k];
+    __syncthreads();
+    if (threadIdx.x < 11) {
+        const int k = threadIdx.x;
+        const int nw = blockDim.x >> 5;
+        double a = red[0][k];
+        for (int w = 1; w < nw; ++w) a = (k >= 6) ? fmax(a, red[w][k]) : a + red[w][k];
+        if (k < 6) { if (a != 0.0) atomicAdd(acc + k, a); }
+        else atomic_max_nonneg(acc + k, a);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_stencil: Pass1 + Pass2 + Pass3 + aux + stats for one 32x16 tile per iteration.
+// ---------------------------------------------------------------------------------------------
+template <bool MIXED>
+__global__ void __launch_bounds__(NT1) k_stencil(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
+                                                 int ntiles, PassArgs pa) {
+    extern __shared__ float smem[];
+    float* sW = smem;
+    float* sHU = sW + SH * SW;
+    float* sHV = sHU + SH * SW;
+    float* sBA = sHV + SH * SW;
+    float* sBX = sBA + SH * SW;
+    float* sBY = sBX + SH * SW;
+    float* fh = sBY + SH * SW;        // [4][FH*FW]  N, E, S, W
+    float* fu = fh + 4 * FH * FW;
+    float* fv = fu + 4 * FH * FW;
+    float* xf = fv + 4 * FH * FW;     // [3][TY*(TX+1)]
+    float* yf = xf + 3 * TY * (TX + 1); // [3][(TY+1)*TX]
+    __shared__ double red[NT1 / 32][STATS_N];
+    const int tid = threadIdx.x;
+    constexpr int FA = FH * FW;
+
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        const MemberDev& M = mems[tl.x];
+        const SimConsts c = M.c;
+        const int P = M.P, NX = c.NX, NY = c.NY, nx = c.nx, ny = c.ny;
+        const int x0 = tl.y, y0 = tl.z;
+        const float* Win = M.S[pa.in][0];
+        const float* HUin = M.S[pa.in][1];
+        const float* HVin = M.S[pa.in][2];
+        __syncthreads();  // smem reuse across tiles
+        // ---- load the state / bottom tile (2-cell halo; outside the texture reads zero) ----
+        for (int k = tid; k < SH * SW; k += NT1) {
+            const int ly = k / SW, lx = k - ly * SW;
+            const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
+            const bool ok = gx >= 0 && gx < NX && gy >= 0 && gy < NY;
+            const size_t gi = size_t(gy) * P + gx;
+            sW[k] = ok ? Win[gi] : 0.f;
+            sHU[k] = ok ? HUin[gi] : 0.f;
+            sHV[k] = ok ? HVin[gi] : 0.f;
+            sBA[k] = ok ? M.BA[gi] : 0.f;
+            sBX[k] = ok ? M.BX[gi] : 0.f;
+            sBY[k] = ok ? M.BY[gi] : 0.f;
+        }
+        __syncthreads();
+        // ---- Pass1: faces over [x0-1, x0+TX+1) x [y0-1, y0+TY+1), with the aux update ----
+        const float decay = powf(fabsf(c.whitewater_decay_rate), M.dt);
+        for (int k = tid; k < FA; k += NT1) {
+            const int fy = k / FW, fx = k - fy * FW;
+            const int si = (fy + 1) * SW + (fx + 1);
+            const float wc = sW[si], wl = sW[si - 1], wr = sW[si + 1], wd = sW[si - SW], wu = sW[si + SW];
+            const float BN = sBY[si], BE = sBX[si], BS = sBY[si - SW], BW = sBX[si - 1];
+            float wN, wE, wS, wW, huN, huE, huS, huW, hvN, hvE, hvS, hvW, sd1, sd2;
+            reconstruct_sd(c.two_theta, wl, wc, wr, wW, wE, sd1);
+            reconstruct_sd(c.two_theta, wd, wc, wu, wS, wN, sd2);
+            reconstruct(c.two_theta, sHU[si - 1], sHU[si], sHU[si + 1], huW, huE);
+            reconstruct(c.two_theta, sHU[si - SW], sHU[si], sHU[si + SW], huS, huN);
+            reconstruct(c.two_theta, sHV[si - 1], sHV[si], sHV[si + 1], hvW, hvE);
+            reconstruct(c.two_theta, sHV[si - SW], sHV[si], sHV[si + SW], hvS, hvN);
+            correct_w(BW, BE, wc, wW, wE);
+            correct_w(BS, BN, wc, wS, wN);
+            const float hN = wN - BN, hE = wE - BE, hS = wS - BS, hW = wW - BW;
+            float q;
+            q = div_by_h(hN, c.epsilon); fh[0 * FA + k] = hN; fu[0 * FA + k] = q * huN; fv[0 * FA + k] = q * hvN;
+            q = div_by_h(hE, c.epsilon); fh[1 * FA + k] = hE; fu[1 * FA + k] = q * huE; fv[1 * FA + k] = q * hvE;
+            q = div_by_h(hS, c.epsilon); fh[2 * FA + k] = hS; fu[2 * FA + k] = q * huS; fv[2 * FA + k] = q * hvS;
+            q = div_by_h(hW, c.epsilon); fh[3 * FA + k] = hW; fu[3 * FA + k] = q * huW; fv[3 * FA + k] = q * hvW;
+            // aux (Pass1 then Pass2 of txAuxiliary) for cells in [1,nx+2)x[1,ny+2) owned by this tile
+            const int gx = x0 - 1 + fx, gy = y0 - 1 + fy;
+            if (gx >= 1 && gx < nx + 2 && gy >= 1 && gy < ny + 2) {
+                const int cx = gx < 2 ? 2 : gx, cy = gy < 2 ? 2 : gy;
+                if (cx >= x0 && cx < x0 + TX && cy >= y0 && cy < y0 + TY) {
+                    const size_t gi = size_t(gy) * P + gx;
+                    const float msd = atanf(fmaxf(sd1 * c.one_over_dx, sd2 * c.one_over_dy));
+                    const float md = fmaxf((hN + hE + hS + hW) / 4.0f, M.AUX[0][gi]);
+                    float bw = M.AUX[1][gi];
+                    if (msd > c.dissipation_threshold) bw = 1.0f;
+                    M.AUX[0][gi] = md;
+                    M.AUX[1][gi] = bw * decay;
+                }
+            }
+        }
+        __syncthreads();
+        // ---- Pass2: x fluxes at [x0-1, x0+TX) x [y0, y0+TY), y fluxes at [x0, x0+TX) x [y0-1, y0+TY) ----
+        {
+            const float g = c.g, hg = c.half_g;
+            constexpr int NXF = TY * (TX + 1), NYF = (TY + 1) * TX;
+            for (int k = tid; k < NXF + NYF; k += NT1) {
+                if (k < NXF) {
+                    const int ly = k / (TX + 1), lxx = k - ly * (TX + 1);
+                    const int fl = (ly + 1) * FW + lxx;   // face cell west of the face
+                    const float hE = fh[1 * FA + fl], uE = fu[1 * FA + fl], vE = fv[1 * FA + fl];
+                    const float hWe = fh[3 * FA + fl + 1], uWe = fu[3 * FA + fl + 1], vWe = fv[3 * FA + fl + 1];
+                    const float cE = sqrtf(g * hE), cW = sqrtf(g * hWe);
+                    const float ap = fmaxf(fmaxf(uE + cE, uWe + cW), 0.f);
+                    const float am = fminf(fminf(uE - cE, uWe - cW), 0.f);
+                    xf[0 * NXF + k] = numflux(ap, am, hWe * uWe, hE * uE, hWe - hE);
+                    xf[1 * NXF + k] = numflux(ap, am, hWe * (uWe * uWe + hg * hWe), hE * (uE * uE + hg * hE),
+                                              hWe * uWe - hE * uE);
+                    xf[2 * NXF + k] = numflux(ap, am, hWe * uWe * vWe, hE * uE * vE, hWe * vWe - hE * vE);
+                } else {
+                    const int kk = k - NXF;
+                    const int ly = kk / TX, lx = kk - ly * TX;
+                    const int fl = ly * FW + lx + 1;      // face cell south of the face
+                    const float hN = fh[0 * FA + fl], uN = fu[0 * FA + fl], vN = fv[0 * FA + fl];
+                    const float hSn = fh[2 * FA + fl + FW], uSn = fu[2 * FA + fl + FW], vSn = fv[2 * FA + fl + FW];
+                    const float cN = sqrtf(g * hN), cS = sqrtf(g * hSn);
+                    const float bp = fmaxf(fmaxf(vN + cN, vSn + cS), 0.f);
+                    const float bm = fminf(fminf(vN - cN, vSn - cS), 0.f);
+                    yf[0 * NYF + kk] = numflux(bp, bm, hSn * vSn, hN * vN, hSn - hN);
+                    yf[1 * NYF + kk] = numflux(bp, bm, hSn * uSn * vSn, hN * uN * vN, hSn * uSn - hN * uN);
+                    yf[2 * NYF + kk] = numflux(bp, bm, hSn * (vSn * vSn + hg * hSn), hN * (vN * vN + hg * hN),
+                                               hSn * vSn - hN * vN);
+                }
+            }
+        }
+        __syncthreads();
+        // ---- zero the ghost ring of the output state (engine.cpp:1007) ----
+        for (int k = tid; k < SH * SW; k += NT1) {
+            const int ly = k / SW, lx = k - ly * SW;
+            const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
+            if (gx < 0 || gx >= NX || gy < 0 || gy >= NY) continue;
+            if (gx >= 2 && gx < nx + 2 && gy >= 2 && gy < ny + 2) continue;
+            const int cx = min(max(gx, 2), nx + 1), cy = min(max(gy, 2), ny + 1);
+            if (cx < x0 || cx >= x0 + TX || cy < y0 || cy >= y0 + TY) continue;
+            const size_t gi = size_t(gy) * P + gx;
+            M.S[pa.out][0][gi] = 0.f; M.S[pa.out][1][gi] = 0.f; M.S[pa.out][2][gi] = 0.f;
+            if (MIXED) { M.L[pa.out][0][gi] = 0.f; M.L[pa.out][1][gi] = 0.f; M.L[pa.out][2][gi] = 0.f; }
+        }
+        // ---- Pass3: one interior cell per thread ----
+        const int lx = tid % TX, ly = tid / TX;
+        const int gx = x0 + lx, gy = y0 + ly;
+        const bool valid = gx < nx + 2 && gy < ny + 2;
+        const int si = (ly + 2) * SW + (lx + 2);
+        const size_t gi = size_t(gy) * P + gx;
+        float sh_h = 0.f, sh_B = 0.f, sh_hu = 0.f, sh_hv = 0.f, sh_u = 0.f, sh_v = 0.f, sh_q = 0.f, sh_c = 0.f;
+        bool bad = false;
+        if (valid) {
+            constexpr int NXF = TY * (TX + 1), NYF = (TY + 1) * TX;
+            const float sl = c.sea_level;
+            const float wc = sW[si], huc = sHU[si], hvc = sHV[si];
+            const float BAh = sBA[si], BXh = sBX[si], BYh = sBY[si];
+            const float BXw = sBX[si - 1], BYs = sBY[si - SW];
+            const float h = fmaxf(0.f, wc - BAh);
+            const float dh = fmaxf(0.f, sl - BAh), d2 = dh * dh, d3 = d2 * dh;
+            const float dl = fmaxf(0.f, sl - sBA[si - 1]), dr = fmaxf(0.f, sl - sBA[si + 1]);
+            const float ddn = fmaxf(0.f, sl - sBA[si - SW]), du = fmaxf(0.f, sl - sBA[si + SW]);
+            const float dll = fmaxf(0.f, sl - sBA[si - 2]), drr = fmaxf(0.f, sl - sBA[si + 2]);
+            const float ddd = fmaxf(0.f, sl - sBA[si - 2 * SW]), duu = fmaxf(0.f, sl - sBA[si + 2 * SW]);
+            const float e0 = wc - sl;
+            const float el = sW[si - 1] - sl, er = sW[si + 1] - sl, ed = sW[si - SW] - sl, eu = sW[si + SW] - sl;
+            const float ell = sW[si - 2] - sl, err = sW[si + 2] - sl, edd = sW[si - 2 * SW] - sl, euu = sW[si + 2 * SW] - sl;
+            const float eul = sW[si + SW - 1] - sl, eur = sW[si + SW + 1] - sl;
+            const float edl = sW[si - SW - 1] - sl, edr = sW[si - SW + 1] - sl;
+            const int xk = ly * (TX + 1) + lx;
+            const int yk = ly * TX + lx;
+            const float odx = c.one_over_dx, ody = c.one_over_dy;
+            const float od2x = odx * odx, od3x = od2x * odx, od2y = ody * ody, od3y = od2y * ody;
+            const float ddx = (-drr + 8 * dr - 8 * dl + dll) * odx / 12.0f;
+            const float ddy = (-duu + 8 * du - 8 * ddn + ddd) * ody / 12.0f;
+            const float exy = (0.25f * odx * ody * (eur - edr - eul + edl));
+            const float exx = od2x * (er - 2 * e0 + el);
+            const float eyy = od2y * (eu - 2 * e0 + ed);
+            const float Bg = c.Bcoef_g;
+            const float P1x = Bg * (d3) * ((err - 2 * er + 2 * el - ell) * (0.5f * od3x) +
+                                           (eur - eul - 2 * er + 2 * el + edr - edl) * (0.5f * odx * od2y));
+            const float P2x = Bg * (d2) * (ddx * (2 * exx + eyy) + ddy * exy);
+            const float P1y = Bg * (d3) * ((euu - 2 * eu + 2 * ed - edd) * (0.5f * od3y) +
+                                           (eur + eul - 2 * eu + 2 * ed - edr - edl) * (0.5f * ody * od2x));
+            const float P2y = Bg * (d2) * (ddy * (exx + 2 * eyy) + ddx * exy);
+            const float fr = friction_calc(huc, hvc, h, c.friction, c.is_manning, c.g, c.epsilon);
+            const float s1 = -c.g_over_dx * h * (BXh - BXw) - huc * fr + (P1x + P2x);
+            const float s2 = -c.g_over_dy * h * (BYh - BYs) - hvc * fr + (P1y + P2y);
+            const float f0 = (xf[0 * NXF + xk] - xf[0 * NXF + xk + 1]) * odx + (yf[0 * NYF + yk] - yf[0 * NYF + yk + TX]) * ody;
+            const float f1 = (xf[1 * NXF + xk] - xf[1 * NXF + xk + 1]) * odx + (yf[1 * NYF + yk] - yf[1 * NYF + yk + TX]) * ody + s1;
+            const float f2 = (xf[2 * NXF + xk] - xf[2 * NXF + xk + 1]) * odx + (yf[2 * NYF + yk] - yf[2 * NYF + yk + TX]) * ody + s2;
+            const float sixth = 1.0f / 6.0f;
+            const float Fs = (sixth * dh * (ddx * ((ody / 2.0f) * (sHV[si + SW] - sHV[si - SW])) +
+                                            (ddy * ((odx / 2.0f) * (sHV[si + 1] - sHV[si - 1])))));
+            const float Gs = (sixth * dh * (ddx * ((ody / 2.0f) * (sHU[si + SW] - sHU[si - SW])) +
+                                            (ddy * ((odx / 2.0f) * (sHU[si + 1] - sHU[si - 1])))));
+            const float dt = M.dt;
+            float dw, rhu, rhv;
+            float wbase = wc, wbase_lo = 0.f;
+            if (pa.scheme == CEL_SCHEME_EULER) {
+                dw = dt * f0;
+                rhu = dt * f1;
+                rhv = dt * f2;
+            } else {
+                const float o0 = M.G[pa.og][0][gi], o1 = M.G[pa.og][1][gi], o2 = M.G[pa.og][2][gi];
+                const float q0 = M.G[pa.oog][0][gi], q1 = M.G[pa.oog][1][gi], q2 = M.G[pa.oog][2][gi];
+                const float fo0 = M.F[pa.og][0][gi], fo1 = M.F[pa.og][1][gi];
+                const float foo0 = M.F[pa.oog][0][gi], foo1 = M.F[pa.oog][1][gi];
+                if (pa.scheme == CEL_SCHEME_PREDICTOR) {
+                    dw = dt / 12.0f * (23.0f * f0 - 16.0f * o0 + 5.0f * q0);
+                    rhu = dt / 12.0f * (23.0f * f1 - 16.0f * o1 + 5.0f * q1) + (2.0f * Fs - 3.0f * fo0 + foo0);
+                    rhv = dt / 12.0f * (23.0f * f2 - 16.0f * o2 + 5.0f * q2) + (2.0f * Gs - 3.0f * fo1 + foo1);
+                } else {  // corrector, from CURRENT_STATE
+                    const float p0 = M.G[pa.pred][0][gi], p1 = M.G[pa.pred][1][gi], p2 = M.G[pa.pred][2][gi];
+                    const float fp0 = M.F[pa.pred][0][gi], fp1 = M.F[pa.pred][1][gi];
+                    dw = dt / 24.0f * (9 * f0 + 19 * p0 - 5 * o0 + 1 * q0);
+                    rhu = dt / 24.0f * (9 * f1 + 19 * p1 - 5 * o1 + 1 * q1) + Fs - fp0;
+                    rhv = dt / 24.0f * (9 * f2 + 19 * p2 - 5 * o2 + 1 * q2) + Gs - fp1;
+                    wbase = M.S[pa.cur][0][gi];
+                    if (MIXED) wbase_lo = M.L[pa.cur][0][gi];
+                }
+            }
+            if (MIXED && pa.scheme != CEL_SCHEME_CORRECTOR) wbase_lo = M.L[pa.in][0][gi];
+            float wn = wbase, wl = wbase_lo;
+            if (MIXED) two_sum_add(wn, wl, dw);
+            else wn = wbase + dw;
+            M.S[pa.out][0][gi] = wn;
+            if (MIXED) M.L[pa.out][0][gi] = wl;
+            M.R[0][gi] = rhu;
+            M.R[1][gi] = rhv;
+            M.G[pa.scr][0][gi] = f0; M.G[pa.scr][1][gi] = f1; M.G[pa.scr][2][gi] = f2;
+            M.F[pa.scr][0][gi] = Fs; M.F[pa.scr][1][gi] = Gs;
+            // GetStats quantities of the input state (compute.hlsl:1319-1378)
+            sh_h = h; sh_B = BAh; sh_hu = huc; sh_hv = hvc;
+            sh_q = div_by_h(h, c.epsilon);
+            sh_u = sh_q * huc; sh_v = sh_q * hvc;
+            sh_c = sqrtf(c.g * h);
+            bad = !isfinite(wc) || !isfinite(huc) || !isfinite(hvc);
+        }
+        const bool in_block = valid && gx < 2 + 4 * (nx / 4) && gy < 2 + 4 * (ny / 4);
+        stats_reduce(M.stats, in_block, valid, sh_h, sh_B, sh_hu, sh_hv, sh_u, sh_v, sh_q, sh_c, c.one_over_dx,
+                     c.one_over_dy, bad, red);
+    }
+}
+
+// Stats of the current state only (resetTimestep on demand).
+__global__ void __launch_bounds__(256) k_stats_only(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
+                                                    int ntiles, int buf) {
+    __shared__ double red[256 / 32][STATS_N];
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        const MemberDev& M = mems[tl.x];
+        const SimConsts c = M.c;
+        for (int sub = 0; sub < (TX * TY) / 256; ++sub) {
+            const int k = sub * 256 + threadIdx.x;
+            const int gx = tl.y + k % TX, gy = tl.z + k / TX;
+            const bool valid = gx < c.nx + 2 && gy < c.ny + 2;
+            float h = 0, B = 0, hu = 0, hv = 0, u = 0, v = 0, q = 0, cc = 0;
+            bool bad = false;
+            if (valid) {
+                const size_t gi = size_t(gy) * M.P + gx;
+                const float w = M.S[buf][0][gi];
+                hu = M.S[buf][1][gi]; hv = M.S[buf][2][gi]; B = M.BA[gi];
+                h = fmaxf(0.f, w - B);
+                q = div_by_h(h, c.epsilon);
+                u = q * hu; v = q * hv;
+                cc = sqrtf(c.g * h);
+                bad = !isfinite(w) || !isfinite(hu) || !isfinite(hv);
+            }
+            const bool in_block = valid && gx < 2 + 4 * (c.nx / 4) && gy < 2 + 4 * (c.ny / 4);
+            stats_reduce(M.stats_now, in_block, valid, h, B, hu, hv, u, v, q, cc, c.one_over_dx, c.one_over_dy, bad, red);
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Tridiagonal solves.  For one system with Thomas factors (c', inv, m):
+//   forward   d'_i = inv_i r_i + m_i d'_{i-1}
+//   backward  x_i  = d'_i - c'_i x_{i+1}
+// Each thread runs both recurrences over a contiguous chunk with zero carry-in; the chunk
+// transfer maps (product of multipliers, local end value) are combined by a scan and the
+// chunk values are corrected with the running products.
+// ---------------------------------------------------------------------------------------------
+struct Affine { float a, b; };  // x -> b + a x
+
+__device__ __forceinline__ Affine compose(const Affine& later, const Affine& earlier) {
+    return Affine{later.a * earlier.a, later.b + later.a * earlier.b};
+}
+
+// Exclusive scan of affine maps over the threads of a block in thread order; returns the carry
+// (the composition of all earlier maps applied to 0).
+template <int NT>
+__device__ float block_exclusive_carry(Affine mine, Affine* sw) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    Affine inc = mine;
+    for (int off = 1; off < 32; off <<= 1) {
+        Affine o;
+        o.a = __shfl_up_sync(0xffffffffu, inc.a, off);
+        o.b = __shfl_up_sync(0xffffffffu, inc.b, off);
+        if (lane >= off) inc = compose(inc, o);
+    }
+    if (lane == 31) sw[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        Affine v = lane < NT / 32 ? sw[lane] : Affine{1.f, 0.f};
+        for (int off = 1; off < 32; off <<= 1) {
+            Affine o;
+            o.a = __shfl_up_sync(0xffffffffu, v.a, off);
+            o.b = __shfl_up_sync(0xffffffffu, v.b, off);
+            if (lane >= off) v = compose(v, o);
+        }
+        if (lane < NT / 32) sw[32 + lane] = v;  // inclusive totals of warps
+    }
+    __syncthreads();
+    Affine before = wid > 0 ? sw[32 + wid - 1] : Affine{1.f, 0.f};
+    Affine exl;
+    {
+        Affine o;
+        o.a = __shfl_up_sync(0xffffffffu, inc.a, 1);
+        o.b = __shfl_up_sync(0xffffffffu, inc.b, 1);
+        exl = lane > 0 ? o : Affine{1.f, 0.f};
+    }
+    const Affine tot = compose(exl, before);
+    __syncthreads();
+    return tot.b;
+}
+
+__host__ __device__ __forceinline__ int pidx(int i) { return i + (i >> 5); }
+
+template <bool MIXED>
+__global__ void __launch_bounds__(NTR) k_rows(const MemberDev* __restrict__ mems, const int2* __restrict__ rows,
+                                              int nrows, PassArgs pa) {
+    extern __shared__ float rs[];
+    __shared__ Affine sw[64];
+    for (int it = blockIdx.x; it < nrows; it += gridDim.x) {
+        const int2 rw = rows[it];
+        const MemberDev& M = mems[rw.x];
+        const int n = M.c.nx, P = M.P, y = rw.y;
+        const size_t row = size_t(y) * P + 2;
+        const float* r = M.R[0] + row;
+        const float* cp = M.FX[0] + row;
+        const float* inv = M.FX[1] + row;
+        const float* mm = M.FX[2] + row;
+        float* sy = rs;
+        float* sm = rs + pidx(n) + 1;
+        float* sc = sm + pidx(n) + 1;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += NTR) {
+            sy[pidx(i)] = inv[i] * r[i];
+            sm[pidx(i)] = mm[i];
+            sc[pidx(i)] = cp[i];
+        }
+        __syncthreads();
+        const int mc = (n + NTR - 1) / NTR;
+        const int i0 = min(n, int(threadIdx.x) * mc), i1 = min(n, i0 + mc);
+        float yv = 0.f, pa_ = 1.f;
+        for (int i = i0; i < i1; ++i) {
+            const float m = sm[pidx(i)];
+            yv = sy[pidx(i)] + m * yv;
+            pa_ *= m;
+            sy[pidx(i)] = yv;
+        }
+        const float carry = block_exclusive_carry<NTR>(Affine{pa_, yv}, sw);
+        float pref = 1.f;
+        for (int i = i0; i < i1; ++i) {
+            pref *= sm[pidx(i)];
+            sy[pidx(i)] += pref * carry;
+        }
+        // backward: chunks in reverse order; thread j handles chunk NTR-1-j of the scan
+        float z = 0.f, qa = 1.f;
+        for (int i = i1 - 1; i >= i0; --i) {
+            const float cv = sc[pidx(i)];
+            z = sy[pidx(i)] - cv * z;
+            qa *= -cv;
+            sy[pidx(i)] = z;
+        }
+        // reverse scan: reuse the forward scan on reversed thread order via shared memory
+        __shared__ Affine rev[NTR];
+        rev[threadIdx.x] = Affine{qa, z};
+        __syncthreads();
+        const Affine mine = rev[NTR - 1 - threadIdx.x];
+        __syncthreads();
+        const float carry_r = block_exclusive_carry<NTR>(mine, sw);
+        __shared__ float carries[NTR];
+        carries[NTR - 1 - threadIdx.x] = carry_r;
+        __syncthreads();
+        const float cnext = carries[threadIdx.x];
+        float suf = 1.f;
+        const int out = pa.out, base = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
+        float* ohi = M.S[out][1] + row;
+        const float* bhi = M.S[base][1] + row;
+        for (int i = i1 - 1; i >= i0; --i) {
+            suf *= -sc[pidx(i)];
+            const float x = sy[pidx(i)] + suf * cnext;
+            if (MIXED) {
+                float hi = bhi[i], lo = (M.L[base][1] + row)[i];
+                two_sum_add(hi, lo, x);
+                ohi[i] = hi;
+                (M.L[out][1] + row)[i] = lo;
+            } else {
+                ohi[i] = bhi[i] + x;
+            }
+        }
+    }
+}
+
+template <bool MIXED, int CW>
+__global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems, const int2* __restrict__ bands,
+                                              int nbands, PassArgs pa) {
+    constexpr int NCH = NTC / CW;
+    extern __shared__ float cs[];
+    __shared__ float carP[NCH][CW], carY[NCH][CW], carry_in[NCH][CW];
+    const int c = threadIdx.x % CW, k = threadIdx.x / CW;
+    for (int it = blockIdx.x; it < nbands; it += gridDim.x) {
+        const int2 bd = bands[it];
+        const MemberDev& M = mems[bd.x];
+        const int n = M.c.ny, P = M.P;
+        const int gx = bd.y + c;
+        const bool col_ok = gx >= 2 && gx < M.c.nx + 2;
+        const int mc = (n + NCH - 1) / NCH;
+        const int i0 = min(n, k * mc), i1 = min(n, i0 + mc);
+        const float* r = M.R[1];
+        const float* cp = M.FYF[0];
+        const float* inv = M.FYF[1];
+        const float* mm = M.FYF[2];
+        __syncthreads();
+        float yv = 0.f, pa_ = 1.f;
+        if (col_ok)
+            for (int i = i0; i < i1; ++i) {
+                const size_t gi = size_t(i + 2) * P + gx;
+                const float m = mm[gi];
+                yv = inv[gi] * r[gi] + m * yv;
+                pa_ *= m;
+                cs[i * CW + c] = yv;
+            }
+        carP[k][c] = pa_;
+        carY[k][c] = yv;
+        __syncthreads();
+        if (k == 0) {
+            float cur = 0.f;
+            for (int q = 0; q < NCH; ++q) {
+                carry_in[q][c] = cur;
+                cur = carY[q][c] + carP[q][c] * cur;
+            }
+        }
+        __syncthreads();
+        float z = 0.f, qa = 1.f;
+        if (col_ok) {
+            const float cin = carry_in[k][c];
+            float pref = 1.f;
+            for (int i = i0; i < i1; ++i) {
+                const size_t gi = size_t(i + 2) * P + gx;
+                pref *= mm[gi];
+                cs[i * CW + c] += pref * cin;
+            }
+            for (int i = i1 - 1; i >= i0; --i) {
+                const size_t gi = size_t(i + 2) * P + gx;
+                const float cv = cp[gi];
+                z = cs[i * CW + c] - cv * z;
+                qa *= -cv;
+                cs[i * CW + c] = z;
+            }
+        }
+        __syncthreads();
+        carP[k][c] = qa;
+        carY[k][c] = z;
+        __syncthreads();
+        if (k == 0) {
+            float cur = 0.f;
+            for (int q = NCH - 1; q >= 0; --q) {
+                carry_in[q][c] = cur;
+                cur = carY[q][c] + carP[q][c] * cur;
+            }
+        }
+        __syncthreads();
+        if (col_ok) {
+            const float cnext = carry_in[k][c];
+            float suf = 1.f;
+            const int out = pa.out, base = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
+            for (int i = i1 - 1; i >= i0; --i) {
+                const size_t gi = size_t(i + 2) * P + gx;
+                suf *= -cp[gi];
+                const float x = cs[i * CW + c] + suf * cnext;
+                if (MIXED) {
+                    float hi = M.S[base][2][gi], lo = M.L[base][2][gi];
+                    two_sum_add(hi, lo, x);
+                    M.S[out][2][gi] = hi;
+                    M.L[out][2][gi] = lo;
+                } else {
+                    M.S[out][2][gi] = M.S[base][2][gi] + x;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Boundary strips (compute.hlsl:985-1309), one side per launch over every member.
+// work item: {member, first strip cell}; 256 strip cells per item.
+// phase 0: compute and write in place; 1: compute into the member's scratch; 2: copy back.
+// ---------------------------------------------------------------------------------------------
+__device__ float3 irregular_tree(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, double t64,
+                                 bool use64, float dh, float g) {
+    float3 stk[17];
+    int sz[17];
+    int top = 0;
+    const int nreal = (dh > CEL_MIN_DEPTH) ? min(b.n_waves, b.nleaf) : 0;
+    int m = 0;
+    while (m < b.nleaf) {
+        float3 v;
+        int s;
+        if (m < nreal) {
+            float e, hu, hv;
+            const float4 wv = waves[b.wave_offset + m];
+            if (use64) sine_wave_t64(xx, yy, t64, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
+            else sine_wave(xx, yy, t, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
+            v = make_float3(e + b.sea_level, hu, hv);
+            s = 1;
+        } else {
+            s = (m == 0) ? b.nleaf : (m & -m);
+            while (m + s > b.nleaf) s >>= 1;
+            v = make_float3(float(s) * b.sea_level, 0.f, 0.f);
+        }
+        m += s;
+        stk[top] = v;
+        sz[top] = s;
+        ++top;
+        while (top >= 2 && sz[top - 1] == sz[top - 2]) {
+            const float3 r = stk[top - 1], l = stk[top - 2];
+            stk[top - 2] = make_float3(l.x + r.x, l.y + r.y, l.z + r.z);
+            sz[top - 2] *= 2;
+            --top;
+        }
+    }
+    return stk[0];
+}
+
+__device__ void uts_lookup(const float* tab, int n, float t, float out[3]) {
+    // timeSeriesHelper (engine.cpp:1882-1904) for a table sorted by time: the first row at or
+    // after t (from row 1 on), linear interpolation from the row before; zero past the end.
+    out[0] = out[1] = out[2] = 0.f;
+    int lo = 1, hi = n;  // first index in [1, n) with tab.t >= t, or n
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        if (tab[4 * mid] < t) lo = mid + 1; else hi = mid;
+    }
+    if (lo >= n) return;
+    const float t0 = tab[4 * (lo - 1)], t1 = tab[4 * lo];
+    const float m = (t - t0) / (t1 - t0);
+    for (int q = 0; q < 3; ++q) {
+        const float v0 = tab[4 * (lo - 1) + q + 1], v1 = tab[4 * lo + q + 1];
+        out[q] = v0 + (v1 - v0) * m;
+    }
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ mems, const int2* __restrict__ items,
+                                                  int nitems, int side, int phase, int out) {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int2 wi = items[it];
+        const MemberDev& M = mems[wi.x];
+        const SimConsts c = M.c;
+        const BoundaryDesc& b = M.bd[side];
+        const int NX = c.NX, NY = c.NY, P = M.P;
+        int x0, y0, sw, sh;
+        if (side == 0) { x0 = 0; sw = NX; y0 = NY - b.width; sh = b.width; }
+        else if (side == 1) { x0 = NX - b.width; sw = b.width; y0 = 0; sh = NY; }
+        else if (side == 2) { x0 = 0; sw = NX; y0 = 0; sh = b.width; }
+        else { x0 = 0; sw = b.width; y0 = 0; sh = NY; }
+        if (x0 < 0) { sw += x0; x0 = 0; }
+        if (y0 < 0) { sh += y0; y0 = 0; }
+        sw = min(sw, NX - x0); sh = min(sh, NY - y0);
+        const int cell = wi.y + threadIdx.x;
+        if (cell >= sw * sh) continue;
+        const int x = x0 + cell % sw, y = y0 + cell / sw;
+        const size_t gi = size_t(y) * P + x;
+        float* W = M.S[out][0];
+        float* HU = M.S[out][1];
+        float* HV = M.S[out][2];
+        if (phase == 2) {
+            W[gi] = M.strip[3 * cell]; HU[gi] = M.strip[3 * cell + 1]; HV[gi] = M.strip[3 * cell + 2];
+            if (MIXED) { M.L[out][0][gi] = 0.f; M.L[out][1][gi] = 0.f; M.L[out][2][gi] = 0.f; }
+            continue;
+        }
+        float ow = 0.f, ou = 0.f, ov = 0.f;
+        float lw = 0.f, lu = 0.f, lv = 0.f;
+        const float sl = b.sea_level;
+        const double t64 = *M.time64;
+        const float t32 = *M.time32;
+        if (b.type == CEL_BC_SOLID) {
+            int qx = x, qy = y;
+            if (side == 3) qx = 4 - x;
+            else if (side == 1) qx = (2 * c.nx + 2) - x;
+            else if (side == 2) qy = 4 - y;
+            else qy = (2 * c.ny + 2) - y;
+            float sw_ = 0.f, su = 0.f, sv = 0.f, lw_ = 0.f, lu_ = 0.f, lv_ = 0.f;
+            if (qx >= 0 && qy >= 0 && qx < NX && qy < NY) {
+                const size_t qi = size_t(qy) * P + qx;
+                sw_ = W[qi]; su = HU[qi]; sv = HV[qi];
+                if (MIXED) { lw_ = M.L[out][0][qi]; lu_ = M.L[out][1][qi]; lv_ = M.L[out][2][qi]; }
+            }
+            ow = sw_; lw = lw_;
+            ou = (side == 1 || side == 3) ? -su : su; lu = (side == 1 || side == 3) ? -lu_ : lu_;
+            ov = (side == 0 || side == 2) ? -sv : sv; lv = (side == 0 || side == 2) ? -lv_ : lv_;
+        } else if (b.type == CEL_BC_SPONGE) {
+            const float dh = fmaxf(CEL_MIN_DEPTH, sl - M.BA[gi]);
+            float L, dist;
+            if (side == 3) { L = float(b.width) * c.dx; dist = float(x) * c.dx; }
+            else if (side == 1) { L = float(b.width) * c.dx; dist = float(NX - x) * c.dx; }
+            else if (side == 2) { L = float(b.width) * c.dy; dist = float(y) * c.dy; }
+            else { L = float(b.width) * c.dy; dist = float(NY - y) * c.dy; }
+            const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * M.dt);
+            ow = gam * (W[gi] - sl) + sl;
+            ou = gam * HU[gi];
+            ov = gam * HV[gi];
+            if (MIXED) { lw = gam * M.L[out][0][gi]; lu = gam * M.L[out][1][gi]; lv = gam * M.L[out][2][gi]; }
+        } else if (b.type == CEL_BC_SINEWAVE) {
+            const float dh = fmaxf(0.f, sl - M.BA[gi]);
+            const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
+            const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
+            float e = 0.f, hu = 0.f, hv = 0.f;
+            if (dh > CEL_MIN_DEPTH) {
+                if (MIXED) sine_wave_t64(xx, yy, t64, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
+                else sine_wave(xx, yy, t32, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
+            }
+            ow = e + sl; ou = hu; ov = hv;
+        } else if (b.type == CEL_BC_UTS) {
+            float v[3];
+            uts_lookup(M.uts[side], M.nuts[side], MIXED ? float(t64) : t32, v);
+            ow = v[0] + sl; ou = v[1]; ov = v[2];
+        } else {
+            const bool colwise = (side == 1 || side == 3);
+            const int along = colwise ? y : x;
+            const int lim = colwise ? c.ny : c.nx;
+            if (along >= 2 && along < lim + 2) {
+                const float dh = fmaxf(0.f, sl - M.BA[gi]);
+                const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
+                const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
+                const float3 r = irregular_tree(b, M.waves, xx, yy, t32, t64, MIXED, dh, c.g);
+                ow = r.x; ou = r.y; ov = r.z;
+            }
+        }
+        if (phase == 1) {
+            M.strip[3 * cell] = ow; M.strip[3 * cell + 1] = ou; M.strip[3 * cell + 2] = ov;
+        } else {
+            W[gi] = ow; HU[gi] = ou; HV[gi] = ov;
+            if (MIXED) { M.L[out][0][gi] = lw; M.L[out][1][gi] = lu; M.L[out][2][gi] = lv; }
+        }
+    }
+}
+
+__global__ void k_advance_time(const MemberDev* __restrict__ mems, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const MemberDev& M = mems[i];
+    *M.time64 += double(M.dt);
+    *M.time32 += M.dt;
+}
+
+// Final Pass1 aux update of the current state (txAuxiliary2 -> reported txAuxiliary1 values are
+// what the device keeps; this kernel is not needed for them).
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------------------
+struct Member {
+    cel_params p{};
+    HostSetup hs;
+    int P = 0;
+    size_t plane = 0;
+    std::vector<float> uts_host[4];
+};
+
+struct Idx {
+    int sin = 0, cur = 0;
+    int og = 0, oog = 1, scr = 2, spare = 3, pred = 3;
+    bool operator==(const Idx& o) const {
+        return sin == o.sin && cur == o.cur && og == o.og && oog == o.oog && scr == o.scr && spare == o.spare;
+    }
+};
+
+}  // namespace cel
+
+struct cel_batch {
+    int form = CEL_FORM_FUSED;
+    bool mixed = false;
+    std::vector<cel::Member> mem;
+    std::vector<cel::MemberDev> hdev;
+    cel::MemberDev* ddev = nullptr;
+    std::vector<void*> allocs;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cel::KernelTimer tm;
+    cel::Scheme sch;      // shared pass sequence (all members use the same correction count)
+    cel::Idx ix;
+    int4* tiles = nullptr; int ntiles = 0;
+    int2* rows = nullptr; int nrows = 0;
+    int2* bands = nullptr; int nbands = 0;
+    int2* bitems[4] = {nullptr, nullptr, nullptr, nullptr};
+    int nbitems[4] = {0, 0, 0, 0};
+    bool two_phase[4] = {false, false, false, false};
+    double* stats_all = nullptr;       // members * STATS_N (per pass, fused into the stencil)
+    double* stats_now_all = nullptr;
+    size_t smem_stencil = 0, smem_rows = 0, smem_cols = 0;
+    int grid_stencil = 0, grid_rows = 0, grid_cols = 0;
+    int sms = 148;
+    bool use_graph = false;
+    std::vector<cudaGraphExec_t> graphs;
+    std::vector<cel::Idx> graph_idx;   // index state at the start of each captured step
+    int graph_pos = 0;
+    long long cells = 0;
+    int tile_x = cel::TX, tile_y = cel::TY, pcr_switch = 0;
+    int cw = 16;
+};
+
+namespace cel {
+
+namespace {
+
+int dalloc(cel_batch* b, void** ptr, size_t bytes, std::string& err) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) { err = std::string("cudaMalloc: ") + cudaGetErrorString(e); return CEL_ERR_CUDA; }
+    e = cudaMemset(q, 0, bytes);
+    if (e != cudaSuccess) { err = std::string("cudaMemset: ") + cudaGetErrorString(e); return CEL_ERR_CUDA; }
+    b->allocs.push_back(q);
+    *ptr = q;
+    return CEL_OK;
+}
+
+#define B_TRY(expr)                                                                     \
+    do {                                                                                \
+        cudaError_t _e = (expr);                                                        \
+        if (_e != cudaSuccess) { err = std::string(#expr) + ": " + cudaGetErrorString(_e); return CEL_ERR_CUDA; } \
+    } while (0)
+
+int upload_state(cel_batch* b, int i, const float* rgba, std::string& err) {
+    Member& m = b->mem[i];
+    const MemberDev& d = b->hdev[i];
+    const int NX = m.hs.NX, NY = m.hs.NY;
+    std::vector<float> pl[3];
+    for (int q = 0; q < 3; ++q) pl[q].assign(m.plane, 0.f);
+    for (int y = 0; y < NY; ++y)
+        for (int x = 0; x < NX; ++x)
+            for (int q = 0; q < 3; ++q) pl[q][size_t(y) * m.P + x] = rgba[(size_t(y) * NX + x) * 4 + q];
+    for (int q = 0; q < 3; ++q) {
+        B_TRY(cudaMemcpyAsync(d.S[b->ix.sin][q], pl[q].data(), m.plane * sizeof(float), cudaMemcpyHostToDevice, b->stream));
+        if (b->mixed) B_TRY(cudaMemsetAsync(d.L[b->ix.sin][q], 0, m.plane * sizeof(float), b->stream));
+    }
+    B_TRY(cudaStreamSynchronize(b->stream));
+    return CEL_OK;
+}
+
+int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
+    const size_t nm = b->mem.size();
+    B_TRY(cudaMemsetAsync(b->stats_all, 0, nm * STATS_N * sizeof(double), b->stream));
+    {
+        TimedLaunch t(&b->tm, b->stream, "fused_stencil");
+        if (b->mixed)
+            k_stencil<true><<<b->grid_stencil, NT1, b->smem_stencil, b->stream>>>(b->ddev, b->tiles, b->ntiles, pa);
+        else
+            k_stencil<false><<<b->grid_stencil, NT1, b->smem_stencil, b->stream>>>(b->ddev, b->tiles, b->ntiles, pa);
+    }
+    {
+        TimedLaunch t(&b->tm, b->stream, "tridiag_rows");
+        if (b->mixed) k_rows<true><<<b->grid_rows, NTR, b->smem_rows, b->stream>>>(b->ddev, b->rows, b->nrows, pa);
+        else k_rows<false><<<b->grid_rows, NTR, b->smem_rows, b->stream>>>(b->ddev, b->rows, b->nrows, pa);
+    }
+    {
+        TimedLaunch t(&b->tm, b->stream, "tridiag_cols");
+        if (b->cw == 16) {
+            if (b->mixed) k_cols<true, 16><<<b->grid_cols, NTC, b->smem_cols, b->stream>>>(b->ddev, b->bands, b->nbands, pa);
+            else k_cols<false, 16><<<b->grid_cols, NTC, b->smem_cols, b->stream>>>(b->ddev, b->bands, b->nbands, pa);
+        } else {
+            if (b->mixed) k_cols<true, 8><<<b->grid_cols, NTC, b->smem_cols, b->stream>>>(b->ddev, b->bands, b->nbands, pa);
+            else k_cols<false, 8><<<b->grid_cols, NTC, b->smem_cols, b->stream>>>(b->ddev, b->bands, b->nbands, pa);
+        }
+    }
+    for (int side : {1, 0, 3, 2}) {
+        if (b->nbitems[side] == 0) continue;
+        const int g = std::min(b->nbitems[side], b->sms * 8);
+        TimedLaunch t(&b->tm, b->stream, "boundary");
+        if (b->two_phase[side]) {
+            if (b->mixed) {
+                k_boundary<true><<<g, 256, 0, b->stream>>>(b->ddev, b->bitems[side], b->nbitems[side], side, 1, pa.out);
+                k_boundary<true><<<g, 256, 0, b->stream>>>(b->ddev, b->bitems[side], b->nbitems[side], side, 2, pa.out);
+            } else {
+                k_boundary<false><<<g, 256, 0, b->stream>>>(b->ddev, b->bitems[side], b->nbitems[side], side, 1, pa.out);
+                k_boundary<false><<<g, 256, 0, b->stream>>>(b->ddev, b->bitems[side], b->nbitems[side], side, 2, pa.out);
+            }
+        } else {
+            if (b->mixed) k_boundary<true><<<g, 256, 0, b->stream>>>(b->ddev, b->bitems[side], b->nbitems[side], side, 0, pa.out);
+            else k_boundary<false><<<g, 256, 0, b->stream>>>(b->ddev, b->bitems[side], b->nbitems[side], side, 0, pa.out);
+        }
+    }
+    B_TRY(cudaGetLastError());
+    return CEL_OK;
+}
+
+// One pass with the host state machine; updates the buffer indices.
+int run_pass(cel_batch* b, std::string& err) {
+    Scheme& s = b->sch;
+    Idx& ix = b->ix;
+    if (!s.initialized) s.choose_dt(0.f);
+    else s.choose_dt(0.f);
+    PassArgs pa{};
+    pa.scheme = s.time_scheme;
+    pa.in = ix.sin;
+    if (s.time_scheme == CEL_SCHEME_CORRECTOR) {
+        pa.cur = ix.cur;
+        pa.out = 3 - pa.in - pa.cur;
+    } else {
+        ix.cur = ix.sin;
+        pa.cur = ix.cur;
+        pa.out = (ix.sin + 1) % 3;
+    }
+    pa.og = ix.og; pa.oog = ix.oog; pa.scr = ix.scr; pa.pred = ix.pred;
+    if (int e = launch_pass(b, pa, err)) return e;
+    const bool was_pred = s.is_predictor();
+    const bool book = s.after_pass();
+    if (book) {
+        const int o = ix.og, oo = ix.oog, sc = ix.scr;
+        ix.og = sc; ix.oog = o; ix.scr = oo;
+        k_advance_time<<<(int(b->mem.size()) + 127) / 128, 128, 0, b->stream>>>(b->ddev, int(b->mem.size()));
+        B_TRY(cudaGetLastError());
+    } else if (was_pred) {
+        ix.pred = ix.scr;
+        std::swap(ix.scr, ix.spare);
+    }
+    ix.sin = pa.out;
+    return CEL_OK;
+}
+
+int run_physical_step(cel_batch* b, std::string& err) {
+    if (int e = run_pass(b, err)) return e;
+    while (b->sch.time_scheme == CEL_SCHEME_CORRECTOR)
+        if (int e = run_pass(b, err)) return e;
+    return CEL_OK;
+}
+
+void free_graphs(cel_batch* b) {
+    for (cudaGraphExec_t g : b->graphs) cudaGraphExecDestroy(g);
+    b->graphs.clear();
+    b->graph_idx.clear();
+    b->graph_pos = 0;
+}
+
+// Captures one graph per physical step until the buffer-rotation state repeats.
+int build_graphs(cel_batch* b, std::string& err) {
+    free_graphs(b);
+    Scheme s0 = b->sch;
+    Idx i0 = b->ix;
+    std::vector<Idx> starts;
+    for (int k = 0; k < 24; ++k) {
+        starts.push_back(b->ix);
+        cudaGraph_t g = nullptr;
+        B_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const bool tm_on = b->tm.enabled;
+        b->tm.enabled = false;
+        int st = run_physical_step(b, err);
+        b->tm.enabled = tm_on;
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+        if (st) { if (g) cudaGraphDestroy(g); return st; }
+        if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return CEL_ERR_CUDA; }
+        cudaGraphExec_t ge = nullptr;
+        ce = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { err = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ce); return CEL_ERR_CUDA; }
+        b->graphs.push_back(ge);
+        if (b->ix == starts[0]) break;
+    }
+    b->graph_idx = starts;
+    b->sch = s0;
+    b->ix = i0;
+    b->graph_pos = 0;
+    return CEL_OK;
+}
+
+}  // namespace
+
+void byte_model(int form, int N, double& stencil, double& step) {
+    // Algorithmic HBM bytes per interior cell (compulsory traffic of this design):
+    //  stencil, predictor: read state 12 + bottom 12 + history 40 + aux 8;
+    //                      write w 4 + rhs 8 + history 20 + aux 8  -> 112
+    //  stencil, corrector: + predicted history 20 + CURRENT_STATE w 4  -> 136
+    //  tridiagonal (x and y): read rhs 8 + factors 24 + base 8, write 8 -> 48
+    //  mixed form: + compensation words: stencil w lo read/write 8, solves hu/hv lo 16 -> +24
+    const double comp = (form == CEL_FORM_MIXED) ? 1.0 : 0.0;
+    const double st_pred = 112 + 8 * comp, st_corr = 136 + 8 * comp;
+    const double tri = 48 + 16 * comp;
+    stencil = st_pred;
+    step = (st_pred + tri) + N * (st_corr + tri);
+}
+
+cel_batch* batch_create(int n, const cel_params* const* params, const float* const* bathy, const int* bnx,
+                        const int* bny, int form, std::string& err) {
+    std::unique_ptr<cel_batch> b(new cel_batch());
+    b->form = form;
+    b->mixed = (form == CEL_FORM_MIXED);
+    const int N0 = params[0]->correction_steps;
+    for (int i = 0; i < n; ++i) {
+        if (params[i]->correction_steps != N0) { err = "batch members must share correctionStepsNum"; return nullptr; }
+        if (params[i]->adaptive) { err = "batches run fixed time steps (adaptive members are not supported)"; return nullptr; }
+        if (params[i]->ny > 6900) { err = "fused form supports ny <= 6900 (column band in shared memory)"; return nullptr; }
+        if (params[i]->nx > 16000) { err = "fused form supports nx <= 16000 (row in shared memory)"; return nullptr; }
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { err = "no CUDA device"; return nullptr; }
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { err = "stream creation failed"; return nullptr; }
+    b->own_stream = true;
+    b->mem.resize(n);
+    b->hdev.resize(n);
+    std::vector<float4> waves;
+    {
+        void* p = nullptr;
+        if (dalloc(b.get(), &p, size_t(n) * STATS_N * sizeof(double), err)) return nullptr;
+        b->stats_all = static_cast<double*>(p);
+        if (dalloc(b.get(), &p, size_t(n) * STATS_N * sizeof(double), err)) return nullptr;
+        b->stats_now_all = static_cast<double*>(p);
+    }
+    std::vector<int4> tiles;
+    std::vector<int2> rows, bands, bitems[4];
+    int max_nx = 0, max_ny = 0;
+    for (int i = 0; i < n; ++i) {
+        Member& m = b->mem[i];
+        m.p = *params[i];
+        if (make_setup(m.p, bathy[i], bnx[i], bny[i], m.hs, err)) return nullptr;
+        // the fused solver needs only the level-0 systems
+        m.hs.ABCx.resize(1);
+        m.hs.ABCy.resize(1);
+        const int NX = m.hs.NX, NY = m.hs.NY;
+        m.P = (NX + 31) / 32 * 32;
+        m.plane = size_t(m.P) * NY;
+        b->cells += (long long)m.hs.nx * m.hs.ny;
+        max_nx = std::max(max_nx, m.hs.nx);
+        max_ny = std::max(max_ny, m.hs.ny);
+        MemberDev& d = b->hdev[i];
+        std::memset(&d, 0, sizeof(d));
+        d.c = make_consts(m.p, m.hs, m.P);
+        d.P = m.P;
+        d.dt = float(m.p.timestep);
+        // planes: state 9 (+9 lo), bottom 3, rhs 2, history 12 + 8, aux 2, factors 6
+        const int nplanes = 9 + (b->mixed ? 9 : 0) + 3 + 2 + 12 + 8 + 2 + 6;
+        void* base = nullptr;
+        if (dalloc(b.get(), &base, m.plane * nplanes * sizeof(float), err)) return nullptr;
+        float* q = static_cast<float*>(base);
+        auto next = [&]() { float* r = q; q += m.plane; return r; };
+        for (int s = 0; s < 3; ++s) for (int k = 0; k < 3; ++k) d.S[s][k] = next();
+        if (b->mixed) for (int s = 0; s < 3; ++s) for (int k = 0; k < 3; ++k) d.L[s][k] = next();
+        float* by = next(); float* bx = next(); float* ba = next();
+        d.BY = by; d.BX = bx; d.BA = ba;
+        d.R[0] = next(); d.R[1] = next();
+        for (int s = 0; s < 4; ++s) for (int k = 0; k < 3; ++k) d.G[s][k] = next();
+        for (int s = 0; s < 4; ++s) for (int k = 0; k < 2; ++k) d.F[s][k] = next();
+        d.AUX[0] = next(); d.AUX[1] = next();
+        float* fx[3]; float* fy[3];
+        for (int k = 0; k < 3; ++k) fx[k] = next();
+        for (int k = 0; k < 3; ++k) fy[k] = next();
+        for (int k = 0; k < 3; ++k) { d.FX[k] = fx[k]; d.FYF[k] = fy[k]; }
+        d.stats = b->stats_all + size_t(i) * STATS_N;
+        d.stats_now = b->stats_now_all + size_t(i) * STATS_N;
+        {
+            void* tp = nullptr;
+            if (dalloc(b.get(), &tp, 64, err)) return nullptr;
+            d.time64 = static_cast<double*>(tp);
+            d.time32 = reinterpret_cast<float*>(static_cast<char*>(tp) + 16);
+        }
+        // upload planes (pitched)
+        auto put = [&](float* dst, const std::vector<float>& src) -> int {
+            std::vector<float> pl(m.plane, 0.f);
+            for (int y = 0; y < NY; ++y) std::memcpy(&pl[size_t(y) * m.P], &src[size_t(y) * NX], NX * sizeof(float));
+            cudaError_t e = cudaMemcpy(dst, pl.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) { err = cudaGetErrorString(e); return CEL_ERR_CUDA; }
+            return CEL_OK;
+        };
+        if (put(by, m.hs.BY) || put(bx, m.hs.BX) || put(ba, m.hs.BA)) return nullptr;
+        {
+            std::vector<float> cpv, inv, mv;
+            thomas_factors_x(m.hs, cpv, inv, mv);
+            if (put(fx[0], cpv) || put(fx[1], inv) || put(fx[2], mv)) return nullptr;
+            thomas_factors_y(m.hs, cpv, inv, mv);
+            if (put(fy[0], cpv) || put(fy[1], inv) || put(fy[2], mv)) return nullptr;
+        }
+        // boundaries
+        const cel_boundary* sides[4] = {&m.p.north, &m.p.east, &m.p.south, &m.p.west};
+        for (int s = 0; s < 4; ++s) {
+            const cel_boundary& bb = *sides[s];
+            BoundaryDesc& bd = d.bd[s];
+            bd.type = bb.type; bd.width = bb.width;
+            bd.sea_level = float(bb.sea_level); bd.amplitude = float(bb.amplitude);
+            bd.period = float(bb.period); bd.theta = float(bb.theta);
+            bd.n_waves = bb.type == CEL_BC_IRREGULAR ? bb.n_waves : 0;
+            const int Kn = (s == 0 || s == 2) ? m.hs.Ky : m.hs.Kx;
+            bd.nleaf = 1 << (Kn - 1);
+            bd.wave_offset = int(waves.size());
+            for (int k = 0; k < bd.n_waves; ++k)
+                waves.push_back(make_float4(float(bb.waves[k][0]), float(bb.waves[k][1]), float(bb.waves[k][2]),
+                                            float(bb.waves[k][3])));
+            if (bb.type == CEL_BC_UTS) {
+                m.uts_host[s].resize(size_t(bb.n_uts) * 4);
+                for (int k = 0; k < 4 * bb.n_uts; ++k) m.uts_host[s][k] = float(bb.uts[k]);
+                void* up = nullptr;
+                if (dalloc(b.get(), &up, m.uts_host[s].size() * sizeof(float), err)) return nullptr;
+                cudaMemcpy(up, m.uts_host[s].data(), m.uts_host[s].size() * sizeof(float), cudaMemcpyHostToDevice);
+                d.uts[s] = static_cast<float*>(up);
+                d.nuts[s] = bb.n_uts;
+            }
+            const int cellsn = (s == 0 || s == 2) ? NX * std::min(bb.width, NY) : std::min(bb.width, NX) * NY;
+            for (int c0 = 0; c0 < cellsn; c0 += 256) bitems[s].push_back(make_int2(i, c0));
+            if (bb.type == CEL_BC_SOLID && bb.width >= 4) b->two_phase[s] = true;
+        }
+        {
+            size_t strip = 0;
+            for (int s = 0; s < 4; ++s) {
+                const int w = sides[s]->width;
+                strip = std::max(strip, size_t((s == 0 || s == 2) ? NX * std::min(w, NY) : std::min(w, NX) * NY));
+            }
+            void* sp = nullptr;
+            if (dalloc(b.get(), &sp, std::max<size_t>(strip, 1) * 3 * sizeof(float), err)) return nullptr;
+            d.strip = static_cast<float*>(sp);
+        }
+        // work lists
+        for (int y0 = 2; y0 < m.hs.ny + 2; y0 += TY)
+            for (int x0 = 2; x0 < m.hs.nx + 2; x0 += TX) tiles.push_back(make_int4(i, x0, y0, 0));
+        for (int y = 2; y < m.hs.ny + 2; ++y) rows.push_back(make_int2(i, y));
+    }
+    // column bands: 16 columns per CTA, or 8 for tall domains (shared-memory capacity)
+    b->cw = (size_t(max_ny) * 16 * sizeof(float) + 8192 <= 227 * 1024) ? 16 : 8;
+    for (int i = 0; i < n; ++i) {
+        // bands start on multiples of the band width so column loads are sector aligned
+        for (int x0 = 0; x0 < b->mem[i].hs.nx + 2; x0 += b->cw) bands.push_back(make_int2(i, x0));
+    }
+    {
+        void* wp = nullptr;
+        if (waves.empty()) waves.push_back(make_float4(0, 0, 0, 0));
+        if (dalloc(b.get(), &wp, waves.size() * sizeof(float4), err)) return nullptr;
+        cudaMemcpy(wp, waves.data(), waves.size() * sizeof(float4), cudaMemcpyHostToDevice);
+        for (auto& d : b->hdev) d.waves = static_cast<float4*>(wp);
+    }
+    // Sort tiles and lines so that large domains are scheduled first (load balance).
+    auto upload_list = [&](auto& v, auto** dst, int& cnt) -> int {
+        cnt = int(v.size());
+        void* p = nullptr;
+        if (dalloc(b.get(), &p, std::max<size_t>(v.size(), 1) * sizeof(v[0]), err)) return CEL_ERR_CUDA;
+        if (!v.empty()) cudaMemcpy(p, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice);
+        *dst = static_cast<std::remove_reference_t<decltype(**dst)>*>(p);
+        return CEL_OK;
+    };
+    if (upload_list(tiles, &b->tiles, b->ntiles) || upload_list(rows, &b->rows, b->nrows) ||
+        upload_list(bands, &b->bands, b->nbands))
+        return nullptr;
+    for (int s = 0; s < 4; ++s)
+        if (upload_list(bitems[s], &b->bitems[s], b->nbitems[s])) return nullptr;
+    {
+        void* p = nullptr;
+        if (dalloc(b.get(), &p, sizeof(MemberDev) * n, err)) return nullptr;
+        b->ddev = static_cast<MemberDev*>(p);
+        cudaMemcpy(b->ddev, b->hdev.data(), sizeof(MemberDev) * n, cudaMemcpyHostToDevice);
+    }
+    b->smem_stencil = sizeof(float) * (6 * SH * SW + 12 * FH * FW + 3 * TY * (TX + 1) + 3 * (TY + 1) * TX);
+    b->smem_rows = sizeof(float) * 3 * (pidx(max_nx) + 1);
+    b->smem_cols = sizeof(float) * size_t(max_ny) * b->cw;
+    if (b->smem_cols + 8192 > 227 * 1024 || b->smem_rows + 8192 > 227 * 1024) { err = "domain too large for the fused solver"; return nullptr; }
+    cudaFuncSetAttribute(k_stencil<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_stencil));
+    cudaFuncSetAttribute(k_stencil<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_stencil));
+    cudaFuncSetAttribute(k_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
+    cudaFuncSetAttribute(k_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
+    cudaFuncSetAttribute(k_cols<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
+    cudaFuncSetAttribute(k_cols<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
+    cudaFuncSetAttribute(k_cols<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
+    cudaFuncSetAttribute(k_cols<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
+    {
+        int occ = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stencil<false>, NT1, b->smem_stencil);
+        b->grid_stencil = std::max(1, std::min(b->ntiles, b->sms * std::max(occ, 1)));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rows<false>, NTR, b->smem_rows);
+        b->grid_rows = std::max(1, std::min(b->nrows, b->sms * std::max(occ, 1) * 4));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cols<false, 16>, NTC, b->smem_cols);
+        b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
+    }
+    b->sch.reset(*params[0]);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { err = std::string("batch setup: ") + cudaGetErrorString(e); return nullptr; }
+    // initial condition
+    for (int i = 0; i < n; ++i) {
+        const HostSetup& hs = b->mem[i].hs;
+        std::vector<float> rgba(size_t(hs.NX) * hs.NY * 4, 0.f);
+        for (size_t k = 0; k < size_t(hs.NX) * hs.NY; ++k) {
+            rgba[4 * k] = hs.ic[3 * k]; rgba[4 * k + 1] = hs.ic[3 * k + 1]; rgba[4 * k + 2] = hs.ic[3 * k + 2];
+        }
+        if (upload_state(b.get(), i, rgba.data(), err)) return nullptr;
+    }
+    return b.release();
+}
+
+void batch_destroy(cel_batch* b) {
+    if (!b) return;
+    free_graphs(b);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (void* a : b->allocs) cudaFree(a);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int batch_set_stream(cel_batch* b, cudaStream_t s, std::string& err) {
+    B_TRY(cudaStreamSynchronize(b->stream));
+    free_graphs(b);
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    b->own_stream = (s == nullptr);
+    if (b->own_stream) B_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    else b->stream = s;
+    return CEL_OK;
+}
+
+int batch_step(cel_batch* b, int nsteps, std::string& err) {
+    for (int k = 0; k < nsteps; ++k) {
+        const bool bootstrap = b->sch.timestep_count < 3;
+        if (b->use_graph && !bootstrap) {
+            if (b->graphs.empty()) { if (int e = build_graphs(b, err)) return e; }
+            // keep the host state machine and indices in step with the replayed graph
+            if (!(b->ix == b->graph_idx[b->graph_pos])) { if (int e = build_graphs(b, err)) return e; }
+            B_TRY(cudaGraphLaunch(b->graphs[b->graph_pos], b->stream));
+            // advance host bookkeeping exactly like run_physical_step without launching
+            Scheme& s = b->sch;
+            Idx& ix = b->ix;
+            do {
+                s.choose_dt(0.f);
+                const int in = ix.sin;
+                int out;
+                if (s.time_scheme == CEL_SCHEME_CORRECTOR) out = 3 - in - ix.cur;
+                else { ix.cur = ix.sin; out = (ix.sin + 1) % 3; }
+                const bool was_pred = s.is_predictor();
+                const bool book = s.after_pass();
+                if (book) { const int o = ix.og, oo = ix.oog, sc = ix.scr; ix.og = sc; ix.oog = o; ix.scr = oo; }
+                else if (was_pred) { ix.pred = ix.scr; std::swap(ix.scr, ix.spare); }
+                ix.sin = out;
+            } while (s.time_scheme == CEL_SCHEME_CORRECTOR);
+            b->graph_pos = (b->graph_pos + 1) % int(b->graphs.size());
+        } else {
+            if (int e = run_physical_step(b, err)) return e;
+        }
+    }
+    return CEL_OK;
+}
+
+int batch_stats(cel_batch* b, cel_stats* out, std::string& err) {
+    const size_t n = b->mem.size();
+    B_TRY(cudaMemsetAsync(b->stats_now_all, 0, n * STATS_N * sizeof(double), b->stream));
+    k_stats_only<<<std::min(b->ntiles, b->sms * 8), 256, 0, b->stream>>>(b->ddev, b->tiles, b->ntiles, b->ix.sin);
+    B_TRY(cudaGetLastError());
+    std::vector<double> v(n * STATS_N);
+    std::vector<double> t(n * 2);
+    B_TRY(cudaMemcpyAsync(v.data(), b->stats_now_all, v.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    std::vector<double> t64(n);
+    for (size_t i = 0; i < n; ++i)
+        B_TRY(cudaMemcpyAsync(&t64[i], b->hdev[i].time64, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    B_TRY(cudaStreamSynchronize(b->stream));
+    for (size_t i = 0; i < n; ++i) {
+        const double* s = &v[i * STATS_N];
+        const Member& m = b->mem[i];
+        const double DENSITY = 1000;
+        const double AREA = double(float(m.p.width) / float(m.hs.nx - 1) * float(m.p.length) / float(m.hs.ny - 1));
+        const double g = m.p.gravity;
+        cel_stats& o = out[i];
+        std::memset(&o, 0, sizeof(o));
+        o.mass = s[0] * DENSITY * AREA;
+        o.potential_energy = s[1] * g * DENSITY * AREA;
+        o.x_momentum = s[2] * DENSITY * AREA;
+        o.y_momentum = s[3] * DENSITY * AREA;
+        o.kinetic_energy = s[4] * 0.5 * DENSITY * AREA;
+        o.total_energy = o.kinetic_energy + o.potential_energy;
+        o.mass_full = s[5];
+        o.max_speed = std::sqrt(s[6]);
+        o.max_depth = s[7];
+        o.cfl_rate = s[8];
+        o.max_froude = std::sqrt(s[9] / g);
+        o.health = s[10] != 0 ? CEL_ERR_NUMERIC : 0;
+        o.timestep = double(float(m.p.timestep));
+        o.cfl_number = o.cfl_rate * o.timestep;
+        o.total_time = t64[i];
+        o.time_scheme = b->sch.time_scheme;
+    }
+    return CEL_OK;
+}
+
+int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err) {
+    if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
+    Member& m = b->mem[i];
+    const MemberDev& d = b->hdev[i];
+    const int NX = m.hs.NX, NY = m.hs.NY;
+    std::vector<float> pl[3], lo[3];
+    for (int q = 0; q < 3; ++q) {
+        pl[q].resize(m.plane);
+        B_TRY(cudaMemcpyAsync(pl[q].data(), d.S[b->ix.sin][q], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+        if (b->mixed) {
+            lo[q].resize(m.plane);
+            B_TRY(cudaMemcpyAsync(lo[q].data(), d.L[b->ix.sin][q], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+        }
+    }
+    B_TRY(cudaStreamSynchronize(b->stream));
+    for (int y = 0; y < NY; ++y)
+        for (int x = 0; x < NX; ++x) {
+            const size_t k = size_t(y) * m.P + x;
+            float* o = rgba + (size_t(y) * NX + x) * 4;
+            for (int q = 0; q < 3; ++q) o[q] = b->mixed ? float(double(pl[q][k]) + double(lo[q][k])) : pl[q][k];
+            o[3] = 0.f;
+        }
+    return CEL_OK;
+}
+
+int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err) {
+    if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
+    return upload_state(b, i, rgba, err);
+}
+
+int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err) {
+    if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
+    Member& m = b->mem[i];
+    const MemberDev& d = b->hdev[i];
+    std::vector<float> a0(m.plane), a1(m.plane);
+    B_TRY(cudaMemcpyAsync(a0.data(), d.AUX[0], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+    B_TRY(cudaMemcpyAsync(a1.data(), d.AUX[1], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+    B_TRY(cudaStreamSynchronize(b->stream));
+    const int NX = m.hs.NX, NY = m.hs.NY;
+    for (int y = 0; y < NY; ++y)
+        for (int x = 0; x < NX; ++x) {
+            float* o = rgba + (size_t(y) * NX + x) * 4;
+            o[0] = a0[size_t(y) * m.P + x]; o[1] = 0.f; o[2] = 0.f; o[3] = a1[size_t(y) * m.P + x];
+        }
+    return CEL_OK;
+}
+
+int batch_use_graph(cel_batch* b, bool enable, std::string& err) {
+    (void)err;
+    if (!enable) free_graphs(b);
+    b->use_graph = enable;
+    return CEL_OK;
+}
+
+long long batch_cells(const cel_batch* b) { return b->cells; }
+
+int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err) {
+    (void)err;
+    b->tile_x = tx; b->tile_y = ty; b->pcr_switch = pcr;
+    return CEL_OK;
+}
+
+KernelTimer* batch_timer(cel_batch* b) { return &b->tm; }
+
+// ---- single-domain fused engine (a batch of one) behind the engine interface ---------------
+namespace {
+
+class FusedEngine : public EngineIface {
+public:
+    cel_batch* b = nullptr;
+    cel_params p{};
+    std::vector<float> bathy;
+    int bnx = 0, bny = 0, form = CEL_FORM_FUSED;
+    ~FusedEngine() override { batch_destroy(b); }
+    int make() {
+        const cel_params* pp = &p;
+        const float* bz = bathy.empty() ? nullptr : bathy.data();
+        std::vector<float> tmp;
+        if (!bz) {
+            if (int st = read_cbf(p.bathymetry_path, &tmp, bnx, bny, err)) return st;
+            bz = tmp.data();
+        }
+        b = batch_create(1, &pp, &bz, &bnx, &bny, form, err);
+        return b ? CEL_OK : CEL_ERR_ARG;
+    }
+    int remesh() override {
+        batch_destroy(b);
+        b = nullptr;
+        return make();
+    }
+    int set_state(const float* rgba) override { return batch_set_state(b, 0, rgba, err); }
+    int get_state(float* rgba) override { return batch_get_state(b, 0, rgba, err); }
+    int get_bottom(float* b3) override {
+        const HostSetup& hs = b->mem[0].hs;
+        for (size_t i = 0; i < hs.BA.size(); ++i) { b3[3 * i] = hs.BY[i]; b3[3 * i + 1] = hs.BX[i]; b3[3 * i + 2] = hs.BA[i]; }
+        return CEL_OK;
+    }
+    int get_aux(float* rgba) override { return batch_get_aux(b, 0, rgba, err); }
+    int reset_timestep(float, float, cel_stats* out) override {
+        b->sch.choose_dt(0.f);
+        if (!out) return CEL_OK;
+        return batch_stats(b, out, err);
+    }
+    int timestep() override { return run_pass(b, err); }
+    int timesteps(int n) override {
+        for (int i = 0; i < n; ++i) if (int e = run_pass(b, err)) return e;
+        return CEL_OK;
+    }
+    int physical_steps(int n) override { return batch_step(b, n, err); }
+    int get_stats(cel_stats* out) override { return batch_stats(b, out, err); }
+    int add_solitary_wave(double, double, double, double) override {
+        err = "cel_add_solitary_wave is available on CEL_FORM_PLAIN engines";
+        return CEL_ERR_STATE;
+    }
+    int set_stream(cudaStream_t s) override { return batch_set_stream(b, s, err); }
+    int synchronize() override {
+        cudaError_t e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) { err = cudaGetErrorString(e); return CEL_ERR_CUDA; }
+        return CEL_OK;
+    }
+    int set_tuning(int tx, int ty, int pcr) override { return batch_set_tuning(b, tx, ty, pcr, err); }
+    KernelTimer* timer() override { return &b->tm; }
+    int nx() const override { return p.nx; }
+    int ny() const override { return p.ny; }
+};
+
+}  // namespace
+
+EngineIface* make_fused_engine(const cel_params& p, const float* bathy, int bnx, int bny, int form, std::string& err) {
+    auto* e = new FusedEngine();
+    e->p = p;
+    e->form = form;
+    e->bnx = bnx;
+    e->bny = bny;
+    if (bathy) e->bathy.assign(bathy, bathy + size_t(bnx) * bny);
+    if (int st = e->make()) {
+        err = e->err;
+        delete e;
+        (void)st;
+        return nullptr;
+    }
+    return e;
+}
+
+}  // namespace cel

@@ -1,0 +1,203 @@
+/*
+ * celeris_b200.h — C ABI of the B200-native Celeris Boussinesq timestep path.
+ *
+ * Drop-in boundary for the reference's `class ShallowWaterEngine` (engine.hpp:58-312):
+ * one `cel_engine` handle equals one engine (one simulated domain) with its own CUDA stream.
+ * Parameters come in as a `cel_params` value (the fields readInputCML fills from a `.cml`
+ * file, main.cpp:500-913) instead of the reference's `initSetting` / `GetSetting` globals.
+ *
+ * Conventions
+ *   - Every function returns `int` status: 0 = CEL_OK, non-zero = error; the message is
+ *     available from `cel_last_error()` (thread-local).  No C++ exception crosses the ABI.
+ *   - Host buffers are owned by the caller; device memory is owned by the library.
+ *   - Grid arrays use the reference texture layout: (nx+4) x (ny+4) texels with two ghost
+ *     cells per side, row-major `y*(nx+4)+x` (engine.cpp:413-489).  State texels are
+ *     {w = eta + still water level, hu, hv, unused} (compute.hlsl:160-164); bottom texels are
+ *     {BY, BX, BA} (terrain_heightfield.hpp:50-52).
+ *   - A handle is not thread-safe; distinct handles may be used concurrently.
+ *   - The library never falls back to a CPU path: without a CUDA device every call that
+ *     needs one returns CEL_ERR_CUDA.
+ */
+#ifndef CELERIS_B200_H
+#define CELERIS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CEL_OK 0
+#define CEL_ERR_ARG 1        /* invalid argument / size */
+#define CEL_ERR_IO 2         /* file missing or malformed */
+#define CEL_ERR_CUDA 3       /* CUDA runtime error or no device */
+#define CEL_ERR_STATE 4      /* call not valid in the handle's current state */
+#define CEL_ERR_NUMERIC 5    /* device health flag: NaN/Inf or negative depth detected */
+
+#define CEL_MAX_WAVES 1000   /* MAX_NUM_OF_IRREGULAR_WAVES (engine.hpp:214) */
+#define CEL_MAX_SOLITONS 100 /* InitSetting::MAX_NUM_SOLITARY (settings.hpp:356) */
+#define CEL_MAX_CR_LEVELS 15 /* ST_MAX_CR_MATRIX_NUM_X/Y (engine.hpp:173-176) */
+
+/* Boundary types (settings.hpp:99-105; the .cml `type` string) */
+#define CEL_BC_SOLID 0
+#define CEL_BC_SPONGE 1
+#define CEL_BC_SINEWAVE 2
+#define CEL_BC_IRREGULAR 3
+#define CEL_BC_UTS 4
+
+/* Solver forms */
+#define CEL_FORM_PLAIN 0  /* FP32, one kernel per reference pass and per CR level */
+#define CEL_FORM_FUSED 1  /* FP32, fused stencil + PCR/Thomas tridiagonal */
+#define CEL_FORM_MIXED 2  /* fused, FP16 coefficients, compensated state, FP64 time/reductions */
+
+/* Time schemes (settings.hpp:298: enum TimeIntegrationScheme) */
+#define CEL_SCHEME_EULER 0
+#define CEL_SCHEME_PREDICTOR 1
+#define CEL_SCHEME_CORRECTOR 2
+#define CEL_SCHEME_PREDICTOR_ADAPTIVE 3
+
+typedef struct cel_boundary {
+    int type;                 /* CEL_BC_* */
+    int width;                /* widthNum: cells in the boundary strip */
+    double sea_level;         /* seaLevel */
+    double amplitude;         /* SineWave amplitude (m) */
+    double period;            /* SineWave period (s) */
+    double theta;             /* SineWave direction (radians; the .cml gives degrees) */
+    int n_waves;              /* IrregularWaves component count (<= CEL_MAX_WAVES) */
+    double waves[CEL_MAX_WAVES][4]; /* amplitude, period, theta (rad), phase */
+    int n_uts;                /* UniformTimeSeries rows */
+    double* uts;              /* n_uts x {t, eta, hu, hv}; owned by the cel_params */
+} cel_boundary;
+
+typedef struct cel_soliton {
+    double H, theta, xc, yc, length; /* theta in radians; length 1e30 = infinite crest */
+} cel_soliton;
+
+typedef struct cel_params {
+    int nx, ny;                       /* gridSize */
+    double width, length;             /* fieldDimensions (x, y extent in m) */
+    double still_water_elevation;     /* fieldDimensions stillWaterElevation */
+    int boussinesq;                   /* model type BSNQ (1) / NLSW (0) */
+    double epsilon, theta;            /* parameters epsilon, Theta */
+    int correction_steps;             /* parameters correctionStepsNum */
+    double timestep;                  /* parameters timestep */
+    int adaptive;                     /* parameters adaptive */
+    double ema_alpha;                 /* parameters exponentialMovingAverageAlpha */
+    double min_timestep_ratio;        /* InitSetting::min_timestep_ratio */
+    int manning;                      /* friction type Manning (1) / Quadratic (0) */
+    double friction;                  /* friction coef */
+    double gravity;                   /* 9.81 (gui_manager.cpp:106) */
+    double dissipation_threshold;     /* graphics dissipationIntensity threshold */
+    double whitewater_decay;          /* graphics dissipationIntensity decay */
+    cel_boundary west, east, south, north;
+    int n_solitons;
+    cel_soliton solitons[CEL_MAX_SOLITONS];
+    char bathymetry_path[1024];       /* bathymetryFilePath, resolved against the .cml folder */
+    char hotstart_path[1024];         /* hotStartFilePath, resolved; "" if none */
+    char project_name[256];
+} cel_params;
+
+/* resetTimestep() outputs (engine.cpp:1685-1746), reduced on the device in FP64. */
+typedef struct cel_stats {
+    double mass, x_momentum, y_momentum;
+    double kinetic_energy, potential_energy, total_energy;
+    double max_speed, max_depth, max_froude;
+    double cfl_rate;      /* max((|u|+c)/dx, (|v|+c)/dy) */
+    double cfl_number;    /* cfl_rate * dt */
+    double timestep;      /* dt for the next pass */
+    double total_time;    /* simulated time */
+    double mass_full;     /* sum of h over every interior cell (FP64), m */
+    int time_scheme;      /* scheme of the next pass (CEL_SCHEME_*) */
+    int health;           /* 0 = ok, else CEL_ERR_NUMERIC */
+} cel_stats;
+
+typedef struct cel_engine cel_engine;
+typedef struct cel_batch cel_batch;
+
+/* ---- errors ---------------------------------------------------------------------------- */
+const char* cel_last_error(void);
+const char* cel_version(void);
+
+/* ---- parameters ------------------------------------------------------------------------- */
+/* InitSetting defaults (settings.hpp:370-438); replaces `InitSetting()` */
+int cel_params_default(cel_params* p);
+/* readInputCML (main.cpp:500-913): lenient XML (unquoted attributes, comments).  Irregular
+ * wave and uniform-time-series files named in the .cml are read too (engine.cpp:3512-3560,
+ * 3863-3909).  Free with cel_params_release. */
+int cel_params_from_cml(const char* path, cel_params* out);
+/* Reads an IrregularWaves component file into a boundary (engine.cpp:3520-3551) */
+int cel_read_irregular_waves(const char* path, cel_boundary* b);
+/* Reads a UniformTimeSeries file into a boundary (engine.cpp:3863-3874) */
+int cel_read_uts(const char* path, cel_boundary* b);
+void cel_params_release(cel_params* p);
+
+/* Reads a .cbf bathymetry grid (terrain_heightfield.cpp:136-209).  If z is NULL, only the
+ * header size is returned. */
+int cel_read_cbf(const char* path, float* z, size_t capacity, int* bnx, int* bny);
+
+/* ---- engine lifecycle (ShallowWaterEngine ctor + remesh, engine.cpp:709-737) ------------- */
+/* bathy: bnx*bny row-major grid spanning x in [-W/2, W/2], y in [0, L] (the .cbf content);
+ * NULL = read params->bathymetry_path.  Builds the staggered bottom, the tridiagonal
+ * coefficients and the initial condition (hot start + solitary waves) and uploads them. */
+int cel_create(const cel_params* p, const float* bathy, int bnx, int bny, int form, cel_engine** out);
+int cel_destroy(cel_engine* h);
+int cel_remesh(cel_engine* h);   /* remesh(R_MESH): back to the initial condition, Euler bootstrap */
+int cel_set_stream(cel_engine* h, void* cuda_stream);   /* NULL = the library's own stream */
+int cel_get_dims(const cel_engine* h, int* nx, int* ny);
+
+/* ---- state import/export in the reference layout ---------------------------------------- */
+int cel_set_state(cel_engine* h, const float* rgba);      /* (nx+4)(ny+4) x {w,hu,hv,_} */
+int cel_get_state(cel_engine* h, float* rgba);
+int cel_get_bottom(cel_engine* h, float* by_bx_ba);      /* (nx+4)(ny+4) x {BY,BX,BA} */
+int cel_get_aux(cel_engine* h, float* rgba);             /* txAuxiliary1: {maxdepth,0,0,breaking} */
+
+/* ---- the step (engine.hpp:64-93) --------------------------------------------------------- */
+/* resetTimestep(realworld_dt, elapsed): stats of the current state, then dt for the next pass */
+int cel_reset_timestep(cel_engine* h, float realworld_dt, float elapsed, cel_stats* out);
+/* timestep(): one pass (Euler, AB3 predictor or AM4 corrector) */
+int cel_timestep(cel_engine* h);
+/* n passes, each preceded by the device-side resetTimestep (no host readback) */
+int cel_timesteps(cel_engine* h, int n);
+/* n physical steps (a predictor/Euler pass plus its correctors), device-side stats */
+int cel_physical_steps(cel_engine* h, int n);
+/* latest device-side stats (copies to host; synchronizes the stream) */
+int cel_get_stats(cel_engine* h, cel_stats* out);
+int cel_add_solitary_wave(cel_engine* h, double H, double theta_deg, double xc, double yc);
+int cel_get_water_height(cel_engine* h, float x, float y, float* out);
+int cel_synchronize(cel_engine* h);
+
+/* ---- batched ensembles: many domains advanced by one launch per phase ------------------- */
+/* params[i] and bathy[i] (bnx[i] x bny[i]) describe member i; form is CEL_FORM_FUSED or
+ * CEL_FORM_MIXED. */
+int cel_batch_create(int n, const cel_params* const* params, const float* const* bathy,
+                     const int* bnx, const int* bny, int form, cel_batch** out);
+int cel_batch_destroy(cel_batch* b);
+int cel_batch_set_stream(cel_batch* b, void* cuda_stream);
+int cel_batch_step(cel_batch* b, int nsteps);            /* physical steps, all members */
+int cel_batch_stats(cel_batch* b, cel_stats* out);        /* n entries */
+int cel_batch_get_state(cel_batch* b, int i, float* rgba);
+int cel_batch_set_state(cel_batch* b, int i, const float* rgba);
+int cel_batch_get_aux(cel_batch* b, int i, float* rgba);
+int cel_batch_use_graph(cel_batch* b, int enable);        /* capture one physical step in a CUDA graph */
+long long cel_batch_cells(const cel_batch* b);            /* sum of interior nx*ny */
+
+/* ---- tuning and measurement ------------------------------------------------------------- */
+/* tile_x, tile_y: stencil tile; pcr_switch: system length at which PCR hands over to Thomas */
+int cel_set_tuning(cel_engine* h, int tile_x, int tile_y, int pcr_switch);
+int cel_batch_set_tuning(cel_batch* b, int tile_x, int tile_y, int pcr_switch);
+/* Per-kernel CUDA-event timing on the launching stream (off by default). */
+int cel_batch_kernel_timing(cel_batch* b, int enable);
+int cel_engine_kernel_timing(cel_engine* h, int enable);
+/* Copies up to cap (name, total ms, launches) records; returns the count in *n. */
+int cel_kernel_times(void* handle, int is_batch, char (*names)[64], double* total_ms, long long* launches,
+                     int cap, int* n);
+/* Algorithmic HBM bytes per cell for one pass of the dominant kernel and for a whole
+ * physical step (the roofline byte model recorded in code). */
+int cel_byte_model(int form, int correction_steps, double* stencil_bytes_per_cell_pass,
+                   double* step_bytes_per_cell);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CELERIS_B200_H */

@@ -1,0 +1,119 @@
+"""CPU-side checks of the C-ABI library: it loads, exports every symbol declared in
+include/celeris_b200.h, parses settings, and refuses to run without a GPU (no CPU fallback)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from celeris_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "celeris_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:const char\*|int|void|long long)\s+(cel_\w+)\s*\(", txt, re.M)))
+
+
+def test_header_symbol_list_matches_binding():
+    assert header_symbols() == sorted(abi.EXPORTED)
+
+
+def test_library_exports_every_symbol(celeris):
+    L = celeris.lib()
+    for name in header_symbols():
+        assert hasattr(L, name), name
+
+
+def test_no_device_is_an_error_not_a_fallback(celeris):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from celeris_b200 import cases
+    p, z, bnx, bny = cases.small_case(16, 12, "solid")
+    with pytest.raises(celeris.CelError):
+        celeris.Engine(p, z, "plain")
+
+
+def test_defaults_match_initsetting(celeris):
+    p = abi.Params()
+    assert celeris.lib().cel_params_default(C.byref(p)) == 0
+    assert (p.nx, p.ny, p.width, p.length) == (100, 100, 100.0, 100.0)
+    assert p.boussinesq == 1 and p.epsilon == 5e-8 and p.theta == 2 and p.timestep == 1e-4
+    assert p.west.type == abi.CEL_BC_SOLID and p.west.width == 2
+
+
+CML = """<?xml version="1.0" ?>
+<Experiment>
+  <name>unit test case</name>
+  <!-- comment with <tags> inside -->
+  <model type = "BSNQ">
+    <parameters epsilon = 5e-12 Theta = 1.5 correctionStepsNum = 2 timestep = 0.005></parameters>
+    <friction type = "Manning" coef = 0.02></friction>
+  </model>
+  <fieldDimensions width = 200 length = 5 stillWaterElevation = 0.25></fieldDimensions>
+  <gridSize nx = 160 ny = 9></gridSize>
+  <bathymetryFilePath> bathy.cbf </bathymetryFilePath>
+  <hotStartFilePath> N/A </hotStartFilePath>
+  <solitaryWave H = 0.05 theta = 30 xc = 45 yc = 2 ></solitaryWave>
+  <solitaryWave H = 0.02 theta = 0 xc = 10 yc = 2 length = 3></solitaryWave>
+  <westBoundary type = "SineWave" seaLevel = 0 widthNum = 2>
+    <sineWave amplitude = 0.1 period = 8 theta = 10></sineWave>
+  </westBoundary>
+  <eastBoundary  type = "Sponge" seaLevel = 0.1 widthNum = 40></eastBoundary>
+  <southBoundary type = "IrregularWaves" seaLevel = 0 widthNum = 2>
+    <filePath> waves.txt </filePath>
+  </southBoundary>
+  <northBoundary type = "UniformTimeSeries" seaLevel = 0 widthNum = 2>
+    <filePath>uts.txt</filePath>
+  </northBoundary>
+  <graphics><surfaceShading type = 2><dissipationIntensity show = true threshold = 0.3 decay = 0.2></dissipationIntensity></surfaceShading></graphics>
+</Experiment>
+"""
+
+
+def test_cml_parser(tmp_path, celeris):
+    (tmp_path / "case.cml").write_text(CML)
+    (tmp_path / "waves.txt").write_text("# header\n[NumberOfWaves] 2\n=====\n0.04 2 .785 0.0\n0.03 3 -.785 1.5\n")
+    (tmp_path / "uts.txt").write_text("comment\n====\n0 0 0 0\n1 0.1 0.2 0.3\n2 0 0 0\n")
+    z = np.arange(12, dtype=np.float32).reshape(3, 4)
+    with open(tmp_path / "bathy.cbf", "w") as f:
+        f.write("[nx] 4\n[ny] 3\n\n====\n")
+        for row in z:
+            f.write(" ".join(f"{v:.3f}" for v in row) + "\n")
+    p = celeris.params_from_cml(str(tmp_path / "case.cml"))
+    assert (p.nx, p.ny, p.width, p.length, p.still_water_elevation) == (160, 9, 200.0, 5.0, 0.25)
+    assert p.epsilon == 5e-12 and p.theta == 1.5 and p.correction_steps == 2 and p.timestep == 0.005
+    assert p.manning == 1 and p.friction == 0.02 and p.boussinesq == 1
+    assert p.n_solitons == 2 and abs(p.solitons[0].theta - np.pi / 6) < 1e-12 and p.solitons[0].length == 1e30
+    assert p.solitons[1].length == 3
+    assert p.west.type == abi.CEL_BC_SINEWAVE and abs(p.west.theta - np.pi / 18) < 1e-12 and p.west.period == 8
+    assert p.east.type == abi.CEL_BC_SPONGE and p.east.width == 40 and p.east.sea_level == 0.1
+    assert p.south.type == abi.CEL_BC_IRREGULAR and p.south.n_waves == 2 and p.south.waves[1][3] == 1.5
+    assert p.north.type == abi.CEL_BC_UTS and p.north.n_uts == 3 and p.north.uts[5] == 0.1
+    assert p.dissipation_threshold == 0.3 and p.whitewater_decay == 0.2
+    assert p.bathymetry_path.decode().endswith("bathy.cbf")
+    np.testing.assert_array_equal(celeris.read_cbf(p.bathymetry_path.decode()), z.round(3))
+    celeris.lib().cel_params_release(C.byref(p))
+
+
+def test_cml_errors(tmp_path, celeris):
+    (tmp_path / "bad.cml").write_text("<Experiment><gridSize nx = 10 ny = 10></Experiment>")
+    with pytest.raises(celeris.CelError):
+        celeris.params_from_cml(str(tmp_path / "bad.cml"))
+    with pytest.raises(celeris.CelError):
+        celeris.params_from_cml(str(tmp_path / "missing.cml"))
+    (tmp_path / "bt.cml").write_text('<E><westBoundary type = "Wall" widthNum = 2></westBoundary></E>')
+    with pytest.raises(celeris.CelError):
+        celeris.params_from_cml(str(tmp_path / "bt.cml"))
+
+
+def test_byte_model(celeris):
+    s, t = celeris.byte_model("fused", 1)
+    assert s == 112 and t == (112 + 48) + (136 + 48)
+    s2, t2 = celeris.byte_model("mixed", 1)
+    assert t2 > t

@@ -1,0 +1,123 @@
+"""GPU parity: the CUDA forms against the CPU oracle on the same seeded inputs.
+
+* plain FP32 form vs the FP32 transcription: the same passes and CR levels in the same order
+  (compiled without FMA), so fields agree to 1e-5 relative (the gate for the plain form);
+* fused FP32 and mixed forms vs the FP64 oracle: eta RMS error within 1e-4 m;
+* batches give the same fields as single-domain fused engines.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from celeris_b200 import cases
+from util import eta_rms, field_errors, rel_ok
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ["solid", "mixed", "sponge", "irregular", "uts"]
+
+
+def _uts_rows():
+    t = np.linspace(0.0, 40.0, 81)
+    return np.stack([t, 0.2 * np.sin(2 * np.pi * t / 5.0), 0.3 * np.sin(2 * np.pi * t / 5.0),
+                     0.05 * np.cos(2 * np.pi * t / 5.0)], axis=1)
+
+
+def _case(kind, nx=40, ny=24, N=1):
+    p, z, bnx, bny = cases.small_case(nx, ny, kind, correction_steps=N)
+    keep = []
+    if kind == "uts":
+        keep += cases.attach_uts(p, "west", _uts_rows())
+        keep += cases.attach_uts(p, "north", _uts_rows())
+    return p, z, bnx, bny, keep
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("N", [0, 1, 2])
+def test_plain_matches_fp32_transcription(celeris, kind, N):
+    p, z, bnx, bny, keep = _case(kind, N=N)
+    ref = O.Oracle(p, z, bnx, bny, "f32")
+    eng = celeris.Engine(p, z, "plain")
+    # state, bottom and aux agree before the first step
+    np.testing.assert_array_equal(eng.bottom().astype(np.float64), ref.bottom())
+    np.testing.assert_allclose(eng.state()[..., :3], ref.state()[..., :3], rtol=0, atol=1e-6)
+    ref.physical_steps(150)
+    eng.physical_steps(150)
+    errs = field_errors(eng.state(), ref.state())
+    assert rel_ok(errs, 1e-5, 1e-9), errs
+    aux_g, aux_r = eng.aux(), ref.aux()
+    np.testing.assert_allclose(aux_g[2:-2, 2:-2, 0], aux_r[2:-2, 2:-2, 0], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("kind", ["mixed", "sponge"])
+def test_plain_pass_by_pass(celeris, kind):
+    p, z, bnx, bny, keep = _case(kind, N=1)
+    ref = O.Oracle(p, z, bnx, bny, "f32")
+    eng = celeris.Engine(p, z, "plain")
+    for k in range(8):
+        s_ref = ref.reset_timestep()
+        s_gpu = eng.reset_timestep()
+        assert s_gpu["time_scheme"] == s_ref["time_scheme"]
+        assert abs(s_gpu["mass"] - s_ref["mass"]) <= 1e-5 * abs(s_ref["mass"])
+        ref.timestep()
+        eng.timestep()
+        errs = field_errors(eng.state(), ref.state())
+        assert rel_ok(errs, 1e-6, 1e-9), (k, errs)
+
+
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+@pytest.mark.parametrize("kind", KINDS)
+def test_fused_forms_vs_fp64_oracle(celeris, form, kind):
+    p, z, bnx, bny, keep = _case(kind, nx=70, ny=45, N=1)
+    ref = O.Oracle(p, z, bnx, bny, "f64")
+    eng = celeris.Engine(p, z, form)
+    ref.physical_steps(200)
+    eng.physical_steps(200)
+    a, b = eng.state(), ref.state()
+    assert np.isfinite(a).all()
+    rms = eta_rms(a, b)
+    assert rms <= 1e-4, rms
+    errs = field_errors(a, b)
+    assert rel_ok(errs, 2e-3, 1e-6), errs
+
+
+def test_batch_equals_single_engines(celeris):
+    members = [_case(k, nx=40 + 8 * i, ny=24 + 4 * i, N=1)[:4] for i, k in enumerate(["solid", "mixed", "sponge", "irregular"])]
+    batch = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    batch.step(30)
+    for i, (p, z, bnx, bny) in enumerate(members):
+        e = celeris.Engine(p, z, "mixed")
+        e.physical_steps(30)
+        np.testing.assert_array_equal(batch.state(i), e.state())
+
+
+def test_batch_graph_replay_matches_direct(celeris):
+    members = [_case(k, nx=48, ny=32, N=1)[:4] for k in ["mixed", "sponge", "irregular"]]
+    b1 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    b2 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    b2.use_graph(True)
+    b1.step(25)
+    b2.step(25)
+    for i in range(len(members)):
+        np.testing.assert_array_equal(b1.state(i), b2.state(i))
+    s1, s2 = b1.stats(), b2.stats()
+    for a, b in zip(s1, s2):
+        assert a["mass_full"] == b["mass_full"]
+        assert abs(a["total_time"] - b["total_time"]) < 1e-12
+
+
+def test_flume_config1_plain_1000_steps(celeris):
+    """C1 (512x64 flume, sine wave-maker): plain FP32 GPU vs the FP32 transcription after
+    1000 physical steps, 1e-5 relative in eta/hu/hv; mass agrees too."""
+    p, z, bnx, bny = cases.config1()
+    ref = O.Oracle(p, z, bnx, bny, "f32")
+    eng = celeris.Engine(p, z, "plain")
+    s_ref = ref.physical_steps(1000)
+    eng.physical_steps(1000)
+    errs = field_errors(eng.state(), ref.state())
+    assert rel_ok(errs, 1e-5, 1e-9), errs
+    s_gpu = eng.reset_timestep()
+    s_ref = ref.reset_timestep()
+    assert abs(s_gpu["mass_full"] - s_ref["mass_full"]) <= 1e-6 * s_ref["mass_full"]
