@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""Benchmark of the Celeris Boussinesq timestep path on B200 (Gcell-steps/s).
+
+Default workload: configuration C4 — a 64-domain uneven ensemble (sizes drawn by seed from
+256^2, 512x256, 1024x512, 1024^2, 2048x512; seeded slopes, bumps and sine wave-makers) advanced
+by the batched mixed-precision form (one launch per phase for all domains, each physical step a
+replayed CUDA graph), with correctionStepsNum = 1 (AB3 predictor + AM4 corrector).
+
+One JSON line on rank 0:
+  value     whole-job Gcell-steps/s with the state resident in HBM (device clock, CUDA events,
+            max over ranks);
+  e2e       the same through the public C ABI with, every step, a host->device upload of the
+            per-member time steps from pinned memory and a device->host read of the step's
+            statistics (mass, energy, CFL — what resetTimestep reads back every pass);
+  roofline  the dominant kernel (the fused stencil) timed live with CUDA events on its stream;
+  cpu_baseline  the FP32 transcription (OpenMP, all host threads) on a bounded sample.
+``--impl reference`` times the CPU implementation of the path (the reference's own shader code
+compiled for the CPU when that build is present, else the FP32 transcription) on the same
+metric.  Multi-GPU (torchrun): every rank runs its own ensemble (weak scaling), no collective in
+the step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c4", choices=["c4", "c2", "c3", "c5"])
+    ap.add_argument("--form", default="mixed", choices=["mixed", "fused"])
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--no-plain", action="store_true", help="skip the per-domain plain FP32 comparison")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def members_for(cfg: str, rank: int, count: int):
+    from celeris_b200 import cases
+    if cfg == "c4":
+        return cases.config4(count, 1, first_member=rank * count), \
+            f"C4 {count}-domain uneven ensemble (256^2..2048x512, dx=1 m, slope+bumps, sine wave-maker, N/S solid, E sponge)"
+    if cfg == "c5":
+        return cases.config5(count, 1, first_member=rank * count), f"C5 {count}-domain ensemble (128..512 sides)"
+    if cfg == "c2":
+        return [cases.config2(member=rank)], "C2 2048^2 single domain, JONSWAP wave-maker, sponges, Manning 0.02"
+    return [cases.config3(4096, 4096)], "C3 4096^2 single domain, solitary wave on a truncated cone"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.f = open(self.path, "w")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample(seconds: float, members):
+    """FP32 transcription (OpenMP) on one representative member: cell-steps per second."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    # the member closest to the ensemble's mean size
+    sizes = [p.nx * p.ny for p, *_ in members]
+    mean = sum(sizes) / len(sizes)
+    k = min(range(len(sizes)), key=lambda i: abs(sizes[i] - mean))
+    p, z, bnx, bny = members[k]
+    o = O.Oracle(p, z, bnx, bny, "f32")
+    o.physical_steps(3)
+    t = o.time_physical_steps(2)
+    n = max(2, int(seconds / max(t / 2, 1e-6)))
+    t = o.time_physical_steps(n)
+    rate = p.nx * p.ny * n / t
+    return rate, O.threads("f32"), f"{n} physical steps of one {p.nx}x{p.ny} member (FP32 transcription, OpenMP)"
+
+
+def reference_arm(args):
+    """CPU implementation of the path on the host cores, same metric and config."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    members, workload = members_for(args.config, 0, args.members)
+    rate, cores, sample = cpu_sample(max(1.0, args.cpu_seconds), members)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    kind = "port"
+    # the reference's own shader code compiled for the CPU, when that build is present
+    try:
+        import ref_shader  # noqa: F401
+        if ref_shader.available():
+            p, z, bnx, bny = members[0]
+            r2, c2, s2 = ref_shader.time_sample(members, max(1.0, args.cpu_seconds))
+            rate, cores, sample, kind = r2, c2, s2, "reference"
+    except Exception:
+        pass
+    val = rate / 1e9
+    out = {"metric": "Gcell-steps/s", "value": val, "unit": "Gcell-steps/s", "impl": "reference",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": workload},
+           "cpu_baseline": {"value": val, "unit": "Gcell-steps/s", "cores": cores, "kind": kind, "sample": sample},
+           "e2e": {"value": val, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.cuda.current_device()
+    import celeris_b200 as cb
+
+    members, workload = members_for(args.config, rank, args.members)
+    batch = cb.Batch([(m[0], m[1]) for m in members], args.form)
+    stream = torch.cuda.Stream()
+    batch.set_stream(stream.cuda_stream)
+    batch.use_graph(True)
+    cells = batch.cells
+    N = members[0][0].correction_steps
+    with torch.cuda.stream(stream):
+        batch.step(max(3, args.warmup))
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident throughput --------------------------------------------------------
+    barrier()
+    clk = Clocks(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    barrier()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    cells_t = torch.tensor([float(cells)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(cells_t, op=dist.ReduceOp.SUM)
+    ms_max = float(ms_t.item())
+    total_cells = float(cells_t.item())
+    value = total_cells * args.steps / (ms_max / 1e3) / 1e9
+
+    # ---- end to end through the C ABI: pinned dt upload + stats readback every step -------
+    n = batch.n
+    dt_pinned = torch.tensor([float(np.float32(m[0].timestep)) for m in members], dtype=torch.float32).pin_memory()
+    e2e_steps = max(5, args.steps // 4)
+    barrier()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        batch.set_timestep(dt_pinned.data_ptr())
+        batch.step(1)
+        batch.stats()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
+    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = total_cells * e2e_steps / (float(e2e_t.item()) / 1e3) / 1e9
+    h2d = n * 4
+    d2h = n * (12 * 8 + 8)
+
+    # ---- roofline of the dominant kernel: per-launch CUDA events, direct launches ----------
+    batch.use_graph(False)
+    batch.kernel_timing(True)
+    kt_steps = 10
+    batch.step(kt_steps)
+    torch.cuda.synchronize()
+    kt = batch.kernel_times()
+    batch.kernel_timing(False)
+    batch.use_graph(True)
+    st_ms, st_n = kt.get("fused_stencil", (0.0, 0))
+    comp = 8.0 if args.form == "mixed" else 0.0
+    stencil_bytes_cell = ((112 + comp) + N * (136 + comp)) / (1 + N)  # average over pass kinds
+    avg_launch_s = st_ms / max(st_n, 1) / 1e3
+    achieved = stencil_bytes_cell * cells / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    traffic = None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "stencil_traffic.json")))
+        traffic = tr["dram_bytes_per_cell"] * cells
+    except Exception:
+        pass
+    total_kernel_ms = sum(v[0] for v in kt.values())
+    shares = {k: round(v[0] / total_kernel_ms, 4) for k, v in kt.items()} if total_kernel_ms > 0 else {}
+    step_bytes = cb.byte_model(args.form, N)[1]
+
+    # ---- per-domain plain FP32 form (the comparison form) ---------------------------------
+    plain = None
+    if not args.no_plain and rank == 0 and args.config in ("c4", "c5"):
+        engines = [cb.Engine(m[0], m[1], "plain") for m in members]
+        for e in engines:
+            e.set_stream(stream.cuda_stream)
+        for e in engines:
+            e.physical_steps(3)
+        torch.cuda.synchronize()
+        psteps = 10
+        e0.record(stream)
+        for _ in range(psteps):
+            for e in engines:
+                e.physical_steps(1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain = cells * psteps / (e0.elapsed_time(e1) / 1e3) / 1e9
+        del engines
+
+    # ---- CPU baseline (rank 0, N=1) ---------------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1:
+        rate, cores, sample = cpu_sample(args.cpu_seconds, members)
+        cpu = {"value": rate / 1e9, "unit": "Gcell-steps/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        out = {
+            "metric": "Gcell-steps/s", "value": value, "unit": "Gcell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload, "form": args.form, "members_per_gpu": len(members),
+                       "cells_per_gpu": cells, "correction_steps": N, "cuda_graph": True,
+                       "l2": "working set (%.1f GB) larger than L2 (126 MB); no flush" % (
+                           cells * 4 * (42 + (9 if args.form == "mixed" else 0)) / 1e9),
+                       "parallelism": f"ensemble sharded by domain over {world} GPU(s)"},
+            "e2e": {"value": e2e_value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "kernel": "fused_stencil", "peak_source": peak_src,
+                         "algorithmic_bytes_per_cell": stencil_bytes_cell, "cells_per_launch": cells,
+                         "avg_launch_ms": avg_launch_s * 1e3},
+            "step_roofline": {"bytes_per_cell_step": step_bytes,
+                              "achieved_gbs": value * 1e9 * step_bytes / world / 1e9,
+                              "frac": value * 1e9 * step_bytes / world / 1e9 / peak if peak else None},
+            "kernel_shares": shares,
+            "gpu_launches": batch.launches_per_step * args.steps,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "plain_per_domain": plain,
+            "vs_plain_per_domain": (value / world / plain) if plain else None,
+        }
+        print(json.dumps(out), flush=True)
+    batch.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -179,6 +179,14 @@ class Batch:
     def use_graph(self, enable: bool = True):
         check(lib().cel_batch_use_graph(self.h, int(enable)))
 
+    @property
+    def launches_per_step(self) -> int:
+        return int(lib().cel_batch_launches_per_step(self.h))
+
+    def set_timestep(self, dt: np.ndarray):
+        """Per-member time step from a float32 array (pinned memory makes the copy async)."""
+        check(lib().cel_batch_set_timestep(self.h, C.cast(C.c_void_p(dt.ctypes.data if isinstance(dt, np.ndarray) else int(dt)), C.POINTER(C.c_float))))
+
     def step(self, n: int = 1):
         check(lib().cel_batch_step(self.h, n))
 

@@ -156,6 +156,8 @@ def _declare(L: C.CDLL) -> None:
         "cel_batch_get_aux": (i, [vp, i, fp]),
         "cel_batch_use_graph": (i, [vp, i]),
         "cel_batch_cells": (C.c_longlong, [vp]),
+        "cel_batch_set_timestep": (i, [vp, fp]),
+        "cel_batch_launches_per_step": (i, [vp]),
         "cel_set_tuning": (i, [vp, i, i, i]),
         "cel_batch_set_tuning": (i, [vp, i, i, i]),
         "cel_batch_kernel_timing": (i, [vp, i]),
@@ -190,6 +192,6 @@ EXPORTED = [
     "cel_add_solitary_wave", "cel_get_water_height", "cel_synchronize",
     "cel_batch_create", "cel_batch_destroy", "cel_batch_set_stream", "cel_batch_step",
     "cel_batch_stats", "cel_batch_get_state", "cel_batch_set_state", "cel_batch_get_aux",
-    "cel_batch_use_graph", "cel_batch_cells", "cel_set_tuning", "cel_batch_set_tuning",
+    "cel_batch_use_graph", "cel_batch_cells", "cel_batch_set_timestep", "cel_batch_launches_per_step", "cel_set_tuning", "cel_batch_set_tuning",
     "cel_batch_kernel_timing", "cel_engine_kernel_timing", "cel_kernel_times", "cel_byte_model",
 ]

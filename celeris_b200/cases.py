@@ -172,21 +172,22 @@ def ensemble_member(nx: int, ny: int, rng: np.random.Generator, correction_steps
     return p, B.astype(np.float32), nx, ny
 
 
-def config4(members: int = 64, correction_steps: int = 1):
-    """C4: 64 domains with sizes drawn by seed from C4_SIZES."""
+def config4(members: int = 64, correction_steps: int = 1, first_member: int = 0):
+    """C4: 64 domains with sizes drawn by seed from C4_SIZES (``first_member`` offsets the seeds,
+    e.g. per rank of a multi-GPU run)."""
     out = []
-    for m in range(members):
+    for m in range(first_member, first_member + members):
         rng = np.random.default_rng(12345 + 4000 + m)
         nx, ny = C4_SIZES[int(rng.integers(0, len(C4_SIZES)))]
         out.append(ensemble_member(nx, ny, rng, correction_steps))
     return out
 
 
-def config5(members: int = 1024, correction_steps: int = 1):
+def config5(members: int = 1024, correction_steps: int = 1, first_member: int = 0):
     """C5: 1024 domains, nx and ny i.i.d. uniform over {128, 160, ..., 512}; Manning 0.02."""
     sizes = list(range(128, 513, 32))
     out = []
-    for m in range(members):
+    for m in range(first_member, first_member + members):
         rng = np.random.default_rng(12345 + 5000 + m)
         nx = sizes[int(rng.integers(0, len(sizes)))]
         ny = sizes[int(rng.integers(0, len(sizes)))]

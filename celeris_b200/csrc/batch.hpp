@@ -23,8 +23,10 @@ int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err);
 int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err);
 int batch_use_graph(cel_batch* b, bool enable, std::string& err);
 long long batch_cells(const cel_batch* b);
+int batch_set_timestep(cel_batch* b, const float* dt, std::string& err);
 int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err);
 KernelTimer* batch_timer(cel_batch* b);
+int batch_launches_per_step(const cel_batch* b);
 void byte_model(int form, int correction_steps, double& stencil_bytes, double& step_bytes);
 
 }  // namespace cel

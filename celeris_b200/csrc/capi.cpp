@@ -324,6 +324,12 @@ int cel_batch_get_aux(cel_batch* b, int i, float* rgba) {
 }
 int cel_batch_use_graph(cel_batch* b, int enable) { BAT(b); CEL_GUARD_BEGIN BRET(cel::batch_use_graph(b, enable != 0, err)); CEL_GUARD_END }
 long long cel_batch_cells(const cel_batch* b) { return b ? cel::batch_cells(b) : 0; }
+int cel_batch_launches_per_step(const cel_batch* b) { return b ? cel::batch_launches_per_step(b) : 0; }
+int cel_batch_set_timestep(cel_batch* b, const float* dt) {
+    BAT(b);
+    if (!dt) { set_error("null buffer"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN BRET(cel::batch_set_timestep(b, dt, err)); CEL_GUARD_END
+}
 int cel_batch_set_tuning(cel_batch* b, int tx, int ty, int pcr) {
     BAT(b);
     CEL_GUARD_BEGIN BRET(cel::batch_set_tuning(b, tx, ty, pcr, err)); CEL_GUARD_END

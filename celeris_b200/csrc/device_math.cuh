@@ -1,6 +1,12 @@
 // Device restatements of the per-cell shader helpers of compute.hlsl (lines cited per
 // function).  Operation order follows the shader expressions, so a translation unit compiled
 // with -fmad=false reproduces IEEE single-precision results of the same expressions.
+//
+// Transcendentals: with CEL_EXACT_FP32 defined (the plain form) every single-precision
+// transcendental is evaluated in double and rounded once to float — the correctly rounded
+// value, which the FP32 transcription on the CPU computes the same way, so the two agree bit for
+// bit.  Without it (fused forms) the CUDA single-precision functions are used.  All helpers
+// have internal linkage because the two builds differ.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -8,6 +14,23 @@
 #include "celeris_internal.hpp"
 
 namespace cel {
+namespace {
+
+#ifdef CEL_EXACT_FP32
+__device__ __forceinline__ float t_sin(float x) { return float(sin(double(x))); }
+__device__ __forceinline__ float t_cos(float x) { return float(cos(double(x))); }
+__device__ __forceinline__ float t_tanh(float x) { return float(tanh(double(x))); }
+__device__ __forceinline__ float t_atan(float x) { return float(atan(double(x))); }
+__device__ __forceinline__ float t_cosh(float x) { return float(cosh(double(x))); }
+__device__ __forceinline__ float t_pow(float x, float y) { return float(pow(double(x), double(y))); }
+#else
+__device__ __forceinline__ float t_sin(float x) { return sinf(x); }
+__device__ __forceinline__ float t_cos(float x) { return cosf(x); }
+__device__ __forceinline__ float t_tanh(float x) { return tanhf(x); }
+__device__ __forceinline__ float t_atan(float x) { return atanf(x); }
+__device__ __forceinline__ float t_cosh(float x) { return coshf(x); }
+__device__ __forceinline__ float t_pow(float x, float y) { return powf(x, y); }
+#endif
 
 #define CEL_MIN_DEPTH 0.0001f  // compute.hlsl:1062
 #define CEL_PI_F 3.14159274101257324f  // 4*atan(1.0f) in float (engine.cpp:89)
@@ -56,28 +79,28 @@ __device__ __forceinline__ float numflux(float ap, float am, float Fp, float Fm,
 __device__ __forceinline__ float friction_calc(float hu, float hv, float h, float friction, int manning, float g,
                                                float eps) {
     float f = friction;
-    const float h4 = powf(h, 4.0f);
+    const float h4 = t_pow(h, 4.0f);
     const float dbh = 1.41421354f * h / sqrtf(h4 + fmaxf(h4, eps));
-    if (manning == 1) f = g * friction * friction * powf(fabsf(dbh), 0.3333f);
+    if (manning == 1) f = g * friction * friction * t_pow(fabsf(dbh), 0.3333f);
     return f * sqrtf(hu * hu + hv * hv) * dbh * dbh;
 }
 
 // SpongeFunction (compute.hlsl:1056-1059)
 __device__ __forceinline__ float sponge_fn(float L, float x) {
-    return 0.5f + 0.5f * cosf(CEL_PI_F * fmaxf(L - x, 0.f) / L);
+    return 0.5f + 0.5f * t_cos(CEL_PI_F * fmaxf(L - x, 0.f) / L);
 }
 
 // sineWave with Eckart's wavenumber (compute.hlsl:1080-1101); t is float as in the reference.
 __device__ __forceinline__ void sine_wave(float x, float y, float t, float d, float amp, float period,
                                           float th, float phase, float g, float& e, float& hu, float& hv) {
     const float omega = 2.f * CEL_PI_F / period;
-    const float k = omega * omega / (g * sqrtf(tanhf(omega * omega * d / g)));
+    const float k = omega * omega / (g * sqrtf(t_tanh(omega * omega * d / g)));
     const float c = omega / k;
-    const float kx = cosf(th) * x * k;
-    const float ky = sinf(th) * y * k;
-    e = amp * sinf(omega * t - kx - ky + phase);
-    hu = c * cosf(th) * e;
-    hv = c * sinf(th) * e;
+    const float kx = t_cos(th) * x * k;
+    const float ky = t_sin(th) * y * k;
+    e = amp * t_sin(omega * t - kx - ky + phase);
+    hu = c * t_cos(th) * e;
+    hv = c * t_sin(th) * e;
 }
 
 // The same with the phase omega*t evaluated in FP64 and reduced modulo 2*pi before the FP32
@@ -97,4 +120,5 @@ __device__ __forceinline__ void sine_wave_t64(float x, float y, double t, float 
     hv = c * sinf(th) * e;
 }
 
+}  // namespace
 }  // namespace cel

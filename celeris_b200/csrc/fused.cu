@@ -53,7 +53,7 @@ constexpr int STATS_N = 12;
 struct MemberDev {
     SimConsts c;
     int P;                  // plane pitch in floats
-    float dt;
+    const float* dtp;       // this member's time step (device table, host-updatable)
     float* S[3][3];         // state buffers [buffer][w, hu, hv]
     float* L[3][3];         // compensation words (mixed form)
     const float* BY;
@@ -179,7 +179,8 @@ __global__ void __launch_bounds__(NT1) k_stencil(const MemberDev* __restrict__ m
         }
         __syncthreads();
         // ---- Pass1: faces over [x0-1, x0+TX+1) x [y0-1, y0+TY+1), with the aux update ----
-        const float decay = powf(fabsf(c.whitewater_decay_rate), M.dt);
+        const float dtm = *M.dtp;
+        const float decay = t_pow(fabsf(c.whitewater_decay_rate), dtm);
         for (int k = tid; k < FA; k += NT1) {
             const int fy = k / FW, fx = k - fy * FW;
             const int si = (fy + 1) * SW + (fx + 1);
@@ -206,7 +207,7 @@ __global__ void __launch_bounds__(NT1) k_stencil(const MemberDev* __restrict__ m
                 const int cx = gx < 2 ? 2 : gx, cy = gy < 2 ? 2 : gy;
                 if (cx >= x0 && cx < x0 + TX && cy >= y0 && cy < y0 + TY) {
                     const size_t gi = size_t(gy) * P + gx;
-                    const float msd = atanf(fmaxf(sd1 * c.one_over_dx, sd2 * c.one_over_dy));
+                    const float msd = t_atan(fmaxf(sd1 * c.one_over_dx, sd2 * c.one_over_dy));
                     const float md = fmaxf((hN + hE + hS + hW) / 4.0f, M.AUX[0][gi]);
                     float bw = M.AUX[1][gi];
                     if (msd > c.dissipation_threshold) bw = 1.0f;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(NT1) k_stencil(const MemberDev* __restrict__ m
                                             (ddy * ((odx / 2.0f) * (sHV[si + 1] - sHV[si - 1])))));
             const float Gs = (sixth * dh * (ddx * ((ody / 2.0f) * (sHU[si + SW] - sHU[si - SW])) +
                                             (ddy * ((odx / 2.0f) * (sHU[si + 1] - sHU[si - 1])))));
-            const float dt = M.dt;
+            const float dt = dtm;
             float dw, rhu, rhv;
             float wbase = wc, wbase_lo = 0.f;
             if (pa.scheme == CEL_SCHEME_EULER) {
@@ -730,7 +731,7 @@ __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ 
             else if (side == 1) { L = float(b.width) * c.dx; dist = float(NX - x) * c.dx; }
             else if (side == 2) { L = float(b.width) * c.dy; dist = float(y) * c.dy; }
             else { L = float(b.width) * c.dy; dist = float(NY - y) * c.dy; }
-            const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * M.dt);
+            const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * (*M.dtp));
             ow = gam * (W[gi] - sl) + sl;
             ou = gam * HU[gi];
             ov = gam * HV[gi];
@@ -774,8 +775,8 @@ __global__ void k_advance_time(const MemberDev* __restrict__ mems, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const MemberDev& M = mems[i];
-    *M.time64 += double(M.dt);
-    *M.time32 += M.dt;
+    *M.time64 += double(*M.dtp);
+    *M.time32 += *M.dtp;
 }
 
 // Final Pass1 aux update of the current state (txAuxiliary2 -> reported txAuxiliary1 values are
@@ -823,6 +824,8 @@ struct cel_batch {
     bool two_phase[4] = {false, false, false, false};
     double* stats_all = nullptr;       // members * STATS_N (per pass, fused into the stencil)
     double* stats_now_all = nullptr;
+    float* dt_table = nullptr;         // per-member time step on the device
+    float* dt_host = nullptr;          // pinned mirror of dt_table
     size_t smem_stencil = 0, smem_rows = 0, smem_cols = 0;
     int grid_stencil = 0, grid_rows = 0, grid_cols = 0;
     int sms = 148;
@@ -1040,6 +1043,10 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         b->stats_all = static_cast<double*>(p);
         if (dalloc(b.get(), &p, size_t(n) * STATS_N * sizeof(double), err)) return nullptr;
         b->stats_now_all = static_cast<double*>(p);
+        if (dalloc(b.get(), &p, size_t(n) * sizeof(float), err)) return nullptr;
+        b->dt_table = static_cast<float*>(p);
+        if (cudaMallocHost(&p, size_t(n) * sizeof(float)) != cudaSuccess) { err = "cudaMallocHost failed"; return nullptr; }
+        b->dt_host = static_cast<float*>(p);
     }
     std::vector<int4> tiles;
     std::vector<int2> rows, bands, bitems[4];
@@ -1061,7 +1068,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         std::memset(&d, 0, sizeof(d));
         d.c = make_consts(m.p, m.hs, m.P);
         d.P = m.P;
-        d.dt = float(m.p.timestep);
+        b->dt_host[i] = float(m.p.timestep);
+        d.dtp = b->dt_table + i;
         // planes: state 9 (+9 lo), bottom 3, rhs 2, history 12 + 8, aux 2, factors 6
         const int nplanes = 9 + (b->mixed ? 9 : 0) + 3 + 2 + 12 + 8 + 2 + 6;
         void* base = nullptr;
@@ -1202,6 +1210,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
     }
     b->sch.reset(*params[0]);
+    cudaMemcpy(b->dt_table, b->dt_host, sizeof(float) * n, cudaMemcpyHostToDevice);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { err = std::string("batch setup: ") + cudaGetErrorString(e); return nullptr; }
     // initial condition
@@ -1221,6 +1230,7 @@ void batch_destroy(cel_batch* b) {
     free_graphs(b);
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (void* a : b->allocs) cudaFree(a);
+    if (b->dt_host) cudaFreeHost(b->dt_host);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -1298,7 +1308,7 @@ int batch_stats(cel_batch* b, cel_stats* out, std::string& err) {
         o.cfl_rate = s[8];
         o.max_froude = std::sqrt(s[9] / g);
         o.health = s[10] != 0 ? CEL_ERR_NUMERIC : 0;
-        o.timestep = double(float(m.p.timestep));
+        o.timestep = double(b->dt_host[i]);
         o.cfl_number = o.cfl_rate * o.timestep;
         o.total_time = t64[i];
         o.time_scheme = b->sch.time_scheme;
@@ -1362,6 +1372,17 @@ int batch_use_graph(cel_batch* b, bool enable, std::string& err) {
 
 long long batch_cells(const cel_batch* b) { return b->cells; }
 
+int batch_set_timestep(cel_batch* b, const float* dt, std::string& err) {
+    // the uniform time step of each member (the reference's "uniform time step" setting,
+    // uploaded with the constant buffers before every pass, engine.cpp:1728-1750)
+    for (size_t i = 0; i < b->mem.size(); ++i) {
+        if (!(dt[i] > 0.f)) { err = "time steps must be > 0"; return CEL_ERR_ARG; }
+        b->dt_host[i] = dt[i];
+    }
+    B_TRY(cudaMemcpyAsync(b->dt_table, b->dt_host, sizeof(float) * b->mem.size(), cudaMemcpyHostToDevice, b->stream));
+    return CEL_OK;
+}
+
 int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err) {
     (void)err;
     b->tile_x = tx; b->tile_y = ty; b->pcr_switch = pcr;
@@ -1369,6 +1390,13 @@ int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err) {
 }
 
 KernelTimer* batch_timer(cel_batch* b) { return &b->tm; }
+
+int batch_launches_per_step(const cel_batch* b) {
+    int per_pass = 3;  // stencil, row solve, column solve
+    for (int s = 0; s < 4; ++s)
+        if (b->nbitems[s] > 0) per_pass += b->two_phase[s] ? 2 : 1;
+    return (1 + b->sch.N) * per_pass + 1;  // + the clock advance
+}
 
 // ---- single-domain fused engine (a batch of one) behind the engine interface ---------------
 namespace {

@@ -3,6 +3,7 @@
 // restatement of timestep()/resetTimestep() (engine.cpp:849-1756) and of the compute.hlsl
 // pixel shaders; it is compiled with -fmad=false so its arithmetic follows the FP32
 // transcription operation by operation.  One domain per launch set.
+#define CEL_EXACT_FP32 1
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,7 +40,7 @@ __global__ void k_pass1(const float4* __restrict__ st, const float4* __restrict_
     reconstruct_sd(c.two_theta, w.x, cc.x, e.x, wW, wE, sd);
     msd = sd * c.one_over_dx;
     reconstruct_sd(c.two_theta, s.x, cc.x, n.x, wS, wN, sd);
-    msd = atanf(fmaxf(msd, sd * c.one_over_dy));
+    msd = t_atan(fmaxf(msd, sd * c.one_over_dy));
     reconstruct(c.two_theta, w.y, cc.y, e.y, huW, huE);
     reconstruct(c.two_theta, s.y, cc.y, n.y, huS, huN);
     reconstruct(c.two_theta, w.z, cc.z, e.z, hvW, hvE);
@@ -92,7 +93,7 @@ __global__ void k_pass2(const float4* __restrict__ H, const float4* __restrict__
     yf.w = 0.f;
     XF[i] = xf; YF[i] = yf;
     const float4 a2 = aux2[i];
-    aux1[i] = make_float4(a2.x, 0.f, a2.z, a2.w * powf(fabsf(c.whitewater_decay_rate), dt));
+    aux1[i] = make_float4(a2.x, 0.f, a2.z, a2.w * t_pow(fabsf(c.whitewater_decay_rate), dt));
 }
 
 struct Pass3Args {
@@ -488,11 +489,11 @@ __global__ void k_add_solitary(const float4* __restrict__ copy, const float4* __
     const size_t i = size_t(y) * c.NX + x;
     const float4 s = copy[i];
     const float depth = fmaxf(s.x - bot[i].z, 0.f);
-    const float K = sqrtf(0.75f * fabsf(H) / powf(depth, 3.0f));
+    const float K = sqrtf(0.75f * fabsf(H) / t_pow(depth, 3.0f));
     const float C = sqrtf(c.g * (H + depth));
-    const float ch = coshf(K * ((float(x) * c.dx - xc) * cosf(th) + (float(y) * c.dy - yc) * sinf(th)));
-    const float e = H * 1.0f / powf(ch, 2.0f);
-    st[i] = make_float4(s.x + e, s.y + C * cosf(th) * e, s.z + C * sinf(th) * e, 0.f);
+    const float ch = t_cosh(K * ((float(x) * c.dx - xc) * t_cos(th) + (float(y) * c.dy - yc) * t_sin(th)));
+    const float e = H * 1.0f / t_pow(ch, 2.0f);
+    st[i] = make_float4(s.x + e, s.y + C * t_cos(th) * e, s.z + C * t_sin(th) * e, 0.f);
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -168,6 +168,9 @@ void initial_condition(const cel_params& p, const std::vector<float>* hot, HostS
             for (int q = 0; q < p.n_solitons; ++q) {
                 const cel_soliton& sw = p.solitons[q];
                 if (sw.H == 0) continue;
+                // Over a dry cell the sech^2 profile tends to 0; the reference's formula gives
+                // 0 * sqrt(0/0) = NaN there for a zero-height taper, so the term is skipped.
+                if (depth == 0) continue;
                 const float th = float(sw.theta), H = float(sw.H), xc = float(sw.xc), yc = float(sw.yc);
                 const float len = float(sw.length);
                 const float xs = s.dx * float(i), ys = s.dy * float(j);

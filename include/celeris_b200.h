@@ -180,6 +180,11 @@ int cel_batch_set_state(cel_batch* b, int i, const float* rgba);
 int cel_batch_get_aux(cel_batch* b, int i, float* rgba);
 int cel_batch_use_graph(cel_batch* b, int enable);        /* capture one physical step in a CUDA graph */
 long long cel_batch_cells(const cel_batch* b);            /* sum of interior nx*ny */
+/* Per-member uniform time step (n floats), uploaded asynchronously on the batch stream; the
+ * reference uploads dt with its constant buffers before every pass (engine.cpp:1728-1750). */
+int cel_batch_set_timestep(cel_batch* b, const float* dt);
+/* Kernel launches one physical step issues (all members together). */
+int cel_batch_launches_per_step(const cel_batch* b);
 
 /* ---- tuning and measurement ------------------------------------------------------------- */
 /* tile_x, tile_y: stencil tile; pcr_switch: system length at which PCR hands over to Thomas */

@@ -137,6 +137,23 @@ inline int count_of_matrices(int n) {  // st_getCountOfMatrices (engine.cpp:741-
     return c;
 }
 
+// Transcendentals: in the float build each one is evaluated in double and rounded once to
+// float (the correctly rounded value); the plain GPU form computes them the same way, so the two
+// FP32 paths agree bit for bit.  (The reference's HLSL intrinsics are approximate GPU
+// instructions; no CPU restatement can reproduce them exactly.)
+template <typename R> inline R t_sin(R x) { return std::sin(x); }
+template <typename R> inline R t_cos(R x) { return std::cos(x); }
+template <typename R> inline R t_tanh(R x) { return std::tanh(x); }
+template <typename R> inline R t_atan(R x) { return std::atan(x); }
+template <typename R> inline R t_cosh(R x) { return std::cosh(x); }
+template <typename R> inline R t_pow(R x, R y) { return std::pow(x, y); }
+template <> inline float t_sin<float>(float x) { return float(std::sin(double(x))); }
+template <> inline float t_cos<float>(float x) { return float(std::cos(double(x))); }
+template <> inline float t_tanh<float>(float x) { return float(std::tanh(double(x))); }
+template <> inline float t_atan<float>(float x) { return float(std::atan(double(x))); }
+template <> inline float t_cosh<float>(float x) { return float(std::cosh(double(x))); }
+template <> inline float t_pow<float>(float x, float y) { return float(std::pow(double(x), double(y))); }
+
 // ---------------------------------------------------------------------------------------
 // The engine (templated on the arithmetic type)
 // ---------------------------------------------------------------------------------------
@@ -339,6 +356,9 @@ public:
                 }
                 for (const Soliton& s : p.solitons) {
                     if (s.H == 0) continue;
+                    // Dry cell: the sech^2 profile's limit is 0 there; the reference evaluates
+                    // 0 * sqrt(0/0) = NaN for a zero-height taper and at the crest line.
+                    if (depth == 0) continue;
                     const R th = R(s.theta);
                     const R vd = std::abs(std::sin(th) * (dx * R(i) - R(s.xc))) +
                                  std::abs(std::cos(th) * (dy * R(j) - R(s.yc)));
@@ -404,7 +424,7 @@ public:
                 reconstruct(w_.r, c.r, e.r, wW, wE, sd);
                 msd = sd * odx;
                 reconstruct(s.r, c.r, n.r, wS, wN, sd);
-                msd = std::atan(std::max(msd, sd * ody));
+                msd = t_atan(std::max(msd, sd * ody));
                 reconstruct(w_.g, c.g, e.g, huW, huE, sd);
                 reconstruct(s.g, c.g, n.g, huS, huN, sd);
                 reconstruct(w_.b, c.b, e.b, hvW, hvE, sd);
@@ -431,7 +451,7 @@ public:
     void pass2() {
         const R g = g_(), half_g = R(0.5) * g;
         const R decay = R(1) / (R(1) + R(2) * R(p.whitewater_decay));
-        const R decay_dt = std::pow(std::abs(decay), dt_());
+        const R decay_dt = t_pow(std::abs(decay), dt_());
         std::fill(xflux.begin(), xflux.end(), T4());
         std::fill(yflux.begin(), yflux.end(), T4());
 #pragma omp parallel for schedule(static)
@@ -466,11 +486,11 @@ public:
 
     R friction_calc(R hu, R hv, R h) const {  // compute.hlsl:544-553
         R f = R(p.friction);
-        const R h4 = std::pow(h, R(4));
+        const R h4 = t_pow(h, R(4));
         const R dbh = std::sqrt(R(2)) * h / std::sqrt(h4 + std::max(h4, eps));
         if (p.manning) {
             const R expo = std::is_same<R, float>::value ? R(0.3333f) : R(0.3333);
-            f = g_() * R(p.friction) * R(p.friction) * std::pow(std::abs(dbh), expo);
+            f = g_() * R(p.friction) * R(p.friction) * t_pow(std::abs(dbh), expo);
         }
         return f * std::sqrt(hu * hu + hv * hv) * dbh * dbh;
     }
@@ -682,15 +702,15 @@ public:
     }
 
     // ---- Boundaries (compute.hlsl:985-1309, engine.cpp:1236-1438) ---------------------------
-    R sponge_fn(R L, R x) const { return R(0.5) + R(0.5) * std::cos(PI_ * std::max(L - x, R(0)) / L); }
+    R sponge_fn(R L, R x) const { return R(0.5) + R(0.5) * t_cos(PI_ * std::max(L - x, R(0)) / L); }
     void sine_wave(R x, R y, R t, R d, R amp, R period, R th, R phase, R out[3]) const {
         const R omega = 2 * PI_ / period;
-        const R k = omega * omega / (g_() * std::sqrt(std::tanh(omega * omega * d / g_())));
+        const R k = omega * omega / (g_() * std::sqrt(t_tanh(omega * omega * d / g_())));
         const R c = omega / k;
-        const R kx = std::cos(th) * x * k;
-        const R ky = std::sin(th) * y * k;
-        const R e = amp * std::sin(omega * t - kx - ky + phase);
-        out[0] = e; out[1] = c * std::cos(th) * e; out[2] = c * std::sin(th) * e;
+        const R kx = t_cos(th) * x * k;
+        const R ky = t_sin(th) * y * k;
+        const R e = amp * t_sin(omega * t - kx - ky + phase);
+        out[0] = e; out[1] = c * t_cos(th) * e; out[2] = c * t_sin(th) * e;
     }
     static bool inb(int x, int y, int NXX, int NYY) { return x >= 0 && y >= 0 && x < NXX && y < NYY; }
 
@@ -934,11 +954,11 @@ public:
             for (int x = 1; x < nx + 3; ++x) {
                 const T4 c = copy[at(x, y)];
                 const R depth = std::max(c.r - BA[at(x, y)], R(0));
-                const R K = std::sqrt(R(0.75) * std::abs(R(Hh)) / std::pow(depth, R(3)));
+                const R K = std::sqrt(R(0.75) * std::abs(R(Hh)) / t_pow(depth, R(3)));
                 const R C = std::sqrt(g_() * (R(Hh) + depth));
-                const R ch = std::cosh(K * ((R(x) * dx - R(xc)) * std::cos(th) + (R(y) * dy - R(yc)) * std::sin(th)));
-                const R e = R(Hh) * R(1) / std::pow(ch, R(2));
-                T4 o = c; o.r = c.r + e; o.g = c.g + C * std::cos(th) * e; o.b = c.b + C * std::sin(th) * e; o.a = 0;
+                const R ch = t_cosh(K * ((R(x) * dx - R(xc)) * t_cos(th) + (R(y) * dy - R(yc)) * t_sin(th)));
+                const R e = R(Hh) * R(1) / t_pow(ch, R(2));
+                T4 o = c; o.r = c.r + e; o.g = c.g + C * t_cos(th) * e; o.b = c.b + C * t_sin(th) * e; o.a = 0;
                 st[at(x, y)] = o;
             }
     }

@@ -27,6 +27,10 @@ def _uts_rows():
 
 def _case(kind, nx=40, ny=24, N=1):
     p, z, bnx, bny = cases.small_case(nx, ny, kind, correction_steps=N)
+    if N == 0:
+        # Pure AB3 (no corrector) at Courant 0.2 is unstable on these steep run-up cases in the
+        # FP64 oracle as well; half the step keeps the method inside its stability region.
+        p.timestep *= 0.5
     keep = []
     if kind == "uts":
         keep += cases.attach_uts(p, "west", _uts_rows())
@@ -45,8 +49,11 @@ def test_plain_matches_fp32_transcription(celeris, kind, N):
     np.testing.assert_allclose(eng.state()[..., :3], ref.state()[..., :3], rtol=0, atol=1e-6)
     ref.physical_steps(150)
     eng.physical_steps(150)
-    errs = field_errors(eng.state(), ref.state())
+    a, b = eng.state(), ref.state()
+    errs = field_errors(a, b)
     assert rel_ok(errs, 1e-5, 1e-9), errs
+    # with correctly rounded transcendentals on both sides the two FP32 paths agree bit for bit
+    assert np.array_equal(a[2:-2, 2:-2, :3].astype(np.float64), b[2:-2, 2:-2, :3]), errs
     aux_g, aux_r = eng.aux(), ref.aux()
     np.testing.assert_allclose(aux_g[2:-2, 2:-2, 0], aux_r[2:-2, 2:-2, 0], rtol=1e-5, atol=1e-6)
 

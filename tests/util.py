@@ -9,16 +9,18 @@ def interior(a: np.ndarray) -> np.ndarray:
 
 
 def field_errors(gpu: np.ndarray, ref: np.ndarray, sea_level: float = 0.0) -> dict:
-    """Per-field max abs difference and the reference's max magnitude over interior cells.
-
-    Fields: eta = w - sea level, hu, hv."""
+    """Per-field max abs difference over interior cells, with the scale it is judged against:
+    max |eta| for eta = w - sea level, and the momentum scale max(|hu|, |hv|) for hu and hv
+    (in a one-dimensional run hv is rounding noise, so its own maximum is no scale)."""
     g = interior(np.asarray(gpu, dtype=np.float64))
     r = interior(np.asarray(ref, dtype=np.float64))
+    mom = float(max(np.max(np.abs(r[..., 1])), np.max(np.abs(r[..., 2]))))
     out = {}
     for k, name in enumerate(("eta", "hu", "hv")):
         a = g[..., k] - (sea_level if k == 0 else 0.0)
         b = r[..., k] - (sea_level if k == 0 else 0.0)
-        out[name] = (float(np.max(np.abs(a - b))), float(np.max(np.abs(b))))
+        scale = float(np.max(np.abs(b))) if k == 0 else mom
+        out[name] = (float(np.max(np.abs(a - b))), scale)
     return out
 
 
