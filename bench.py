@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--form", default="mixed", choices=["mixed", "fused"])
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--no-plain", action="store_true", help="skip the per-domain plain FP32 comparison")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="0 skips the CPU baseline")
+    ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA graphs (profiling)")
     return ap.parse_args()
 
 
@@ -174,7 +175,7 @@ def main():
     batch = cb.Batch([(m[0], m[1]) for m in members], args.form)
     stream = torch.cuda.Stream()
     batch.set_stream(stream.cuda_stream)
-    batch.use_graph(True)
+    batch.use_graph(not args.no_graph)
     cells = batch.cells
     N = members[0][0].correction_steps
     with torch.cuda.stream(stream):
@@ -235,7 +236,7 @@ def main():
     torch.cuda.synchronize()
     kt = batch.kernel_times()
     batch.kernel_timing(False)
-    batch.use_graph(True)
+    batch.use_graph(not args.no_graph)
     st_ms, st_n = kt.get("fused_stencil", (0.0, 0))
     comp = 8.0 if args.form == "mixed" else 0.0
     stencil_bytes_cell = ((112 + comp) + N * (136 + comp)) / (1 + N)  # average over pass kinds
@@ -278,7 +279,7 @@ def main():
 
     # ---- CPU baseline (rank 0, N=1) ---------------------------------------------------------
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
         rate, cores, sample = cpu_sample(args.cpu_seconds, members)
         cpu = {"value": rate / 1e9, "unit": "Gcell-steps/s", "cores": cores, "kind": "port", "sample": sample}
 
@@ -290,7 +291,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload, "form": args.form, "members_per_gpu": len(members),
-                       "cells_per_gpu": cells, "correction_steps": N, "cuda_graph": True,
+                       "cells_per_gpu": cells, "correction_steps": N, "cuda_graph": not args.no_graph,
                        "l2": "working set (%.1f GB) larger than L2 (126 MB); no flush" % (
                            cells * 4 * (42 + (9 if args.form == "mixed" else 0)) / 1e9),
                        "parallelism": f"ensemble sharded by domain over {world} GPU(s)"},

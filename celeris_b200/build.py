@@ -26,7 +26,7 @@ UNITS = [
     ("setup.cpp", []),
     ("capi.cpp", []),
     ("plain.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
-    ("fused.cu", ["-prec-div=true", "-prec-sqrt=true"]),
+    ("fused.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
 ]
 HEADERS = ["celeris_internal.hpp", "engine_iface.hpp", "scheme.hpp", "device_math.cuh", "batch.hpp"]
 

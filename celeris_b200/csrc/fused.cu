@@ -2,11 +2,11 @@
 //
 // One pass (predictor, corrector or Euler) of every domain in a batch is three kernels plus the
 // boundary kernels, each launched once for all domains over a cross-domain work list:
-//   k_stencil  : Pass1 (minmod reconstruction, positivity fix, desingularised velocities) +
+//   k_march    : Pass1 (minmod reconstruction, positivity fix, desingularised velocities) +
 //                Pass2 (Kurganov-Petrova central-upwind fluxes) + Pass3Predictor (flux
 //                divergence, bed slope, friction, Madsen-Sorensen dispersion, F*/G*, AB3/AM4
-//                combination) + white-water/inundation aux + the GetStats reduction, over a
-//                32x16 tile staged in shared memory with a 2-cell halo.  It writes the new w
+//                combination) + white-water/inundation aux + the GetStats reduction, marching
+//                down 126-column strips with a 6-row shared-memory ring.  It writes the new w
 //                and, for hu and hv, the right-hand side of the implicit dispersive system in
 //                increment form: M dhu = r, hu_new = hu_base + dhu.
 //   k_rows / k_cols : the tridiagonal solves along x (one CTA per row) and y (one CTA per band
@@ -40,9 +40,6 @@ namespace cel {
 namespace {
 
 constexpr int TX = 32, TY = 16;
-constexpr int SW = TX + 4, SH = TY + 4;      // state tile with a 2-cell halo
-constexpr int FW = TX + 2, FH = TY + 2;      // face tile (1-cell halo)
-constexpr int NT1 = TX * TY;                 // stencil threads (one output cell each)
 constexpr int NTR = 256;                     // row-solver threads
 constexpr int NTC = 512;                     // column solver threads: CWT columns x (512/CWT) chunks
 constexpr int STATS_N = 12;
@@ -133,234 +130,292 @@ __device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h,
 }
 
 // ---------------------------------------------------------------------------------------------
-// k_stencil: Pass1 + Pass2 + Pass3 + aux + stats for one 32x16 tile per iteration.
+// k_march: Pass1 + Pass2 + Pass3 + aux + GetStats, marching down a strip of MO = 126 output
+// columns for MH rows.  Thread i owns column x0 - 1 + i (128 threads: the 126 output columns
+// plus one halo column each side for the faces the fluxes need).  State and bottom rows sit in
+// a 6-row shared-memory ring (rows t-2 .. t+3 around the output row t); faces travel along y in
+// registers (the north face of row t becomes the south side of the y flux), east/west faces and
+// the x fluxes are exchanged through shared memory.  Two barriers per row.
 // ---------------------------------------------------------------------------------------------
-template <bool MIXED>
-__global__ void __launch_bounds__(NT1) k_stencil(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
-                                                 int ntiles, PassArgs pa) {
-    extern __shared__ float smem[];
-    float* sW = smem;
-    float* sHU = sW + SH * SW;
-    float* sHV = sHU + SH * SW;
-    float* sBA = sHV + SH * SW;
-    float* sBX = sBA + SH * SW;
-    float* sBY = sBX + SH * SW;
-    float* fh = sBY + SH * SW;        // [4][FH*FW]  N, E, S, W
-    float* fu = fh + 4 * FH * FW;
-    float* fv = fu + 4 * FH * FW;
-    float* xf = fv + 4 * FH * FW;     // [3][TY*(TX+1)]
-    float* yf = xf + 3 * TY * (TX + 1); // [3][(TY+1)*TX]
-    __shared__ double red[NT1 / 32][STATS_N];
-    const int tid = threadIdx.x;
-    constexpr int FA = FH * FW;
+constexpr int MW = 128;          // threads = columns with faces per row
+constexpr int MO = MW - 2;       // output columns per strip
+constexpr int MH = 64;           // rows per strip
+constexpr int RING = 6;
+constexpr int RW = MW + 2;       // ring row width: columns x0-2 .. x0+MO+1
 
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int4 tl = tiles[t];
+__device__ __forceinline__ int ring_slot(int row) { return ((row % RING) + RING) % RING; }
+
+struct Face { float hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, msd; };
+
+// Pass1 at one cell from ring rows: w/hu/hv/BX/BY at (rc +- 1, row +- 1).
+__device__ __forceinline__ void faces_at(const float (*rg)[RING][RW], int sm, int s0, int sp, int rc,
+                                         const SimConsts& c, Face& f) {
+    // rg[field][slot][col]; field 0 w, 1 hu, 2 hv, 3 BA, 4 BX, 5 BY
+    const float wc = rg[0][s0][rc], wl = rg[0][s0][rc - 1], wr = rg[0][s0][rc + 1];
+    const float wd = rg[0][sm][rc], wu = rg[0][sp][rc];
+    const float BN = rg[5][s0][rc], BE = rg[4][s0][rc], BS = rg[5][sm][rc], BW = rg[4][s0][rc - 1];
+    float wN, wE, wS, wW, huN, huE, huS, huW, hvN, hvE, hvS, hvW, sd1, sd2;
+    reconstruct_sd(c.two_theta, wl, wc, wr, wW, wE, sd1);
+    reconstruct_sd(c.two_theta, wd, wc, wu, wS, wN, sd2);
+    reconstruct(c.two_theta, rg[1][s0][rc - 1], rg[1][s0][rc], rg[1][s0][rc + 1], huW, huE);
+    reconstruct(c.two_theta, rg[1][sm][rc], rg[1][s0][rc], rg[1][sp][rc], huS, huN);
+    reconstruct(c.two_theta, rg[2][s0][rc - 1], rg[2][s0][rc], rg[2][s0][rc + 1], hvW, hvE);
+    reconstruct(c.two_theta, rg[2][sm][rc], rg[2][s0][rc], rg[2][sp][rc], hvS, hvN);
+    correct_w(BW, BE, wc, wW, wE);
+    correct_w(BS, BN, wc, wS, wN);
+    f.hN = wN - BN; f.hE = wE - BE; f.hS = wS - BS; f.hW = wW - BW;
+    float q;
+    q = div_by_h(f.hN, c.epsilon); f.uN = q * huN; f.vN = q * hvN;
+    q = div_by_h(f.hE, c.epsilon); f.uE = q * huE; f.vE = q * hvE;
+    q = div_by_h(f.hS, c.epsilon); f.uS = q * huS; f.vS = q * hvS;
+    q = div_by_h(f.hW, c.epsilon); f.uW = q * huW; f.vW = q * hvW;
+    f.msd = fmaxf(sd1 * c.one_over_dx, sd2 * c.one_over_dy);
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(MW, 4) k_march(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
+                                                 int ntiles, PassArgs pa) {
+    __shared__ float rg[6][RING][RW];
+    __shared__ float fEW[2][6][MW];     // [row parity][hE,uE,vE,hW,uW,vW][thread]
+    __shared__ float xb[2][3][MW];      // [row parity][component][thread] x flux at the thread's east face
+    __shared__ double red[MW / 32][STATS_N];
+    const int tid = threadIdx.x;
+
+    for (int it = blockIdx.x; it < ntiles; it += gridDim.x) {
+        const int4 tl = tiles[it];
         const MemberDev& M = mems[tl.x];
         const SimConsts c = M.c;
         const int P = M.P, NX = c.NX, NY = c.NY, nx = c.nx, ny = c.ny;
         const int x0 = tl.y, y0 = tl.z;
+        const int xc = x0 - 1 + tid;          // this thread's column
+        const int rc = tid + 1;               // its ring column
+        const int yend = min(y0 + MH, ny + 2);
+        const bool out_col = tid >= 1 && tid <= MO && xc < nx + 2;
         const float* Win = M.S[pa.in][0];
         const float* HUin = M.S[pa.in][1];
         const float* HVin = M.S[pa.in][2];
-        __syncthreads();  // smem reuse across tiles
-        // ---- load the state / bottom tile (2-cell halo; outside the texture reads zero) ----
-        for (int k = tid; k < SH * SW; k += NT1) {
-            const int ly = k / SW, lx = k - ly * SW;
-            const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
-            const bool ok = gx >= 0 && gx < NX && gy >= 0 && gy < NY;
-            const size_t gi = size_t(gy) * P + gx;
-            sW[k] = ok ? Win[gi] : 0.f;
-            sHU[k] = ok ? HUin[gi] : 0.f;
-            sHV[k] = ok ? HVin[gi] : 0.f;
-            sBA[k] = ok ? M.BA[gi] : 0.f;
-            sBX[k] = ok ? M.BX[gi] : 0.f;
-            sBY[k] = ok ? M.BY[gi] : 0.f;
-        }
-        __syncthreads();
-        // ---- Pass1: faces over [x0-1, x0+TX+1) x [y0-1, y0+TY+1), with the aux update ----
         const float dtm = *M.dtp;
         const float decay = t_pow(fabsf(c.whitewater_decay_rate), dtm);
-        for (int k = tid; k < FA; k += NT1) {
-            const int fy = k / FW, fx = k - fy * FW;
-            const int si = (fy + 1) * SW + (fx + 1);
-            const float wc = sW[si], wl = sW[si - 1], wr = sW[si + 1], wd = sW[si - SW], wu = sW[si + SW];
-            const float BN = sBY[si], BE = sBX[si], BS = sBY[si - SW], BW = sBX[si - 1];
-            float wN, wE, wS, wW, huN, huE, huS, huW, hvN, hvE, hvS, hvW, sd1, sd2;
-            reconstruct_sd(c.two_theta, wl, wc, wr, wW, wE, sd1);
-            reconstruct_sd(c.two_theta, wd, wc, wu, wS, wN, sd2);
-            reconstruct(c.two_theta, sHU[si - 1], sHU[si], sHU[si + 1], huW, huE);
-            reconstruct(c.two_theta, sHU[si - SW], sHU[si], sHU[si + SW], huS, huN);
-            reconstruct(c.two_theta, sHV[si - 1], sHV[si], sHV[si + 1], hvW, hvE);
-            reconstruct(c.two_theta, sHV[si - SW], sHV[si], sHV[si + SW], hvS, hvN);
-            correct_w(BW, BE, wc, wW, wE);
-            correct_w(BS, BN, wc, wS, wN);
-            const float hN = wN - BN, hE = wE - BE, hS = wS - BS, hW = wW - BW;
-            float q;
-            q = div_by_h(hN, c.epsilon); fh[0 * FA + k] = hN; fu[0 * FA + k] = q * huN; fv[0 * FA + k] = q * hvN;
-            q = div_by_h(hE, c.epsilon); fh[1 * FA + k] = hE; fu[1 * FA + k] = q * huE; fv[1 * FA + k] = q * hvE;
-            q = div_by_h(hS, c.epsilon); fh[2 * FA + k] = hS; fu[2 * FA + k] = q * huS; fv[2 * FA + k] = q * hvS;
-            q = div_by_h(hW, c.epsilon); fh[3 * FA + k] = hW; fu[3 * FA + k] = q * huW; fv[3 * FA + k] = q * hvW;
-            // aux (Pass1 then Pass2 of txAuxiliary) for cells in [1,nx+2)x[1,ny+2) owned by this tile
-            const int gx = x0 - 1 + fx, gy = y0 - 1 + fy;
-            if (gx >= 1 && gx < nx + 2 && gy >= 1 && gy < ny + 2) {
-                const int cx = gx < 2 ? 2 : gx, cy = gy < 2 ? 2 : gy;
-                if (cx >= x0 && cx < x0 + TX && cy >= y0 && cy < y0 + TY) {
-                    const size_t gi = size_t(gy) * P + gx;
-                    const float msd = t_atan(fmaxf(sd1 * c.one_over_dx, sd2 * c.one_over_dy));
-                    const float md = fmaxf((hN + hE + hS + hW) / 4.0f, M.AUX[0][gi]);
-                    float bw = M.AUX[1][gi];
-                    if (msd > c.dissipation_threshold) bw = 1.0f;
-                    M.AUX[0][gi] = md;
-                    M.AUX[1][gi] = bw * decay;
-                }
+        const bool corr = pa.scheme == CEL_SCHEME_CORRECTOR;
+        const bool euler = pa.scheme == CEL_SCHEME_EULER;
+
+        auto load_row = [&](int gy) {
+            const int sl = ring_slot(gy);
+            for (int k = tid; k < RW; k += MW) {
+                const int gx = x0 - 2 + k;
+                const bool ok = gx >= 0 && gx < NX && gy >= 0 && gy < NY;
+                const size_t gi = size_t(gy) * P + gx;
+                rg[0][sl][k] = ok ? Win[gi] : 0.f;
+                rg[1][sl][k] = ok ? HUin[gi] : 0.f;
+                rg[2][sl][k] = ok ? HVin[gi] : 0.f;
+                rg[3][sl][k] = ok ? M.BA[gi] : 0.f;
+                rg[4][sl][k] = ok ? M.BX[gi] : 0.f;
+                rg[5][sl][k] = ok ? M.BY[gi] : 0.f;
             }
-        }
-        __syncthreads();
-        // ---- Pass2: x fluxes at [x0-1, x0+TX) x [y0, y0+TY), y fluxes at [x0, x0+TX) x [y0-1, y0+TY) ----
-        {
-            const float g = c.g, hg = c.half_g;
-            constexpr int NXF = TY * (TX + 1), NYF = (TY + 1) * TX;
-            for (int k = tid; k < NXF + NYF; k += NT1) {
-                if (k < NXF) {
-                    const int ly = k / (TX + 1), lxx = k - ly * (TX + 1);
-                    const int fl = (ly + 1) * FW + lxx;   // face cell west of the face
-                    const float hE = fh[1 * FA + fl], uE = fu[1 * FA + fl], vE = fv[1 * FA + fl];
-                    const float hWe = fh[3 * FA + fl + 1], uWe = fu[3 * FA + fl + 1], vWe = fv[3 * FA + fl + 1];
-                    const float cE = sqrtf(g * hE), cW = sqrtf(g * hWe);
-                    const float ap = fmaxf(fmaxf(uE + cE, uWe + cW), 0.f);
-                    const float am = fminf(fminf(uE - cE, uWe - cW), 0.f);
-                    xf[0 * NXF + k] = numflux(ap, am, hWe * uWe, hE * uE, hWe - hE);
-                    xf[1 * NXF + k] = numflux(ap, am, hWe * (uWe * uWe + hg * hWe), hE * (uE * uE + hg * hE),
-                                              hWe * uWe - hE * uE);
-                    xf[2 * NXF + k] = numflux(ap, am, hWe * uWe * vWe, hE * uE * vE, hWe * vWe - hE * vE);
-                } else {
-                    const int kk = k - NXF;
-                    const int ly = kk / TX, lx = kk - ly * TX;
-                    const int fl = ly * FW + lx + 1;      // face cell south of the face
-                    const float hN = fh[0 * FA + fl], uN = fu[0 * FA + fl], vN = fv[0 * FA + fl];
-                    const float hSn = fh[2 * FA + fl + FW], uSn = fu[2 * FA + fl + FW], vSn = fv[2 * FA + fl + FW];
-                    const float cN = sqrtf(g * hN), cS = sqrtf(g * hSn);
-                    const float bp = fmaxf(fmaxf(vN + cN, vSn + cS), 0.f);
-                    const float bm = fminf(fminf(vN - cN, vSn - cS), 0.f);
-                    yf[0 * NYF + kk] = numflux(bp, bm, hSn * vSn, hN * vN, hSn - hN);
-                    yf[1 * NYF + kk] = numflux(bp, bm, hSn * uSn * vSn, hN * uN * vN, hSn * uSn - hN * uN);
-                    yf[2 * NYF + kk] = numflux(bp, bm, hSn * (vSn * vSn + hg * hSn), hN * (vN * vN + hg * hN),
-                                               hSn * vSn - hN * vN);
-                }
-            }
-        }
-        __syncthreads();
-        // ---- zero the ghost ring of the output state (engine.cpp:1007) ----
-        for (int k = tid; k < SH * SW; k += NT1) {
-            const int ly = k / SW, lx = k - ly * SW;
-            const int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
-            if (gx < 0 || gx >= NX || gy < 0 || gy >= NY) continue;
-            if (gx >= 2 && gx < nx + 2 && gy >= 2 && gy < ny + 2) continue;
-            const int cx = min(max(gx, 2), nx + 1), cy = min(max(gy, 2), ny + 1);
-            if (cx < x0 || cx >= x0 + TX || cy < y0 || cy >= y0 + TY) continue;
-            const size_t gi = size_t(gy) * P + gx;
-            M.S[pa.out][0][gi] = 0.f; M.S[pa.out][1][gi] = 0.f; M.S[pa.out][2][gi] = 0.f;
-            if (MIXED) { M.L[pa.out][0][gi] = 0.f; M.L[pa.out][1][gi] = 0.f; M.L[pa.out][2][gi] = 0.f; }
-        }
-        // ---- Pass3: one interior cell per thread ----
-        const int lx = tid % TX, ly = tid / TX;
-        const int gx = x0 + lx, gy = y0 + ly;
-        const bool valid = gx < nx + 2 && gy < ny + 2;
-        const int si = (ly + 2) * SW + (lx + 2);
-        const size_t gi = size_t(gy) * P + gx;
-        float sh_h = 0.f, sh_B = 0.f, sh_hu = 0.f, sh_hv = 0.f, sh_u = 0.f, sh_v = 0.f, sh_q = 0.f, sh_c = 0.f;
+        };
+
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        float mx[4] = {0.f, 0.f, 0.f, 0.f};
         bool bad = false;
-        if (valid) {
-            constexpr int NXF = TY * (TX + 1), NYF = (TY + 1) * TX;
-            const float sl = c.sea_level;
-            const float wc = sW[si], huc = sHU[si], hvc = sHV[si];
-            const float BAh = sBA[si], BXh = sBX[si], BYh = sBY[si];
-            const float BXw = sBX[si - 1], BYs = sBY[si - SW];
-            const float h = fmaxf(0.f, wc - BAh);
-            const float dh = fmaxf(0.f, sl - BAh), d2 = dh * dh, d3 = d2 * dh;
-            const float dl = fmaxf(0.f, sl - sBA[si - 1]), dr = fmaxf(0.f, sl - sBA[si + 1]);
-            const float ddn = fmaxf(0.f, sl - sBA[si - SW]), du = fmaxf(0.f, sl - sBA[si + SW]);
-            const float dll = fmaxf(0.f, sl - sBA[si - 2]), drr = fmaxf(0.f, sl - sBA[si + 2]);
-            const float ddd = fmaxf(0.f, sl - sBA[si - 2 * SW]), duu = fmaxf(0.f, sl - sBA[si + 2 * SW]);
-            const float e0 = wc - sl;
-            const float el = sW[si - 1] - sl, er = sW[si + 1] - sl, ed = sW[si - SW] - sl, eu = sW[si + SW] - sl;
-            const float ell = sW[si - 2] - sl, err = sW[si + 2] - sl, edd = sW[si - 2 * SW] - sl, euu = sW[si + 2 * SW] - sl;
-            const float eul = sW[si + SW - 1] - sl, eur = sW[si + SW + 1] - sl;
-            const float edl = sW[si - SW - 1] - sl, edr = sW[si - SW + 1] - sl;
-            const int xk = ly * (TX + 1) + lx;
-            const int yk = ly * TX + lx;
-            const float odx = c.one_over_dx, ody = c.one_over_dy;
-            const float od2x = odx * odx, od3x = od2x * odx, od2y = ody * ody, od3y = od2y * ody;
-            const float ddx = (-drr + 8 * dr - 8 * dl + dll) * odx / 12.0f;
-            const float ddy = (-duu + 8 * du - 8 * ddn + ddd) * ody / 12.0f;
-            const float exy = (0.25f * odx * ody * (eur - edr - eul + edl));
-            const float exx = od2x * (er - 2 * e0 + el);
-            const float eyy = od2y * (eu - 2 * e0 + ed);
-            const float Bg = c.Bcoef_g;
-            const float P1x = Bg * (d3) * ((err - 2 * er + 2 * el - ell) * (0.5f * od3x) +
-                                           (eur - eul - 2 * er + 2 * el + edr - edl) * (0.5f * odx * od2y));
-            const float P2x = Bg * (d2) * (ddx * (2 * exx + eyy) + ddy * exy);
-            const float P1y = Bg * (d3) * ((euu - 2 * eu + 2 * ed - edd) * (0.5f * od3y) +
-                                           (eur + eul - 2 * eu + 2 * ed - edr - edl) * (0.5f * ody * od2x));
-            const float P2y = Bg * (d2) * (ddy * (exx + 2 * eyy) + ddx * exy);
-            const float fr = friction_calc(huc, hvc, h, c.friction, c.is_manning, c.g, c.epsilon);
-            const float s1 = -c.g_over_dx * h * (BXh - BXw) - huc * fr + (P1x + P2x);
-            const float s2 = -c.g_over_dy * h * (BYh - BYs) - hvc * fr + (P1y + P2y);
-            const float f0 = (xf[0 * NXF + xk] - xf[0 * NXF + xk + 1]) * odx + (yf[0 * NYF + yk] - yf[0 * NYF + yk + TX]) * ody;
-            const float f1 = (xf[1 * NXF + xk] - xf[1 * NXF + xk + 1]) * odx + (yf[1 * NYF + yk] - yf[1 * NYF + yk + TX]) * ody + s1;
-            const float f2 = (xf[2 * NXF + xk] - xf[2 * NXF + xk + 1]) * odx + (yf[2 * NYF + yk] - yf[2 * NYF + yk + TX]) * ody + s2;
-            const float sixth = 1.0f / 6.0f;
-            const float Fs = (sixth * dh * (ddx * ((ody / 2.0f) * (sHV[si + SW] - sHV[si - SW])) +
-                                            (ddy * ((odx / 2.0f) * (sHV[si + 1] - sHV[si - 1])))));
-            const float Gs = (sixth * dh * (ddx * ((ody / 2.0f) * (sHU[si + SW] - sHU[si - SW])) +
-                                            (ddy * ((odx / 2.0f) * (sHU[si + 1] - sHU[si - 1])))));
-            const float dt = dtm;
-            float dw, rhu, rhv;
-            float wbase = wc, wbase_lo = 0.f;
-            if (pa.scheme == CEL_SCHEME_EULER) {
-                dw = dt * f0;
-                rhu = dt * f1;
-                rhv = dt * f2;
-            } else {
-                const float o0 = M.G[pa.og][0][gi], o1 = M.G[pa.og][1][gi], o2 = M.G[pa.og][2][gi];
-                const float q0 = M.G[pa.oog][0][gi], q1 = M.G[pa.oog][1][gi], q2 = M.G[pa.oog][2][gi];
-                const float fo0 = M.F[pa.og][0][gi], fo1 = M.F[pa.og][1][gi];
-                const float foo0 = M.F[pa.oog][0][gi], foo1 = M.F[pa.oog][1][gi];
-                if (pa.scheme == CEL_SCHEME_PREDICTOR) {
+        float nh = 0.f, nu = 0.f, nv = 0.f;   // north face of the previous row (this column)
+        float ypv0 = 0.f, ypv1 = 0.f, ypv2 = 0.f;  // y flux below the current row
+
+        __syncthreads();  // the previous strip is done with shared memory
+        load_row(y0 - 2);
+        load_row(y0 - 1);
+        for (int t = y0 - 2; t < yend; ++t) {
+            load_row(t + 2);
+            // per-cell inputs of Pass3 at (xc, t), issued before the face work
+            const bool do3 = t >= y0 && out_col;
+            const size_t gi = size_t(t < 0 ? 0 : t) * P + (xc < 0 ? 0 : xc);
+            float o0 = 0, o1 = 0, o2 = 0, q0 = 0, q1 = 0, q2 = 0, fo0 = 0, fo1 = 0, foo0 = 0, foo1 = 0;
+            float p0 = 0, p1 = 0, p2 = 0, fp0 = 0, fp1 = 0, wcur = 0, wlo = 0;
+            if (do3 && !euler) {
+                o0 = M.G[pa.og][0][gi]; o1 = M.G[pa.og][1][gi]; o2 = M.G[pa.og][2][gi];
+                q0 = M.G[pa.oog][0][gi]; q1 = M.G[pa.oog][1][gi]; q2 = M.G[pa.oog][2][gi];
+                fo0 = M.F[pa.og][0][gi]; fo1 = M.F[pa.og][1][gi];
+                foo0 = M.F[pa.oog][0][gi]; foo1 = M.F[pa.oog][1][gi];
+                if (corr) {
+                    p0 = M.G[pa.pred][0][gi]; p1 = M.G[pa.pred][1][gi]; p2 = M.G[pa.pred][2][gi];
+                    fp0 = M.F[pa.pred][0][gi]; fp1 = M.F[pa.pred][1][gi];
+                    wcur = M.S[pa.cur][0][gi];
+                }
+            }
+            if (MIXED && do3) wlo = M.L[corr ? pa.cur : pa.in][0][gi];
+            __syncthreads();
+            // ---- faces of row t+1 (Pass1), aux update of that row, y flux between rows t and t+1 ----
+            const int s_m = ring_slot(t), s_0 = ring_slot(t + 1), s_p = ring_slot(t + 2);
+            Face f;
+            faces_at(rg, s_m, s_0, s_p, rc, c, f);
+            const int par1 = (t + 1) & 1;
+            fEW[par1][0][tid] = f.hE; fEW[par1][1][tid] = f.uE; fEW[par1][2][tid] = f.vE;
+            fEW[par1][3][tid] = f.hW; fEW[par1][4][tid] = f.uW; fEW[par1][5][tid] = f.vW;
+            {
+                const int gy = t + 1;
+                if (xc >= 1 && xc < nx + 2 && gy >= 1 && gy < ny + 2) {
+                    const int cx = xc < 2 ? 2 : xc, cy = gy < 2 ? 2 : gy;
+                    if (cx >= x0 && cx < x0 + MO && cy >= y0 && cy < y0 + MH) {
+                        const size_t ai = size_t(gy) * P + xc;
+                        const float msd = t_atan(f.msd);
+                        const float md = fmaxf((f.hN + f.hE + f.hS + f.hW) / 4.0f, M.AUX[0][ai]);
+                        float bw = M.AUX[1][ai];
+                        if (msd > c.dissipation_threshold) bw = 1.0f;
+                        M.AUX[0][ai] = md;
+                        M.AUX[1][ai] = bw * decay;
+                    }
+                }
+            }
+            const float g = c.g, hg = c.half_g;
+            float yf0 = 0.f, yf1 = 0.f, yf2 = 0.f;
+            {   // y flux at the north face of row t: north face of row t (carried) vs south face of row t+1
+                const float hN = nh, uN = nu, vN = nv;
+                const float hSn = f.hS, uSn = f.uS, vSn = f.vS;
+                const float cN = sqrtf(g * hN), cS = sqrtf(g * hSn);
+                const float bp = fmaxf(fmaxf(vN + cN, vSn + cS), 0.f);
+                const float bm = fminf(fminf(vN - cN, vSn - cS), 0.f);
+                yf0 = numflux(bp, bm, hSn * vSn, hN * vN, hSn - hN);
+                yf1 = numflux(bp, bm, hSn * uSn * vSn, hN * uN * vN, hSn * uSn - hN * uN);
+                yf2 = numflux(bp, bm, hSn * (vSn * vSn + hg * hSn), hN * (vN * vN + hg * hN), hSn * vSn - hN * vN);
+            }
+            // ---- x flux at the east face of (xc, t): faces of row t from the previous step ----
+            const int par = t & 1;
+            if (t >= y0 && tid < MW - 1) {
+                const float hE = fEW[par][0][tid], uE = fEW[par][1][tid], vE = fEW[par][2][tid];
+                const float hWe = fEW[par][3][tid + 1], uWe = fEW[par][4][tid + 1], vWe = fEW[par][5][tid + 1];
+                const float cE = sqrtf(g * hE), cW = sqrtf(g * hWe);
+                const float ap = fmaxf(fmaxf(uE + cE, uWe + cW), 0.f);
+                const float am = fminf(fminf(uE - cE, uWe - cW), 0.f);
+                xb[par][0][tid] = numflux(ap, am, hWe * uWe, hE * uE, hWe - hE);
+                xb[par][1][tid] = numflux(ap, am, hWe * (uWe * uWe + hg * hWe), hE * (uE * uE + hg * hE), hWe * uWe - hE * uE);
+                xb[par][2][tid] = numflux(ap, am, hWe * uWe * vWe, hE * uE * vE, hWe * vWe - hE * vE);
+            }
+            __syncthreads();
+            // ---- Pass3 at (xc, t) ----
+            if (do3) {
+                const int r0 = ring_slot(t), rm = ring_slot(t - 1), rp = ring_slot(t + 1);
+                const int rmm = ring_slot(t - 2), rpp = ring_slot(t + 2);
+                const float sl = c.sea_level;
+                const float wc = rg[0][r0][rc], huc = rg[1][r0][rc], hvc = rg[2][r0][rc];
+                const float BAh = rg[3][r0][rc], BXh = rg[4][r0][rc], BYh = rg[5][r0][rc];
+                const float BXw = rg[4][r0][rc - 1], BYs = rg[5][rm][rc];
+                const float h = fmaxf(0.f, wc - BAh);
+                const float dh = fmaxf(0.f, sl - BAh), d2 = dh * dh, d3 = d2 * dh;
+                const float dl = fmaxf(0.f, sl - rg[3][r0][rc - 1]), dr = fmaxf(0.f, sl - rg[3][r0][rc + 1]);
+                const float ddn = fmaxf(0.f, sl - rg[3][rm][rc]), du = fmaxf(0.f, sl - rg[3][rp][rc]);
+                const float dll = fmaxf(0.f, sl - rg[3][r0][rc - 2]), drr = fmaxf(0.f, sl - rg[3][r0][rc + 2]);
+                const float ddd = fmaxf(0.f, sl - rg[3][rmm][rc]), duu = fmaxf(0.f, sl - rg[3][rpp][rc]);
+                const float e0 = wc - sl;
+                const float el = rg[0][r0][rc - 1] - sl, er = rg[0][r0][rc + 1] - sl;
+                const float ed = rg[0][rm][rc] - sl, eu = rg[0][rp][rc] - sl;
+                const float ell = rg[0][r0][rc - 2] - sl, err = rg[0][r0][rc + 2] - sl;
+                const float edd = rg[0][rmm][rc] - sl, euu = rg[0][rpp][rc] - sl;
+                const float eul = rg[0][rp][rc - 1] - sl, eur = rg[0][rp][rc + 1] - sl;
+                const float edl = rg[0][rm][rc - 1] - sl, edr = rg[0][rm][rc + 1] - sl;
+                const float odx = c.one_over_dx, ody = c.one_over_dy;
+                const float od2x = odx * odx, od3x = od2x * odx, od2y = ody * ody, od3y = od2y * ody;
+                const float ddx = (-drr + 8 * dr - 8 * dl + dll) * odx / 12.0f;
+                const float ddy = (-duu + 8 * du - 8 * ddn + ddd) * ody / 12.0f;
+                const float exy = (0.25f * odx * ody * (eur - edr - eul + edl));
+                const float exx = od2x * (er - 2 * e0 + el);
+                const float eyy = od2y * (eu - 2 * e0 + ed);
+                const float Bg = c.Bcoef_g;
+                const float P1x = Bg * (d3) * ((err - 2 * er + 2 * el - ell) * (0.5f * od3x) +
+                                               (eur - eul - 2 * er + 2 * el + edr - edl) * (0.5f * odx * od2y));
+                const float P2x = Bg * (d2) * (ddx * (2 * exx + eyy) + ddy * exy);
+                const float P1y = Bg * (d3) * ((euu - 2 * eu + 2 * ed - edd) * (0.5f * od3y) +
+                                               (eur + eul - 2 * eu + 2 * ed - edr - edl) * (0.5f * ody * od2x));
+                const float P2y = Bg * (d2) * (ddy * (exx + 2 * eyy) + ddx * exy);
+                const float fr = friction_calc(huc, hvc, h, c.friction, c.is_manning, c.g, c.epsilon);
+                const float s1 = -c.g_over_dx * h * (BXh - BXw) - huc * fr + (P1x + P2x);
+                const float s2 = -c.g_over_dy * h * (BYh - BYs) - hvc * fr + (P1y + P2y);
+                const float f0 = (xb[par][0][tid - 1] - xb[par][0][tid]) * odx + (ypv0 - yf0) * ody;
+                const float f1 = (xb[par][1][tid - 1] - xb[par][1][tid]) * odx + (ypv1 - yf1) * ody + s1;
+                const float f2 = (xb[par][2][tid - 1] - xb[par][2][tid]) * odx + (ypv2 - yf2) * ody + s2;
+                const float sixth = 1.0f / 6.0f;
+                const float Fs = (sixth * dh * (ddx * ((ody / 2.0f) * (rg[2][rp][rc] - rg[2][rm][rc])) +
+                                                (ddy * ((odx / 2.0f) * (rg[2][r0][rc + 1] - rg[2][r0][rc - 1])))));
+                const float Gs = (sixth * dh * (ddx * ((ody / 2.0f) * (rg[1][rp][rc] - rg[1][rm][rc])) +
+                                                (ddy * ((odx / 2.0f) * (rg[1][r0][rc + 1] - rg[1][r0][rc - 1])))));
+                const float dt = dtm;
+                float dw, rhu, rhv;
+                float wbase = wc;
+                if (euler) {
+                    dw = dt * f0; rhu = dt * f1; rhv = dt * f2;
+                } else if (!corr) {
                     dw = dt / 12.0f * (23.0f * f0 - 16.0f * o0 + 5.0f * q0);
                     rhu = dt / 12.0f * (23.0f * f1 - 16.0f * o1 + 5.0f * q1) + (2.0f * Fs - 3.0f * fo0 + foo0);
                     rhv = dt / 12.0f * (23.0f * f2 - 16.0f * o2 + 5.0f * q2) + (2.0f * Gs - 3.0f * fo1 + foo1);
-                } else {  // corrector, from CURRENT_STATE
-                    const float p0 = M.G[pa.pred][0][gi], p1 = M.G[pa.pred][1][gi], p2 = M.G[pa.pred][2][gi];
-                    const float fp0 = M.F[pa.pred][0][gi], fp1 = M.F[pa.pred][1][gi];
+                } else {
                     dw = dt / 24.0f * (9 * f0 + 19 * p0 - 5 * o0 + 1 * q0);
                     rhu = dt / 24.0f * (9 * f1 + 19 * p1 - 5 * o1 + 1 * q1) + Fs - fp0;
                     rhv = dt / 24.0f * (9 * f2 + 19 * p2 - 5 * o2 + 1 * q2) + Gs - fp1;
-                    wbase = M.S[pa.cur][0][gi];
-                    if (MIXED) wbase_lo = M.L[pa.cur][0][gi];
+                    wbase = wcur;
                 }
+                const size_t go = size_t(t) * P + xc;
+                float wn = wbase, wl = wlo;
+                if (MIXED) two_sum_add(wn, wl, dw);
+                else wn = wbase + dw;
+                M.S[pa.out][0][go] = wn;
+                if (MIXED) M.L[pa.out][0][go] = wl;
+                M.R[0][go] = rhu;
+                M.R[1][go] = rhv;
+                M.G[pa.scr][0][go] = f0; M.G[pa.scr][1][go] = f1; M.G[pa.scr][2][go] = f2;
+                M.F[pa.scr][0][go] = Fs; M.F[pa.scr][1][go] = Gs;
+                // GetStats (compute.hlsl:1319-1378) of the input state, FP64 accumulation
+                const float q = div_by_h(h, c.epsilon);
+                const float u = q * huc, v = q * hvc;
+                if (xc < 2 + 4 * (nx / 4) && t < 2 + 4 * (ny / 4)) {
+                    acc[0] += h; acc[1] += double(h * (BAh + 0.5f * h)); acc[2] += huc; acc[3] += hvc;
+                    acc[4] += double(huc * u + hvc * v);
+                    const float u2v2 = u * u + v * v;
+                    const float cc = sqrtf(c.g * h);
+                    mx[0] = fmaxf(mx[0], u2v2); mx[1] = fmaxf(mx[1], h);
+                    mx[2] = fmaxf(mx[2], fmaxf((fabsf(u) + cc) * c.one_over_dx, (fabsf(v) + cc) * c.one_over_dy));
+                    mx[3] = fmaxf(mx[3], u2v2 * q);
+                }
+                acc[5] += h;
+                bad = bad || !isfinite(wc) || !isfinite(huc) || !isfinite(hvc);
             }
-            if (MIXED && pa.scheme != CEL_SCHEME_CORRECTOR) wbase_lo = M.L[pa.in][0][gi];
-            float wn = wbase, wl = wbase_lo;
-            if (MIXED) two_sum_add(wn, wl, dw);
-            else wn = wbase + dw;
-            M.S[pa.out][0][gi] = wn;
-            if (MIXED) M.L[pa.out][0][gi] = wl;
-            M.R[0][gi] = rhu;
-            M.R[1][gi] = rhv;
-            M.G[pa.scr][0][gi] = f0; M.G[pa.scr][1][gi] = f1; M.G[pa.scr][2][gi] = f2;
-            M.F[pa.scr][0][gi] = Fs; M.F[pa.scr][1][gi] = Gs;
-            // GetStats quantities of the input state (compute.hlsl:1319-1378)
-            sh_h = h; sh_B = BAh; sh_hu = huc; sh_hv = hvc;
-            sh_q = div_by_h(h, c.epsilon);
-            sh_u = sh_q * huc; sh_v = sh_q * hvc;
-            sh_c = sqrtf(c.g * h);
-            bad = !isfinite(wc) || !isfinite(huc) || !isfinite(hvc);
+            ypv0 = yf0; ypv1 = yf1; ypv2 = yf2;
+            nh = f.hN; nu = f.uN; nv = f.vN;
         }
-        const bool in_block = valid && gx < 2 + 4 * (nx / 4) && gy < 2 + 4 * (ny / 4);
-        stats_reduce(M.stats, in_block, valid, sh_h, sh_B, sh_hu, sh_hv, sh_u, sh_v, sh_q, sh_c, c.one_over_dx,
-                     c.one_over_dy, bad, red);
+        // ---- zero the ghost ring of the output state next to this strip (engine.cpp:1007) ----
+        const bool west = x0 == 2, east = x0 + MO >= nx + 2, south = y0 == 2, north = y0 + MH >= ny + 2;
+        if (west || east || south || north) {
+            const int cx0 = west ? 0 : x0, cx1 = east ? NX : x0 + MO;
+            const int cy0 = south ? 0 : y0, cy1 = north ? NY : y0 + MH;
+            const int w = cx1 - cx0;
+            for (int k = tid; k < w * (cy1 - cy0); k += MW) {
+                const int gx = cx0 + k % w, gy = cy0 + k / w;
+                if (gx >= 2 && gx < nx + 2 && gy >= 2 && gy < ny + 2) continue;
+                const size_t go = size_t(gy) * P + gx;
+                M.S[pa.out][0][go] = 0.f; M.S[pa.out][1][go] = 0.f; M.S[pa.out][2][go] = 0.f;
+                if (MIXED) { M.L[pa.out][0][go] = 0.f; M.L[pa.out][1][go] = 0.f; M.L[pa.out][2][go] = 0.f; }
+            }
+        }
+        // ---- strip statistics -> member accumulators ----
+        {
+            double s[STATS_N];
+            for (int k = 0; k < 6; ++k) s[k] = acc[k];
+            for (int k = 0; k < 4; ++k) s[6 + k] = mx[k];
+            s[10] = bad ? 1.0 : 0.0;
+            s[11] = 0.0;
+            for (int off = 16; off; off >>= 1)
+                for (int k = 0; k < 11; ++k) {
+                    const double o = __shfl_down_sync(0xffffffffu, s[k], off);
+                    s[k] = (k >= 6) ? fmax(s[k], o) : s[k] + o;
+                }
+            const int lane = tid & 31, wid = tid >> 5;
+            if (lane == 0)
+                for (int k = 0; k < 11; ++k) red[wid][k] = s[k];
+            __syncthreads();
+            if (tid < 11) {
+                double a = red[0][tid];
+                for (int w = 1; w < MW / 32; ++w) a = (tid >= 6) ? fmax(a, red[w][tid]) : a + red[w][tid];
+                if (tid < 6) { if (a != 0.0) atomicAdd(M.stats + tid, a); }
+                else atomic_max_nonneg(M.stats + tid, a);
+            }
+        }
     }
 }
 
@@ -816,7 +871,8 @@ struct cel_batch {
     cel::KernelTimer tm;
     cel::Scheme sch;      // shared pass sequence (all members use the same correction count)
     cel::Idx ix;
-    int4* tiles = nullptr; int ntiles = 0;
+    int4* tiles = nullptr; int ntiles = 0;      // 32x16 tiles (statistics on demand)
+    int4* mtiles = nullptr; int nmtiles = 0;    // marching strips of the fused stencil
     int2* rows = nullptr; int nrows = 0;
     int2* bands = nullptr; int nbands = 0;
     int2* bitems[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -826,7 +882,7 @@ struct cel_batch {
     double* stats_now_all = nullptr;
     float* dt_table = nullptr;         // per-member time step on the device
     float* dt_host = nullptr;          // pinned mirror of dt_table
-    size_t smem_stencil = 0, smem_rows = 0, smem_cols = 0;
+    size_t smem_rows = 0, smem_cols = 0;
     int grid_stencil = 0, grid_rows = 0, grid_cols = 0;
     int sms = 148;
     bool use_graph = false;
@@ -882,9 +938,9 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     {
         TimedLaunch t(&b->tm, b->stream, "fused_stencil");
         if (b->mixed)
-            k_stencil<true><<<b->grid_stencil, NT1, b->smem_stencil, b->stream>>>(b->ddev, b->tiles, b->ntiles, pa);
+            k_march<true><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
         else
-            k_stencil<false><<<b->grid_stencil, NT1, b->smem_stencil, b->stream>>>(b->ddev, b->tiles, b->ntiles, pa);
+            k_march<false><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
     }
     {
         TimedLaunch t(&b->tm, b->stream, "tridiag_rows");
@@ -1048,7 +1104,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         if (cudaMallocHost(&p, size_t(n) * sizeof(float)) != cudaSuccess) { err = "cudaMallocHost failed"; return nullptr; }
         b->dt_host = static_cast<float*>(p);
     }
-    std::vector<int4> tiles;
+    std::vector<int4> tiles, mtiles;
     std::vector<int2> rows, bands, bitems[4];
     int max_nx = 0, max_ny = 0;
     for (int i = 0; i < n; ++i) {
@@ -1153,6 +1209,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         // work lists
         for (int y0 = 2; y0 < m.hs.ny + 2; y0 += TY)
             for (int x0 = 2; x0 < m.hs.nx + 2; x0 += TX) tiles.push_back(make_int4(i, x0, y0, 0));
+        for (int y0 = 2; y0 < m.hs.ny + 2; y0 += MH)
+            for (int x0 = 2; x0 < m.hs.nx + 2; x0 += MO) mtiles.push_back(make_int4(i, x0, y0, 0));
         for (int y = 2; y < m.hs.ny + 2; ++y) rows.push_back(make_int2(i, y));
     }
     // column bands: 16 columns per CTA, or 8 for tall domains (shared-memory capacity)
@@ -1177,7 +1235,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         *dst = static_cast<std::remove_reference_t<decltype(**dst)>*>(p);
         return CEL_OK;
     };
-    if (upload_list(tiles, &b->tiles, b->ntiles) || upload_list(rows, &b->rows, b->nrows) ||
+    if (upload_list(tiles, &b->tiles, b->ntiles) || upload_list(mtiles, &b->mtiles, b->nmtiles) ||
+        upload_list(rows, &b->rows, b->nrows) ||
         upload_list(bands, &b->bands, b->nbands))
         return nullptr;
     for (int s = 0; s < 4; ++s)
@@ -1188,12 +1247,9 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         b->ddev = static_cast<MemberDev*>(p);
         cudaMemcpy(b->ddev, b->hdev.data(), sizeof(MemberDev) * n, cudaMemcpyHostToDevice);
     }
-    b->smem_stencil = sizeof(float) * (6 * SH * SW + 12 * FH * FW + 3 * TY * (TX + 1) + 3 * (TY + 1) * TX);
     b->smem_rows = sizeof(float) * 3 * (pidx(max_nx) + 1);
     b->smem_cols = sizeof(float) * size_t(max_ny) * b->cw;
     if (b->smem_cols + 8192 > 227 * 1024 || b->smem_rows + 8192 > 227 * 1024) { err = "domain too large for the fused solver"; return nullptr; }
-    cudaFuncSetAttribute(k_stencil<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_stencil));
-    cudaFuncSetAttribute(k_stencil<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_stencil));
     cudaFuncSetAttribute(k_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
     cudaFuncSetAttribute(k_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
     cudaFuncSetAttribute(k_cols<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
@@ -1202,8 +1258,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     cudaFuncSetAttribute(k_cols<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
     {
         int occ = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stencil<false>, NT1, b->smem_stencil);
-        b->grid_stencil = std::max(1, std::min(b->ntiles, b->sms * std::max(occ, 1)));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_march<true>, MW, 0);
+        b->grid_stencil = std::max(1, std::min(b->nmtiles, b->sms * std::max(occ, 1)));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rows<false>, NTR, b->smem_rows);
         b->grid_rows = std::max(1, std::min(b->nrows, b->sms * std::max(occ, 1) * 4));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cols<false, 16>, NTC, b->smem_cols);
