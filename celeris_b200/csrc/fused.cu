@@ -20,7 +20,9 @@
 // CEL_FORM_MIXED additionally keeps a compensation (low) word for w, hu and hv and adds every
 // increment with a two-sum, evaluates the wave-maker phase omega*t in FP64 from an FP64 clock,
 // and reduces mass/energy in FP64.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -50,6 +52,10 @@ constexpr int STATS_N = 12;
 struct MemberDev {
     SimConsts c;
     int P;                  // plane pitch in floats
+    float* base;            // first plane; plane k starts at base + k * plane
+    unsigned long long plane;
+    const CUtensorMap* tmaps;  // 2D row maps: state [buffer*3 + field], then BA, BX, BY
+    float tan_thr;          // tan(dissipation threshold): atan(x) > thr  <=>  x > tan(thr)
     const float* dtp;       // this member's time step (device table, host-updatable)
     float* S[3][3];         // state buffers [buffer][w, hu, hv]
     float* L[3][3];         // compensation words (mixed form)
@@ -140,15 +146,75 @@ __device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h,
 constexpr int MW = 128;          // threads = columns with faces per row
 constexpr int MO = MW - 2;       // output columns per strip
 constexpr int MH = 64;           // rows per strip
-constexpr int RING = 6;
-constexpr int RW = MW + 2;       // ring row width: columns x0-2 .. x0+MO+1
+constexpr int RING = 7;          // state / bottom rows resident in shared memory (PREFETCH + 5)
+constexpr int RBOX = 136;        // TMA box width in floats (covers columns x0-2 .. x0+127)
+constexpr int RSTR = 160;        // ring row stride in floats (640 B, a multiple of 128 B)
+constexpr unsigned ROW_BYTES = 6u * RBOX * 4u;
+constexpr int PREFETCH = 2;      // rows requested ahead of the row being consumed
 
-__device__ __forceinline__ int ring_slot(int row) { return ((row % RING) + RING) % RING; }
+// ---- TMA and mbarrier helpers (inline PTX; single-CTA, no multicast) -----------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after a fixed number of polls and reports false (the caller flags the
+// error and carries on with whatever the buffer holds, so no thread can hang on it).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (int k = 0; k < (1 << 22); ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_row(float* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// ---- fast single-precision helpers of the fused forms (same formulas, fewer instructions) ----
+__device__ __forceinline__ float div_by_h_fast(float h, float eps) {
+    const float h2 = h * h, h4 = h2 * h2;
+    return 1.41421354f * h * rsqrtf(h4 + fmaxf(h4, eps));
+}
+// NumericalFlux for the three components of one face, sharing the reciprocal of a+ - a-
+__device__ __forceinline__ void numflux3(float ap, float am, const float Fp[3], const float Fm[3], const float dU[3],
+                                         float out[3]) {
+    const float den = ap - am;
+    const float inv = den != 0.f ? __frcp_rn(den) : 0.f;
+    const float apam = ap * am;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = (ap * Fm[k] - am * Fp[k] + apam * dU[k]) * inv;
+}
+__device__ __forceinline__ float friction_fast(float hu, float hv, float h, float friction, int manning, float g,
+                                              float eps) {
+    const float h2 = h * h, h4 = h2 * h2;
+    const float dbh = 1.41421354f * h * rsqrtf(h4 + fmaxf(h4, eps));
+    float f = friction;
+    if (manning == 1) f = g * friction * friction * exp2f(0.3333f * __log2f(fabsf(dbh)));
+    return f * sqrtf(hu * hu + hv * hv) * dbh * dbh;
+}
 
 struct Face { float hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, msd; };
 
 // Pass1 at one cell from ring rows: w/hu/hv/BX/BY at (rc +- 1, row +- 1).
-__device__ __forceinline__ void faces_at(const float (*rg)[RING][RW], int sm, int s0, int sp, int rc,
+__device__ __forceinline__ void faces_at(const float (*rg)[RING][RSTR], int sm, int s0, int sp, int rc,
                                          const SimConsts& c, Face& f) {
     // rg[field][slot][col]; field 0 w, 1 hu, 2 hv, 3 BA, 4 BX, 5 BY
     const float wc = rg[0][s0][rc], wl = rg[0][s0][rc - 1], wr = rg[0][s0][rc + 1];
@@ -165,86 +231,119 @@ __device__ __forceinline__ void faces_at(const float (*rg)[RING][RW], int sm, in
     correct_w(BS, BN, wc, wS, wN);
     f.hN = wN - BN; f.hE = wE - BE; f.hS = wS - BS; f.hW = wW - BW;
     float q;
-    q = div_by_h(f.hN, c.epsilon); f.uN = q * huN; f.vN = q * hvN;
-    q = div_by_h(f.hE, c.epsilon); f.uE = q * huE; f.vE = q * hvE;
-    q = div_by_h(f.hS, c.epsilon); f.uS = q * huS; f.vS = q * hvS;
-    q = div_by_h(f.hW, c.epsilon); f.uW = q * huW; f.vW = q * hvW;
+    q = div_by_h_fast(f.hN, c.epsilon); f.uN = q * huN; f.vN = q * hvN;
+    q = div_by_h_fast(f.hE, c.epsilon); f.uE = q * huE; f.vE = q * hvE;
+    q = div_by_h_fast(f.hS, c.epsilon); f.uS = q * huS; f.vS = q * hvS;
+    q = div_by_h_fast(f.hW, c.epsilon); f.uW = q * huW; f.vW = q * hvW;
     f.msd = fmaxf(sd1 * c.one_over_dx, sd2 * c.one_over_dy);
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(MW, 4) k_march(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
+__global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
                                                  int ntiles, PassArgs pa) {
-    __shared__ float rg[6][RING][RW];
+    __shared__ __align__(128) float rg[6][RING][RSTR];
+    __shared__ __align__(8) unsigned long long bars[RING];
     __shared__ float fEW[2][6][MW];     // [row parity][hE,uE,vE,hW,uW,vW][thread]
     __shared__ float xb[2][3][MW];      // [row parity][component][thread] x flux at the thread's east face
     __shared__ double red[MW / 32][STATS_N];
+    constexpr int OFF = MIXED ? 18 : 9;  // plane layout: S(9) [L(9)] BY BX BA R0 R1 G(12) F(8) AUX(2) ...
+    constexpr int iBA = OFF + 2, iR0 = OFF + 3, iG0 = OFF + 5, iF0 = OFF + 17, iAUX = OFF + 25;
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int k = 0; k < RING; ++k) mbar_init(&bars[k], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    unsigned seq = 0;          // rows requested by this CTA so far (the same value in every thread)
+    bool tma_late = false;
 
     for (int it = blockIdx.x; it < ntiles; it += gridDim.x) {
         const int4 tl = tiles[it];
         const MemberDev& M = mems[tl.x];
         const SimConsts c = M.c;
-        const int P = M.P, NX = c.NX, NY = c.NY, nx = c.nx, ny = c.ny;
+        const int P = M.P, nx = c.nx, ny = c.ny;
+        float* __restrict__ B = M.base;
+        const size_t PL = M.plane;
+        const CUtensorMap* tm = M.tmaps;
         const int x0 = tl.y, y0 = tl.z;
-        const int xc = x0 - 1 + tid;          // this thread's column
-        const int rc = tid + 1;               // its ring column
+        const int xs = (x0 - 2) & ~3;          // TMA box start, 16-byte aligned
+        const int xc = x0 - 1 + tid;           // this thread's column
+        const int rc = xc - xs;                // its ring column
         const int yend = min(y0 + MH, ny + 2);
+        const int last_row = yend + 1;
         const bool out_col = tid >= 1 && tid <= MO && xc < nx + 2;
-        const float* Win = M.S[pa.in][0];
-        const float* HUin = M.S[pa.in][1];
-        const float* HVin = M.S[pa.in][2];
         const float dtm = *M.dtp;
         const float decay = t_pow(fabsf(c.whitewater_decay_rate), dtm);
         const bool corr = pa.scheme == CEL_SCHEME_CORRECTOR;
         const bool euler = pa.scheme == CEL_SCHEME_EULER;
-
-        auto load_row = [&](int gy) {
-            const int sl = ring_slot(gy);
-            for (int k = tid; k < RW; k += MW) {
-                const int gx = x0 - 2 + k;
-                const bool ok = gx >= 0 && gx < NX && gy >= 0 && gy < NY;
-                const size_t gi = size_t(gy) * P + gx;
-                rg[0][sl][k] = ok ? Win[gi] : 0.f;
-                rg[1][sl][k] = ok ? HUin[gi] : 0.f;
-                rg[2][sl][k] = ok ? HVin[gi] : 0.f;
-                rg[3][sl][k] = ok ? M.BA[gi] : 0.f;
-                rg[4][sl][k] = ok ? M.BX[gi] : 0.f;
-                rg[5][sl][k] = ok ? M.BY[gi] : 0.f;
-            }
+        const unsigned seq0 = seq;             // sequence number of row y0 - 2
+        auto row_seq = [&](int row) { return seq0 + unsigned(row - (y0 - 2)); };
+        auto issue = [&](int row) {            // one thread: request the 6 fields of a row
+            const unsigned q = row_seq(row);
+            const int sl = int(q % RING);
+            mbar_expect_tx(&bars[sl], ROW_BYTES);
+            tma_row(&rg[0][sl][0], tm + pa.in * 3 + 0, xs, row, &bars[sl]);
+            tma_row(&rg[1][sl][0], tm + pa.in * 3 + 1, xs, row, &bars[sl]);
+            tma_row(&rg[2][sl][0], tm + pa.in * 3 + 2, xs, row, &bars[sl]);
+            tma_row(&rg[3][sl][0], tm + 9, xs, row, &bars[sl]);
+            tma_row(&rg[4][sl][0], tm + 10, xs, row, &bars[sl]);
+            tma_row(&rg[5][sl][0], tm + 11, xs, row, &bars[sl]);
         };
+        auto slot = [&](int row) { return int(row_seq(row) % RING); };
 
         double acc[6] = {0, 0, 0, 0, 0, 0};
         float mx[4] = {0.f, 0.f, 0.f, 0.f};
         bool bad = false;
-        float nh = 0.f, nu = 0.f, nv = 0.f;   // north face of the previous row (this column)
-        float ypv0 = 0.f, ypv1 = 0.f, ypv2 = 0.f;  // y flux below the current row
+        float nh = 0.f, nu = 0.f, nv = 0.f;       // north face of the previous row (this column)
+        float ypv0 = 0.f, ypv1 = 0.f, ypv2 = 0.f; // y flux below the current row
 
         __syncthreads();  // the previous strip is done with shared memory
-        load_row(y0 - 2);
-        load_row(y0 - 1);
+        if (tid == 0) {
+            fence_proxy_async();
+            for (int r = y0 - 2; r <= min(y0 + 2, last_row); ++r) issue(r);
+        }
+        for (int r = y0 - 2; r < y0; ++r) {  // the first step also reads rows y0-2 and y0-1
+            const unsigned q = row_seq(r);
+            if (!mbar_wait_bounded(&bars[q % RING], (q / RING) & 1u)) tma_late = true;
+        }
         for (int t = y0 - 2; t < yend; ++t) {
-            load_row(t + 2);
-            // per-cell inputs of Pass3 at (xc, t), issued before the face work
+            // per-cell inputs of Pass3 at (xc, t), requested before the face work
             const bool do3 = t >= y0 && out_col;
-            const size_t gi = size_t(t < 0 ? 0 : t) * P + (xc < 0 ? 0 : xc);
+            const size_t go = size_t(t) * P + xc;
             float o0 = 0, o1 = 0, o2 = 0, q0 = 0, q1 = 0, q2 = 0, fo0 = 0, fo1 = 0, foo0 = 0, foo1 = 0;
             float p0 = 0, p1 = 0, p2 = 0, fp0 = 0, fp1 = 0, wcur = 0, wlo = 0;
             if (do3 && !euler) {
-                o0 = M.G[pa.og][0][gi]; o1 = M.G[pa.og][1][gi]; o2 = M.G[pa.og][2][gi];
-                q0 = M.G[pa.oog][0][gi]; q1 = M.G[pa.oog][1][gi]; q2 = M.G[pa.oog][2][gi];
-                fo0 = M.F[pa.og][0][gi]; fo1 = M.F[pa.og][1][gi];
-                foo0 = M.F[pa.oog][0][gi]; foo1 = M.F[pa.oog][1][gi];
+                o0 = B[size_t(iG0 + 3 * pa.og + 0) * PL + go];
+                o1 = B[size_t(iG0 + 3 * pa.og + 1) * PL + go];
+                o2 = B[size_t(iG0 + 3 * pa.og + 2) * PL + go];
+                q0 = B[size_t(iG0 + 3 * pa.oog + 0) * PL + go];
+                q1 = B[size_t(iG0 + 3 * pa.oog + 1) * PL + go];
+                q2 = B[size_t(iG0 + 3 * pa.oog + 2) * PL + go];
+                fo0 = B[size_t(iF0 + 2 * pa.og + 0) * PL + go];
+                fo1 = B[size_t(iF0 + 2 * pa.og + 1) * PL + go];
+                foo0 = B[size_t(iF0 + 2 * pa.oog + 0) * PL + go];
+                foo1 = B[size_t(iF0 + 2 * pa.oog + 1) * PL + go];
                 if (corr) {
-                    p0 = M.G[pa.pred][0][gi]; p1 = M.G[pa.pred][1][gi]; p2 = M.G[pa.pred][2][gi];
-                    fp0 = M.F[pa.pred][0][gi]; fp1 = M.F[pa.pred][1][gi];
-                    wcur = M.S[pa.cur][0][gi];
+                    p0 = B[size_t(iG0 + 3 * pa.pred + 0) * PL + go];
+                    p1 = B[size_t(iG0 + 3 * pa.pred + 1) * PL + go];
+                    p2 = B[size_t(iG0 + 3 * pa.pred + 2) * PL + go];
+                    fp0 = B[size_t(iF0 + 2 * pa.pred + 0) * PL + go];
+                    fp1 = B[size_t(iF0 + 2 * pa.pred + 1) * PL + go];
+                    wcur = B[size_t(3 * pa.cur) * PL + go];
                 }
             }
-            if (MIXED && do3) wlo = M.L[corr ? pa.cur : pa.in][0][gi];
-            __syncthreads();
-            // ---- faces of row t+1 (Pass1), aux update of that row, y flux between rows t and t+1 ----
-            const int s_m = ring_slot(t), s_0 = ring_slot(t + 1), s_p = ring_slot(t + 2);
+            if (MIXED && do3) wlo = B[size_t(9 + 3 * (corr ? pa.cur : pa.in)) * PL + go];
+            __syncthreads();  // (A) the previous row step is complete: its oldest ring slot is free
+            if (tid == 0 && t + PREFETCH + 2 <= last_row) {
+                fence_proxy_async();
+                issue(t + PREFETCH + 2);
+            }
+            {
+                const unsigned q = row_seq(t + 2);
+                if (!mbar_wait_bounded(&bars[q % RING], (q / RING) & 1u)) tma_late = true;
+            }
+            // ---- faces of row t+1 (Pass1), aux of that row, y flux between rows t and t+1 ----
+            const int s_m = slot(t), s_0 = slot(t + 1), s_p = slot(t + 2);
             Face f;
             faces_at(rg, s_m, s_0, s_p, rc, c, f);
             const int par1 = (t + 1) & 1;
@@ -256,26 +355,28 @@ __global__ void __launch_bounds__(MW, 4) k_march(const MemberDev* __restrict__ m
                     const int cx = xc < 2 ? 2 : xc, cy = gy < 2 ? 2 : gy;
                     if (cx >= x0 && cx < x0 + MO && cy >= y0 && cy < y0 + MH) {
                         const size_t ai = size_t(gy) * P + xc;
-                        const float msd = t_atan(f.msd);
-                        const float md = fmaxf((f.hN + f.hE + f.hS + f.hW) / 4.0f, M.AUX[0][ai]);
-                        float bw = M.AUX[1][ai];
-                        if (msd > c.dissipation_threshold) bw = 1.0f;
-                        M.AUX[0][ai] = md;
-                        M.AUX[1][ai] = bw * decay;
+                        float* a0 = B + size_t(iAUX) * PL + ai;
+                        float* a1 = B + size_t(iAUX + 1) * PL + ai;
+                        const float md = fmaxf((f.hN + f.hE + f.hS + f.hW) / 4.0f, *a0);
+                        float bw = *a1;
+                        if (f.msd > M.tan_thr) bw = 1.0f;  // atan(msd) > threshold
+                        *a0 = md;
+                        *a1 = bw * decay;
                     }
                 }
             }
             const float g = c.g, hg = c.half_g;
-            float yf0 = 0.f, yf1 = 0.f, yf2 = 0.f;
+            float yf[3];
             {   // y flux at the north face of row t: north face of row t (carried) vs south face of row t+1
                 const float hN = nh, uN = nu, vN = nv;
                 const float hSn = f.hS, uSn = f.uS, vSn = f.vS;
                 const float cN = sqrtf(g * hN), cS = sqrtf(g * hSn);
                 const float bp = fmaxf(fmaxf(vN + cN, vSn + cS), 0.f);
                 const float bm = fminf(fminf(vN - cN, vSn - cS), 0.f);
-                yf0 = numflux(bp, bm, hSn * vSn, hN * vN, hSn - hN);
-                yf1 = numflux(bp, bm, hSn * uSn * vSn, hN * uN * vN, hSn * uSn - hN * uN);
-                yf2 = numflux(bp, bm, hSn * (vSn * vSn + hg * hSn), hN * (vN * vN + hg * hN), hSn * vSn - hN * vN);
+                const float Fp[3] = {hSn * vSn, hSn * uSn * vSn, hSn * (vSn * vSn + hg * hSn)};
+                const float Fm[3] = {hN * vN, hN * uN * vN, hN * (vN * vN + hg * hN)};
+                const float dU[3] = {hSn - hN, hSn * uSn - hN * uN, hSn * vSn - hN * vN};
+                numflux3(bp, bm, Fp, Fm, dU, yf);
             }
             // ---- x flux at the east face of (xc, t): faces of row t from the previous step ----
             const int par = t & 1;
@@ -285,15 +386,18 @@ __global__ void __launch_bounds__(MW, 4) k_march(const MemberDev* __restrict__ m
                 const float cE = sqrtf(g * hE), cW = sqrtf(g * hWe);
                 const float ap = fmaxf(fmaxf(uE + cE, uWe + cW), 0.f);
                 const float am = fminf(fminf(uE - cE, uWe - cW), 0.f);
-                xb[par][0][tid] = numflux(ap, am, hWe * uWe, hE * uE, hWe - hE);
-                xb[par][1][tid] = numflux(ap, am, hWe * (uWe * uWe + hg * hWe), hE * (uE * uE + hg * hE), hWe * uWe - hE * uE);
-                xb[par][2][tid] = numflux(ap, am, hWe * uWe * vWe, hE * uE * vE, hWe * vWe - hE * vE);
+                const float Fp[3] = {hWe * uWe, hWe * (uWe * uWe + hg * hWe), hWe * uWe * vWe};
+                const float Fm[3] = {hE * uE, hE * (uE * uE + hg * hE), hE * uE * vE};
+                const float dU[3] = {hWe - hE, hWe * uWe - hE * uE, hWe * vWe - hE * vE};
+                float xo[3];
+                numflux3(ap, am, Fp, Fm, dU, xo);
+                xb[par][0][tid] = xo[0]; xb[par][1][tid] = xo[1]; xb[par][2][tid] = xo[2];
             }
-            __syncthreads();
+            __syncthreads();  // (B)
             // ---- Pass3 at (xc, t) ----
             if (do3) {
-                const int r0 = ring_slot(t), rm = ring_slot(t - 1), rp = ring_slot(t + 1);
-                const int rmm = ring_slot(t - 2), rpp = ring_slot(t + 2);
+                const int r0 = slot(t), rm = slot(t - 1), rp = slot(t + 1);
+                const int rmm = slot(t - 2), rpp = slot(t + 2);
                 const float sl = c.sea_level;
                 const float wc = rg[0][r0][rc], huc = rg[1][r0][rc], hvc = rg[2][r0][rc];
                 const float BAh = rg[3][r0][rc], BXh = rg[4][r0][rc], BYh = rg[5][r0][rc];
@@ -313,8 +417,8 @@ __global__ void __launch_bounds__(MW, 4) k_march(const MemberDev* __restrict__ m
                 const float edl = rg[0][rm][rc - 1] - sl, edr = rg[0][rm][rc + 1] - sl;
                 const float odx = c.one_over_dx, ody = c.one_over_dy;
                 const float od2x = odx * odx, od3x = od2x * odx, od2y = ody * ody, od3y = od2y * ody;
-                const float ddx = (-drr + 8 * dr - 8 * dl + dll) * odx / 12.0f;
-                const float ddy = (-duu + 8 * du - 8 * ddn + ddd) * ody / 12.0f;
+                const float ddx = (-drr + 8 * dr - 8 * dl + dll) * odx * (1.0f / 12.0f);
+                const float ddy = (-duu + 8 * du - 8 * ddn + ddd) * ody * (1.0f / 12.0f);
                 const float exy = (0.25f * odx * ody * (eur - edr - eul + edl));
                 const float exx = od2x * (er - 2 * e0 + el);
                 const float eyy = od2y * (eu - 2 * e0 + ed);
@@ -325,44 +429,48 @@ __global__ void __launch_bounds__(MW, 4) k_march(const MemberDev* __restrict__ m
                 const float P1y = Bg * (d3) * ((euu - 2 * eu + 2 * ed - edd) * (0.5f * od3y) +
                                                (eur + eul - 2 * eu + 2 * ed - edr - edl) * (0.5f * ody * od2x));
                 const float P2y = Bg * (d2) * (ddy * (exx + 2 * eyy) + ddx * exy);
-                const float fr = friction_calc(huc, hvc, h, c.friction, c.is_manning, c.g, c.epsilon);
+                const float fr = friction_fast(huc, hvc, h, c.friction, c.is_manning, c.g, c.epsilon);
                 const float s1 = -c.g_over_dx * h * (BXh - BXw) - huc * fr + (P1x + P2x);
                 const float s2 = -c.g_over_dy * h * (BYh - BYs) - hvc * fr + (P1y + P2y);
-                const float f0 = (xb[par][0][tid - 1] - xb[par][0][tid]) * odx + (ypv0 - yf0) * ody;
-                const float f1 = (xb[par][1][tid - 1] - xb[par][1][tid]) * odx + (ypv1 - yf1) * ody + s1;
-                const float f2 = (xb[par][2][tid - 1] - xb[par][2][tid]) * odx + (ypv2 - yf2) * ody + s2;
+                const float f0 = (xb[par][0][tid - 1] - xb[par][0][tid]) * odx + (ypv0 - yf[0]) * ody;
+                const float f1 = (xb[par][1][tid - 1] - xb[par][1][tid]) * odx + (ypv1 - yf[1]) * ody + s1;
+                const float f2 = (xb[par][2][tid - 1] - xb[par][2][tid]) * odx + (ypv2 - yf[2]) * ody + s2;
                 const float sixth = 1.0f / 6.0f;
-                const float Fs = (sixth * dh * (ddx * ((ody / 2.0f) * (rg[2][rp][rc] - rg[2][rm][rc])) +
-                                                (ddy * ((odx / 2.0f) * (rg[2][r0][rc + 1] - rg[2][r0][rc - 1])))));
-                const float Gs = (sixth * dh * (ddx * ((ody / 2.0f) * (rg[1][rp][rc] - rg[1][rm][rc])) +
-                                                (ddy * ((odx / 2.0f) * (rg[1][r0][rc + 1] - rg[1][r0][rc - 1])))));
+                const float Fs = (sixth * dh * (ddx * ((ody * 0.5f) * (rg[2][rp][rc] - rg[2][rm][rc])) +
+                                                (ddy * ((odx * 0.5f) * (rg[2][r0][rc + 1] - rg[2][r0][rc - 1])))));
+                const float Gs = (sixth * dh * (ddx * ((ody * 0.5f) * (rg[1][rp][rc] - rg[1][rm][rc])) +
+                                                (ddy * ((odx * 0.5f) * (rg[1][r0][rc + 1] - rg[1][r0][rc - 1])))));
                 const float dt = dtm;
                 float dw, rhu, rhv;
                 float wbase = wc;
                 if (euler) {
                     dw = dt * f0; rhu = dt * f1; rhv = dt * f2;
                 } else if (!corr) {
-                    dw = dt / 12.0f * (23.0f * f0 - 16.0f * o0 + 5.0f * q0);
-                    rhu = dt / 12.0f * (23.0f * f1 - 16.0f * o1 + 5.0f * q1) + (2.0f * Fs - 3.0f * fo0 + foo0);
-                    rhv = dt / 12.0f * (23.0f * f2 - 16.0f * o2 + 5.0f * q2) + (2.0f * Gs - 3.0f * fo1 + foo1);
+                    const float k12 = dt * (1.0f / 12.0f);
+                    dw = k12 * (23.0f * f0 - 16.0f * o0 + 5.0f * q0);
+                    rhu = k12 * (23.0f * f1 - 16.0f * o1 + 5.0f * q1) + (2.0f * Fs - 3.0f * fo0 + foo0);
+                    rhv = k12 * (23.0f * f2 - 16.0f * o2 + 5.0f * q2) + (2.0f * Gs - 3.0f * fo1 + foo1);
                 } else {
-                    dw = dt / 24.0f * (9 * f0 + 19 * p0 - 5 * o0 + 1 * q0);
-                    rhu = dt / 24.0f * (9 * f1 + 19 * p1 - 5 * o1 + 1 * q1) + Fs - fp0;
-                    rhv = dt / 24.0f * (9 * f2 + 19 * p2 - 5 * o2 + 1 * q2) + Gs - fp1;
+                    const float k24 = dt * (1.0f / 24.0f);
+                    dw = k24 * (9 * f0 + 19 * p0 - 5 * o0 + 1 * q0);
+                    rhu = k24 * (9 * f1 + 19 * p1 - 5 * o1 + 1 * q1) + Fs - fp0;
+                    rhv = k24 * (9 * f2 + 19 * p2 - 5 * o2 + 1 * q2) + Gs - fp1;
                     wbase = wcur;
                 }
-                const size_t go = size_t(t) * P + xc;
                 float wn = wbase, wl = wlo;
                 if (MIXED) two_sum_add(wn, wl, dw);
                 else wn = wbase + dw;
-                M.S[pa.out][0][go] = wn;
-                if (MIXED) M.L[pa.out][0][go] = wl;
-                M.R[0][go] = rhu;
-                M.R[1][go] = rhv;
-                M.G[pa.scr][0][go] = f0; M.G[pa.scr][1][go] = f1; M.G[pa.scr][2][go] = f2;
-                M.F[pa.scr][0][go] = Fs; M.F[pa.scr][1][go] = Gs;
+                B[size_t(3 * pa.out) * PL + go] = wn;
+                if (MIXED) B[size_t(9 + 3 * pa.out) * PL + go] = wl;
+                B[size_t(iR0) * PL + go] = rhu;
+                B[size_t(iR0 + 1) * PL + go] = rhv;
+                B[size_t(iG0 + 3 * pa.scr + 0) * PL + go] = f0;
+                B[size_t(iG0 + 3 * pa.scr + 1) * PL + go] = f1;
+                B[size_t(iG0 + 3 * pa.scr + 2) * PL + go] = f2;
+                B[size_t(iF0 + 2 * pa.scr + 0) * PL + go] = Fs;
+                B[size_t(iF0 + 2 * pa.scr + 1) * PL + go] = Gs;
                 // GetStats (compute.hlsl:1319-1378) of the input state, FP64 accumulation
-                const float q = div_by_h(h, c.epsilon);
+                const float q = div_by_h_fast(h, c.epsilon);
                 const float u = q * huc, v = q * hvc;
                 if (xc < 2 + 4 * (nx / 4) && t < 2 + 4 * (ny / 4)) {
                     acc[0] += h; acc[1] += double(h * (BAh + 0.5f * h)); acc[2] += huc; acc[3] += hvc;
@@ -376,10 +484,12 @@ __global__ void __launch_bounds__(MW, 4) k_march(const MemberDev* __restrict__ m
                 acc[5] += h;
                 bad = bad || !isfinite(wc) || !isfinite(huc) || !isfinite(hvc);
             }
-            ypv0 = yf0; ypv1 = yf1; ypv2 = yf2;
+            ypv0 = yf[0]; ypv1 = yf[1]; ypv2 = yf[2];
             nh = f.hN; nu = f.uN; nv = f.vN;
         }
+        seq = seq0 + unsigned(last_row - (y0 - 2) + 1);
         // ---- zero the ghost ring of the output state next to this strip (engine.cpp:1007) ----
+        const int NX = c.NX, NY = c.NY;
         const bool west = x0 == 2, east = x0 + MO >= nx + 2, south = y0 == 2, north = y0 + MH >= ny + 2;
         if (west || east || south || north) {
             const int cx0 = west ? 0 : x0, cx1 = east ? NX : x0 + MO;
@@ -388,28 +498,30 @@ __global__ void __launch_bounds__(MW, 4) k_march(const MemberDev* __restrict__ m
             for (int k = tid; k < w * (cy1 - cy0); k += MW) {
                 const int gx = cx0 + k % w, gy = cy0 + k / w;
                 if (gx >= 2 && gx < nx + 2 && gy >= 2 && gy < ny + 2) continue;
-                const size_t go = size_t(gy) * P + gx;
-                M.S[pa.out][0][go] = 0.f; M.S[pa.out][1][go] = 0.f; M.S[pa.out][2][go] = 0.f;
-                if (MIXED) { M.L[pa.out][0][go] = 0.f; M.L[pa.out][1][go] = 0.f; M.L[pa.out][2][go] = 0.f; }
+                const size_t gz = size_t(gy) * P + gx;
+                for (int q = 0; q < 3; ++q) {
+                    B[size_t(3 * pa.out + q) * PL + gz] = 0.f;
+                    if (MIXED) B[size_t(9 + 3 * pa.out + q) * PL + gz] = 0.f;
+                }
             }
         }
         // ---- strip statistics -> member accumulators ----
         {
-            double s[STATS_N];
-            for (int k = 0; k < 6; ++k) s[k] = acc[k];
-            for (int k = 0; k < 4; ++k) s[6 + k] = mx[k];
-            s[10] = bad ? 1.0 : 0.0;
-            s[11] = 0.0;
+            double sv[STATS_N];
+            for (int k = 0; k < 6; ++k) sv[k] = acc[k];
+            for (int k = 0; k < 4; ++k) sv[6 + k] = mx[k];
+            sv[10] = bad ? 1.0 : 0.0;
+            sv[11] = tma_late ? 1.0 : 0.0;
             for (int off = 16; off; off >>= 1)
-                for (int k = 0; k < 11; ++k) {
-                    const double o = __shfl_down_sync(0xffffffffu, s[k], off);
-                    s[k] = (k >= 6) ? fmax(s[k], o) : s[k] + o;
+                for (int k = 0; k < STATS_N; ++k) {
+                    const double o = __shfl_down_sync(0xffffffffu, sv[k], off);
+                    sv[k] = (k >= 6) ? fmax(sv[k], o) : sv[k] + o;
                 }
             const int lane = tid & 31, wid = tid >> 5;
             if (lane == 0)
-                for (int k = 0; k < 11; ++k) red[wid][k] = s[k];
+                for (int k = 0; k < STATS_N; ++k) red[wid][k] = sv[k];
             __syncthreads();
-            if (tid < 11) {
+            if (tid < STATS_N) {
                 double a = red[0][tid];
                 for (int w = 1; w < MW / 32; ++w) a = (tid >= 6) ? fmax(a, red[w][tid]) : a + red[w][tid];
                 if (tid < 6) { if (a != 0.0) atomicAdd(M.stats + tid, a); }
@@ -898,6 +1010,35 @@ namespace cel {
 
 namespace {
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link needed)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+// Row map of one NX x NY plane with pitch P floats: boxes of RBOX x 1 floats; reads outside
+// the plane return zero, like the reference's out-of-range texture loads.
+int encode_row_map(CUtensorMap* m, const float* plane, int NX, int NY, int P, std::string& err) {
+    auto enc = tensor_map_encoder();
+    if (!enc) { err = "cuTensorMapEncodeTiled unavailable"; return CEL_ERR_CUDA; }
+    cuuint64_t dims[2] = {cuuint64_t(NX), cuuint64_t(NY)};
+    cuuint64_t strides[1] = {cuuint64_t(P) * sizeof(float)};
+    cuuint32_t box[2] = {cuuint32_t(RBOX), 1u};
+    cuuint32_t estr[2] = {1u, 1u};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(plane), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) { err = "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")"; return CEL_ERR_CUDA; }
+    return CEL_OK;
+}
+
 int dalloc(cel_batch* b, void** ptr, size_t bytes, std::string& err) {
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, bytes);
@@ -1131,6 +1272,12 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         void* base = nullptr;
         if (dalloc(b.get(), &base, m.plane * nplanes * sizeof(float), err)) return nullptr;
         float* q = static_cast<float*>(base);
+        d.base = q;
+        d.plane = m.plane;
+        {   // tan of the breaking threshold (atan is monotonic on (-pi/2, pi/2))
+            const double th = m.p.dissipation_threshold;
+            d.tan_thr = th >= M_PI / 2 ? INFINITY : th <= -M_PI / 2 ? -INFINITY : float(std::tan(th));
+        }
         auto next = [&]() { float* r = q; q += m.plane; return r; };
         for (int s = 0; s < 3; ++s) for (int k = 0; k < 3; ++k) d.S[s][k] = next();
         if (b->mixed) for (int s = 0; s < 3; ++s) for (int k = 0; k < 3; ++k) d.L[s][k] = next();
@@ -1144,6 +1291,22 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         for (int k = 0; k < 3; ++k) fx[k] = next();
         for (int k = 0; k < 3; ++k) fy[k] = next();
         for (int k = 0; k < 3; ++k) { d.FX[k] = fx[k]; d.FYF[k] = fy[k]; }
+        {   // TMA row maps: the three state buffers (w, hu, hv), then BA, BX, BY
+            std::vector<CUtensorMap> maps(12);
+            for (int sb = 0; sb < 3; ++sb)
+                for (int k = 0; k < 3; ++k)
+                    if (encode_row_map(&maps[sb * 3 + k], d.S[sb][k], NX, NY, m.P, err)) return nullptr;
+            if (encode_row_map(&maps[9], ba, NX, NY, m.P, err) || encode_row_map(&maps[10], bx, NX, NY, m.P, err) ||
+                encode_row_map(&maps[11], by, NX, NY, m.P, err))
+                return nullptr;
+            void* mp = nullptr;
+            if (dalloc(b.get(), &mp, sizeof(CUtensorMap) * 12, err)) return nullptr;
+            if (cudaMemcpy(mp, maps.data(), sizeof(CUtensorMap) * 12, cudaMemcpyHostToDevice) != cudaSuccess) {
+                err = "tensor map upload failed";
+                return nullptr;
+            }
+            d.tmaps = static_cast<const CUtensorMap*>(mp);
+        }
         d.stats = b->stats_all + size_t(i) * STATS_N;
         d.stats_now = b->stats_now_all + size_t(i) * STATS_N;
         {
@@ -1337,9 +1500,10 @@ int batch_stats(cel_batch* b, cel_stats* out, std::string& err) {
     B_TRY(cudaMemsetAsync(b->stats_now_all, 0, n * STATS_N * sizeof(double), b->stream));
     k_stats_only<<<std::min(b->ntiles, b->sms * 8), 256, 0, b->stream>>>(b->ddev, b->tiles, b->ntiles, b->ix.sin);
     B_TRY(cudaGetLastError());
-    std::vector<double> v(n * STATS_N);
-    std::vector<double> t(n * 2);
+    std::vector<double> v(n * STATS_N), pass_stats(n * STATS_N);
     B_TRY(cudaMemcpyAsync(v.data(), b->stats_now_all, v.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    B_TRY(cudaMemcpyAsync(pass_stats.data(), b->stats_all, pass_stats.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                          b->stream));
     std::vector<double> t64(n);
     for (size_t i = 0; i < n; ++i)
         B_TRY(cudaMemcpyAsync(&t64[i], b->hdev[i].time64, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
@@ -1364,6 +1528,8 @@ int batch_stats(cel_batch* b, cel_stats* out, std::string& err) {
         o.cfl_rate = s[8];
         o.max_froude = std::sqrt(s[9] / g);
         o.health = s[10] != 0 ? CEL_ERR_NUMERIC : 0;
+        // a bounded TMA wait that gave up in the last pass (should never happen) is a CUDA error
+        if (pass_stats[i * STATS_N + 11] != 0) o.health = CEL_ERR_CUDA;
         o.timestep = double(b->dt_host[i]);
         o.cfl_number = o.cfl_rate * o.timestep;
         o.total_time = t64[i];
