@@ -175,8 +175,8 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 }
 // Bounded wait: gives up after a fixed number of polls and reports false (the caller flags the
 // error and carries on with whatever the buffer holds, so no thread can hang on it).
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (int k = 0; k < (1 << 22); ++k)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, int polls) {
+    for (int k = 0; k < polls; ++k)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
         }
         for (int r = y0 - 2; r < y0; ++r) {  // the first step also reads rows y0-2 and y0-1
             const unsigned q = row_seq(r);
-            if (!mbar_wait_bounded(&bars[q % RING], (q / RING) & 1u)) tma_late = true;
+            if (!mbar_wait_bounded(&bars[q % RING], (q / RING) & 1u, tma_late ? 1 : (1 << 22))) tma_late = true;
         }
         for (int t = y0 - 2; t < yend; ++t) {
             // per-cell inputs of Pass3 at (xc, t), requested before the face work
@@ -340,7 +340,7 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
             }
             {
                 const unsigned q = row_seq(t + 2);
-                if (!mbar_wait_bounded(&bars[q % RING], (q / RING) & 1u)) tma_late = true;
+                if (!mbar_wait_bounded(&bars[q % RING], (q / RING) & 1u, tma_late ? 1 : (1 << 22))) tma_late = true;
             }
             // ---- faces of row t+1 (Pass1), aux of that row, y flux between rows t and t+1 ----
             const int s_m = slot(t), s_0 = slot(t + 1), s_p = slot(t + 2);
