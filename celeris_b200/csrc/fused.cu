@@ -300,7 +300,9 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
         __syncthreads();  // the previous strip is done with shared memory
         if (tid == 0) {
             fence_proxy_async();
-            for (int r = y0 - 2; r <= min(y0 + 2, last_row); ++r) issue(r);
+            // rows y0-2 .. y0+PREFETCH-1 here; the loop requests row t+PREFETCH+2 at step t, so
+            // every row is requested exactly once (one arrive per mbarrier phase)
+            for (int r = y0 - 2; r <= min(y0 + PREFETCH - 1, last_row); ++r) issue(r);
         }
         for (int r = y0 - 2; r < y0; ++r) {  // the first step also reads rows y0-2 and y0-1
             const unsigned q = row_seq(r);
