@@ -213,20 +213,28 @@ __device__ __forceinline__ float friction_fast(float hu, float hv, float h, floa
 
 struct Face { float hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, msd; };
 
-// Pass1 at one cell from ring rows: w/hu/hv/BX/BY at (rc +- 1, row +- 1).
-__device__ __forceinline__ void faces_at(const float (*rg)[RING][RSTR], int sm, int s0, int sp, int rc,
-                                         const SimConsts& c, Face& f) {
-    // rg[field][slot][col]; field 0 w, 1 hu, 2 hv, 3 BA, 4 BX, 5 BY
-    const float wc = rg[0][s0][rc], wl = rg[0][s0][rc - 1], wr = rg[0][s0][rc + 1];
-    const float wd = rg[0][sm][rc], wu = rg[0][sp][rc];
-    const float BN = rg[5][s0][rc], BE = rg[4][s0][rc], BS = rg[5][sm][rc], BW = rg[4][s0][rc - 1];
+// Ring layout: field f, slot s, column k at ring[f * FSTR + s * RSTR + k]; a "row base" is
+// s * RSTR + (this thread's column), so every access is base + compile-time offset.
+constexpr int FSTR = RING * RSTR;
+
+// Pass1 at one cell: rows below / here / above given by their row bases.
+__device__ __forceinline__ void faces_at(const float* __restrict__ ring, int bm, int b0, int bp, const SimConsts& c,
+                                         Face& f) {
+    const float* W = ring;
+    const float* HU = ring + FSTR;
+    const float* HV = ring + 2 * FSTR;
+    const float* BXr = ring + 4 * FSTR;
+    const float* BYr = ring + 5 * FSTR;
+    const float wc = W[b0], wl = W[b0 - 1], wr = W[b0 + 1], wd = W[bm], wu = W[bp];
+    const float BN = BYr[b0], BE = BXr[b0], BS = BYr[bm], BW = BXr[b0 - 1];
     float wN, wE, wS, wW, huN, huE, huS, huW, hvN, hvE, hvS, hvW, sd1, sd2;
     reconstruct_sd(c.two_theta, wl, wc, wr, wW, wE, sd1);
     reconstruct_sd(c.two_theta, wd, wc, wu, wS, wN, sd2);
-    reconstruct(c.two_theta, rg[1][s0][rc - 1], rg[1][s0][rc], rg[1][s0][rc + 1], huW, huE);
-    reconstruct(c.two_theta, rg[1][sm][rc], rg[1][s0][rc], rg[1][sp][rc], huS, huN);
-    reconstruct(c.two_theta, rg[2][s0][rc - 1], rg[2][s0][rc], rg[2][s0][rc + 1], hvW, hvE);
-    reconstruct(c.two_theta, rg[2][sm][rc], rg[2][s0][rc], rg[2][sp][rc], hvS, hvN);
+    const float huc = HU[b0], hvc = HV[b0];
+    reconstruct(c.two_theta, HU[b0 - 1], huc, HU[b0 + 1], huW, huE);
+    reconstruct(c.two_theta, HU[bm], huc, HU[bp], huS, huN);
+    reconstruct(c.two_theta, HV[b0 - 1], hvc, HV[b0 + 1], hvW, hvE);
+    reconstruct(c.two_theta, HV[bm], hvc, HV[bp], hvS, hvN);
     correct_w(BW, BE, wc, wW, wE);
     correct_w(BS, BN, wc, wS, wN);
     f.hN = wN - BN; f.hE = wE - BE; f.hS = wS - BS; f.hW = wW - BW;
@@ -241,13 +249,13 @@ __device__ __forceinline__ void faces_at(const float (*rg)[RING][RSTR], int sm, 
 template <bool MIXED>
 __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
                                                  int ntiles, PassArgs pa) {
-    __shared__ __align__(128) float rg[6][RING][RSTR];
+    __shared__ __align__(128) float ring[6 * FSTR];
     __shared__ __align__(8) unsigned long long bars[RING];
     __shared__ float fEW[2][6][MW];     // [row parity][hE,uE,vE,hW,uW,vW][thread]
     __shared__ float xb[2][3][MW];      // [row parity][component][thread] x flux at the thread's east face
     __shared__ double red[MW / 32][STATS_N];
     constexpr int OFF = MIXED ? 18 : 9;  // plane layout: S(9) [L(9)] BY BX BA R0 R1 G(12) F(8) AUX(2) ...
-    constexpr int iBA = OFF + 2, iR0 = OFF + 3, iG0 = OFF + 5, iF0 = OFF + 17, iAUX = OFF + 25;
+    constexpr int iR0 = OFF + 3, iG0 = OFF + 5, iF0 = OFF + 17, iAUX = OFF + 25;
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int k = 0; k < RING; ++k) mbar_init(&bars[k], 1);
@@ -256,6 +264,12 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
     __syncthreads();
     unsigned seq = 0;          // rows requested by this CTA so far (the same value in every thread)
     bool tma_late = false;
+    const float* W = ring;
+    const float* HU = ring + FSTR;
+    const float* HV = ring + 2 * FSTR;
+    const float* BAr = ring + 3 * FSTR;
+    const float* BXr = ring + 4 * FSTR;
+    const float* BYr = ring + 5 * FSTR;
 
     for (int it = blockIdx.x; it < ntiles; it += gridDim.x) {
         const int4 tl = tiles[it];
@@ -263,7 +277,7 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
         const SimConsts c = M.c;
         const int P = M.P, nx = c.nx, ny = c.ny;
         float* __restrict__ B = M.base;
-        const size_t PL = M.plane;
+        const unsigned PL = unsigned(M.plane);
         const CUtensorMap* tm = M.tmaps;
         const int x0 = tl.y, y0 = tl.z;
         const int xs = (x0 - 2) & ~3;          // TMA box start, 16-byte aligned
@@ -276,20 +290,26 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
         const float decay = t_pow(fabsf(c.whitewater_decay_rate), dtm);
         const bool corr = pa.scheme == CEL_SCHEME_CORRECTOR;
         const bool euler = pa.scheme == CEL_SCHEME_EULER;
-        const unsigned seq0 = seq;             // sequence number of row y0 - 2
-        auto row_seq = [&](int row) { return seq0 + unsigned(row - (y0 - 2)); };
-        auto issue = [&](int row) {            // one thread: request the 6 fields of a row
-            const unsigned q = row_seq(row);
-            const int sl = int(q % RING);
+        // warp-uniform plane offsets (in floats) for this pass
+        const unsigned oOG = unsigned(iG0 + 3 * pa.og) * PL, oOOG = unsigned(iG0 + 3 * pa.oog) * PL;
+        const unsigned oFO = unsigned(iF0 + 2 * pa.og) * PL, oFOO = unsigned(iF0 + 2 * pa.oog) * PL;
+        const unsigned oPR = unsigned(iG0 + 3 * pa.pred) * PL, oFP = unsigned(iF0 + 2 * pa.pred) * PL;
+        const unsigned oSCR = unsigned(iG0 + 3 * pa.scr) * PL, oFS = unsigned(iF0 + 2 * pa.scr) * PL;
+        const unsigned oOUT = unsigned(3 * pa.out) * PL, oCUR = unsigned(3 * pa.cur) * PL;
+        const unsigned oLB = unsigned(9 + 3 * (corr ? pa.cur : pa.in)) * PL, oLO = unsigned(9 + 3 * pa.out) * PL;
+        const unsigned oR = unsigned(iR0) * PL, oAUX = unsigned(iAUX) * PL;
+
+        auto issue = [&](int row, int sl) {    // one thread: request the 6 fields of a row into slot sl
             mbar_expect_tx(&bars[sl], ROW_BYTES);
-            tma_row(&rg[0][sl][0], tm + pa.in * 3 + 0, xs, row, &bars[sl]);
-            tma_row(&rg[1][sl][0], tm + pa.in * 3 + 1, xs, row, &bars[sl]);
-            tma_row(&rg[2][sl][0], tm + pa.in * 3 + 2, xs, row, &bars[sl]);
-            tma_row(&rg[3][sl][0], tm + 9, xs, row, &bars[sl]);
-            tma_row(&rg[4][sl][0], tm + 10, xs, row, &bars[sl]);
-            tma_row(&rg[5][sl][0], tm + 11, xs, row, &bars[sl]);
+            float* dst = ring + sl * RSTR;
+            tma_row(dst, tm + pa.in * 3 + 0, xs, row, &bars[sl]);
+            tma_row(dst + FSTR, tm + pa.in * 3 + 1, xs, row, &bars[sl]);
+            tma_row(dst + 2 * FSTR, tm + pa.in * 3 + 2, xs, row, &bars[sl]);
+            tma_row(dst + 3 * FSTR, tm + 9, xs, row, &bars[sl]);
+            tma_row(dst + 4 * FSTR, tm + 10, xs, row, &bars[sl]);
+            tma_row(dst + 5 * FSTR, tm + 11, xs, row, &bars[sl]);
         };
-        auto slot = [&](int row) { return int(row_seq(row) % RING); };
+        auto next_slot = [](int s) { return s + 1 == RING ? 0 : s + 1; };
 
         double acc[6] = {0, 0, 0, 0, 0, 0};
         float mx[4] = {0.f, 0.f, 0.f, 0.f};
@@ -297,57 +317,59 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
         float nh = 0.f, nu = 0.f, nv = 0.f;       // north face of the previous row (this column)
         float ypv0 = 0.f, ypv1 = 0.f, ypv2 = 0.f; // y flux below the current row
 
+        // Row r of this strip has sequence number seq0 + (r - (y0 - 2)), ring slot seq % RING and
+        // mbarrier phase parity (seq / RING) & 1.
+        const unsigned seq0 = seq;
+        const int sA = int(seq0 % RING), sB = next_slot(sA), sC = next_slot(sB);  // rows y0-2, y0-1, y0
+
         __syncthreads();  // the previous strip is done with shared memory
         if (tid == 0) {
             fence_proxy_async();
-            // rows y0-2 .. y0+PREFETCH-1 here; the loop requests row t+PREFETCH+2 at step t, so
-            // every row is requested exactly once (one arrive per mbarrier phase)
-            for (int r = y0 - 2; r <= min(y0 + PREFETCH - 1, last_row); ++r) issue(r);
+            // rows y0-2 .. y0+PREFETCH-1 here; the loop requests row t+PREFETCH+2 at step t, so every
+            // row is requested exactly once (one arrive per mbarrier phase)
+            int sl = sA;
+            for (int r = y0 - 2; r <= min(y0 + PREFETCH - 1, last_row); ++r) { issue(r, sl); sl = next_slot(sl); }
         }
-        for (int r = y0 - 2; r < y0; ++r) {  // the first step also reads rows y0-2 and y0-1
-            const unsigned q = row_seq(r);
-            if (!mbar_wait_bounded(&bars[q % RING], (q / RING) & 1u, tma_late ? 1 : (1 << 22))) tma_late = true;
+        {   // the first step also reads rows y0-2 and y0-1
+            const unsigned pA = (seq0 / RING) & 1u, pB = ((seq0 + 1) / RING) & 1u;
+            if (!mbar_wait_bounded(&bars[sA], pA, tma_late ? 1 : (1 << 22))) tma_late = true;
+            if (!mbar_wait_bounded(&bars[sB], pB, tma_late ? 1 : (1 << 22))) tma_late = true;
         }
+        // window of rows t-2, t-1, t, t+1, t+2 at the first step (t = y0-2); the two rows below are
+        // not read before t = y0, by when the window has shifted onto loaded rows
+        int s2m = sA, s1m = sA, s0 = sA, s1p = sB, s2p = sC;
+        unsigned par2p = ((seq0 + 2) / RING) & 1u;            // phase parity of row t+2
+        int sReq = int((seq0 + unsigned(PREFETCH) + 2) % RING);  // slot of row t+PREFETCH+2
+
         for (int t = y0 - 2; t < yend; ++t) {
             // per-cell inputs of Pass3 at (xc, t), requested before the face work
             const bool do3 = t >= y0 && out_col;
-            const size_t go = size_t(t) * P + xc;
+            float* cp = B + (size_t(t) * P + xc);
             float o0 = 0, o1 = 0, o2 = 0, q0 = 0, q1 = 0, q2 = 0, fo0 = 0, fo1 = 0, foo0 = 0, foo1 = 0;
             float p0 = 0, p1 = 0, p2 = 0, fp0 = 0, fp1 = 0, wcur = 0, wlo = 0;
             if (do3 && !euler) {
-                o0 = B[size_t(iG0 + 3 * pa.og + 0) * PL + go];
-                o1 = B[size_t(iG0 + 3 * pa.og + 1) * PL + go];
-                o2 = B[size_t(iG0 + 3 * pa.og + 2) * PL + go];
-                q0 = B[size_t(iG0 + 3 * pa.oog + 0) * PL + go];
-                q1 = B[size_t(iG0 + 3 * pa.oog + 1) * PL + go];
-                q2 = B[size_t(iG0 + 3 * pa.oog + 2) * PL + go];
-                fo0 = B[size_t(iF0 + 2 * pa.og + 0) * PL + go];
-                fo1 = B[size_t(iF0 + 2 * pa.og + 1) * PL + go];
-                foo0 = B[size_t(iF0 + 2 * pa.oog + 0) * PL + go];
-                foo1 = B[size_t(iF0 + 2 * pa.oog + 1) * PL + go];
+                o0 = cp[oOG]; o1 = cp[oOG + PL]; o2 = cp[oOG + 2 * PL];
+                q0 = cp[oOOG]; q1 = cp[oOOG + PL]; q2 = cp[oOOG + 2 * PL];
+                fo0 = cp[oFO]; fo1 = cp[oFO + PL];
+                foo0 = cp[oFOO]; foo1 = cp[oFOO + PL];
                 if (corr) {
-                    p0 = B[size_t(iG0 + 3 * pa.pred + 0) * PL + go];
-                    p1 = B[size_t(iG0 + 3 * pa.pred + 1) * PL + go];
-                    p2 = B[size_t(iG0 + 3 * pa.pred + 2) * PL + go];
-                    fp0 = B[size_t(iF0 + 2 * pa.pred + 0) * PL + go];
-                    fp1 = B[size_t(iF0 + 2 * pa.pred + 1) * PL + go];
-                    wcur = B[size_t(3 * pa.cur) * PL + go];
+                    p0 = cp[oPR]; p1 = cp[oPR + PL]; p2 = cp[oPR + 2 * PL];
+                    fp0 = cp[oFP]; fp1 = cp[oFP + PL];
+                    wcur = cp[oCUR];
                 }
             }
-            if (MIXED && do3) wlo = B[size_t(9 + 3 * (corr ? pa.cur : pa.in)) * PL + go];
+            if (MIXED && do3) wlo = cp[oLB];
             __syncthreads();  // (A) the previous row step is complete: its oldest ring slot is free
             if (tid == 0 && t + PREFETCH + 2 <= last_row) {
                 fence_proxy_async();
-                issue(t + PREFETCH + 2);
+                issue(t + PREFETCH + 2, sReq);
             }
-            {
-                const unsigned q = row_seq(t + 2);
-                if (!mbar_wait_bounded(&bars[q % RING], (q / RING) & 1u, tma_late ? 1 : (1 << 22))) tma_late = true;
-            }
+            sReq = next_slot(sReq);
+            if (!mbar_wait_bounded(&bars[s2p], par2p, tma_late ? 1 : (1 << 22))) tma_late = true;
+            const int bm = s0 * RSTR + rc, b0 = s1p * RSTR + rc, bp = s2p * RSTR + rc;  // rows t, t+1, t+2
             // ---- faces of row t+1 (Pass1), aux of that row, y flux between rows t and t+1 ----
-            const int s_m = slot(t), s_0 = slot(t + 1), s_p = slot(t + 2);
             Face f;
-            faces_at(rg, s_m, s_0, s_p, rc, c, f);
+            faces_at(ring, bm, b0, bp, c, f);
             const int par1 = (t + 1) & 1;
             fEW[par1][0][tid] = f.hE; fEW[par1][1][tid] = f.uE; fEW[par1][2][tid] = f.vE;
             fEW[par1][3][tid] = f.hW; fEW[par1][4][tid] = f.uW; fEW[par1][5][tid] = f.vW;
@@ -356,14 +378,12 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
                 if (xc >= 1 && xc < nx + 2 && gy >= 1 && gy < ny + 2) {
                     const int cx = xc < 2 ? 2 : xc, cy = gy < 2 ? 2 : gy;
                     if (cx >= x0 && cx < x0 + MO && cy >= y0 && cy < y0 + MH) {
-                        const size_t ai = size_t(gy) * P + xc;
-                        float* a0 = B + size_t(iAUX) * PL + ai;
-                        float* a1 = B + size_t(iAUX + 1) * PL + ai;
-                        const float md = fmaxf((f.hN + f.hE + f.hS + f.hW) / 4.0f, *a0);
-                        float bw = *a1;
+                        float* a0 = B + (size_t(gy) * P + xc) + oAUX;
+                        const float md = fmaxf((f.hN + f.hE + f.hS + f.hW) * 0.25f, a0[0]);
+                        float bw = a0[PL];
                         if (f.msd > M.tan_thr) bw = 1.0f;  // atan(msd) > threshold
-                        *a0 = md;
-                        *a1 = bw * decay;
+                        a0[0] = md;
+                        a0[PL] = bw * decay;
                     }
                 }
             }
@@ -373,12 +393,12 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
                 const float hN = nh, uN = nu, vN = nv;
                 const float hSn = f.hS, uSn = f.uS, vSn = f.vS;
                 const float cN = sqrtf(g * hN), cS = sqrtf(g * hSn);
-                const float bp = fmaxf(fmaxf(vN + cN, vSn + cS), 0.f);
-                const float bm = fminf(fminf(vN - cN, vSn - cS), 0.f);
+                const float bpl = fmaxf(fmaxf(vN + cN, vSn + cS), 0.f);
+                const float bmi = fminf(fminf(vN - cN, vSn - cS), 0.f);
                 const float Fp[3] = {hSn * vSn, hSn * uSn * vSn, hSn * (vSn * vSn + hg * hSn)};
                 const float Fm[3] = {hN * vN, hN * uN * vN, hN * (vN * vN + hg * hN)};
                 const float dU[3] = {hSn - hN, hSn * uSn - hN * uN, hSn * vSn - hN * vN};
-                numflux3(bp, bm, Fp, Fm, dU, yf);
+                numflux3(bpl, bmi, Fp, Fm, dU, yf);
             }
             // ---- x flux at the east face of (xc, t): faces of row t from the previous step ----
             const int par = t & 1;
@@ -398,25 +418,25 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
             __syncthreads();  // (B)
             // ---- Pass3 at (xc, t) ----
             if (do3) {
-                const int r0 = slot(t), rm = slot(t - 1), rp = slot(t + 1);
-                const int rmm = slot(t - 2), rpp = slot(t + 2);
+                const int c0 = s0 * RSTR + rc, cm = s1m * RSTR + rc, cpp1 = s1p * RSTR + rc;
+                const int cmm = s2m * RSTR + rc, cpp2 = s2p * RSTR + rc;   // rows t, t-1, t+1, t-2, t+2
                 const float sl = c.sea_level;
-                const float wc = rg[0][r0][rc], huc = rg[1][r0][rc], hvc = rg[2][r0][rc];
-                const float BAh = rg[3][r0][rc], BXh = rg[4][r0][rc], BYh = rg[5][r0][rc];
-                const float BXw = rg[4][r0][rc - 1], BYs = rg[5][rm][rc];
+                const float wc = W[c0], huc = HU[c0], hvc = HV[c0];
+                const float BAh = BAr[c0], BXh = BXr[c0], BYh = BYr[c0];
+                const float BXw = BXr[c0 - 1], BYs = BYr[cm];
                 const float h = fmaxf(0.f, wc - BAh);
                 const float dh = fmaxf(0.f, sl - BAh), d2 = dh * dh, d3 = d2 * dh;
-                const float dl = fmaxf(0.f, sl - rg[3][r0][rc - 1]), dr = fmaxf(0.f, sl - rg[3][r0][rc + 1]);
-                const float ddn = fmaxf(0.f, sl - rg[3][rm][rc]), du = fmaxf(0.f, sl - rg[3][rp][rc]);
-                const float dll = fmaxf(0.f, sl - rg[3][r0][rc - 2]), drr = fmaxf(0.f, sl - rg[3][r0][rc + 2]);
-                const float ddd = fmaxf(0.f, sl - rg[3][rmm][rc]), duu = fmaxf(0.f, sl - rg[3][rpp][rc]);
+                const float dl = fmaxf(0.f, sl - BAr[c0 - 1]), dr = fmaxf(0.f, sl - BAr[c0 + 1]);
+                const float ddn = fmaxf(0.f, sl - BAr[cm]), du = fmaxf(0.f, sl - BAr[cpp1]);
+                const float dll = fmaxf(0.f, sl - BAr[c0 - 2]), drr = fmaxf(0.f, sl - BAr[c0 + 2]);
+                const float ddd = fmaxf(0.f, sl - BAr[cmm]), duu = fmaxf(0.f, sl - BAr[cpp2]);
                 const float e0 = wc - sl;
-                const float el = rg[0][r0][rc - 1] - sl, er = rg[0][r0][rc + 1] - sl;
-                const float ed = rg[0][rm][rc] - sl, eu = rg[0][rp][rc] - sl;
-                const float ell = rg[0][r0][rc - 2] - sl, err = rg[0][r0][rc + 2] - sl;
-                const float edd = rg[0][rmm][rc] - sl, euu = rg[0][rpp][rc] - sl;
-                const float eul = rg[0][rp][rc - 1] - sl, eur = rg[0][rp][rc + 1] - sl;
-                const float edl = rg[0][rm][rc - 1] - sl, edr = rg[0][rm][rc + 1] - sl;
+                const float el = W[c0 - 1] - sl, er = W[c0 + 1] - sl;
+                const float ed = W[cm] - sl, eu = W[cpp1] - sl;
+                const float ell = W[c0 - 2] - sl, err = W[c0 + 2] - sl;
+                const float edd = W[cmm] - sl, euu = W[cpp2] - sl;
+                const float eul = W[cpp1 - 1] - sl, eur = W[cpp1 + 1] - sl;
+                const float edl = W[cm - 1] - sl, edr = W[cm + 1] - sl;
                 const float odx = c.one_over_dx, ody = c.one_over_dy;
                 const float od2x = odx * odx, od3x = od2x * odx, od2y = ody * ody, od3y = od2y * ody;
                 const float ddx = (-drr + 8 * dr - 8 * dl + dll) * odx * (1.0f / 12.0f);
@@ -438,10 +458,10 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
                 const float f1 = (xb[par][1][tid - 1] - xb[par][1][tid]) * odx + (ypv1 - yf[1]) * ody + s1;
                 const float f2 = (xb[par][2][tid - 1] - xb[par][2][tid]) * odx + (ypv2 - yf[2]) * ody + s2;
                 const float sixth = 1.0f / 6.0f;
-                const float Fs = (sixth * dh * (ddx * ((ody * 0.5f) * (rg[2][rp][rc] - rg[2][rm][rc])) +
-                                                (ddy * ((odx * 0.5f) * (rg[2][r0][rc + 1] - rg[2][r0][rc - 1])))));
-                const float Gs = (sixth * dh * (ddx * ((ody * 0.5f) * (rg[1][rp][rc] - rg[1][rm][rc])) +
-                                                (ddy * ((odx * 0.5f) * (rg[1][r0][rc + 1] - rg[1][r0][rc - 1])))));
+                const float Fs = (sixth * dh * (ddx * ((ody * 0.5f) * (HV[cpp1] - HV[cm])) +
+                                                (ddy * ((odx * 0.5f) * (HV[c0 + 1] - HV[c0 - 1])))));
+                const float Gs = (sixth * dh * (ddx * ((ody * 0.5f) * (HU[cpp1] - HU[cm])) +
+                                                (ddy * ((odx * 0.5f) * (HU[c0 + 1] - HU[c0 - 1])))));
                 const float dt = dtm;
                 float dw, rhu, rhv;
                 float wbase = wc;
@@ -462,15 +482,12 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
                 float wn = wbase, wl = wlo;
                 if (MIXED) two_sum_add(wn, wl, dw);
                 else wn = wbase + dw;
-                B[size_t(3 * pa.out) * PL + go] = wn;
-                if (MIXED) B[size_t(9 + 3 * pa.out) * PL + go] = wl;
-                B[size_t(iR0) * PL + go] = rhu;
-                B[size_t(iR0 + 1) * PL + go] = rhv;
-                B[size_t(iG0 + 3 * pa.scr + 0) * PL + go] = f0;
-                B[size_t(iG0 + 3 * pa.scr + 1) * PL + go] = f1;
-                B[size_t(iG0 + 3 * pa.scr + 2) * PL + go] = f2;
-                B[size_t(iF0 + 2 * pa.scr + 0) * PL + go] = Fs;
-                B[size_t(iF0 + 2 * pa.scr + 1) * PL + go] = Gs;
+                cp[oOUT] = wn;
+                if (MIXED) cp[oLO] = wl;
+                cp[oR] = rhu;
+                cp[oR + PL] = rhv;
+                cp[oSCR] = f0; cp[oSCR + PL] = f1; cp[oSCR + 2 * PL] = f2;
+                cp[oFS] = Fs; cp[oFS + PL] = Gs;
                 // GetStats (compute.hlsl:1319-1378) of the input state, FP64 accumulation
                 const float q = div_by_h_fast(h, c.epsilon);
                 const float u = q * huc, v = q * hvc;
@@ -484,10 +501,14 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
                     mx[3] = fmaxf(mx[3], u2v2 * q);
                 }
                 acc[5] += h;
-                bad = bad || !isfinite(wc) || !isfinite(huc) || !isfinite(hvc);
+                bad = bad || !(fabsf(wn) <= 3.0e38f) || !(fabsf(rhu) <= 3.0e38f) || !(fabsf(rhv) <= 3.0e38f);
             }
             ypv0 = yf[0]; ypv1 = yf[1]; ypv2 = yf[2];
             nh = f.hN; nu = f.uN; nv = f.vN;
+            // advance the ring window: rows t-1 .. t+3 become t-2 .. t+2
+            s2m = s1m; s1m = s0; s0 = s1p; s1p = s2p;
+            s2p = next_slot(s2p);
+            if (s2p == 0) par2p ^= 1u;
         }
         seq = seq0 + unsigned(last_row - (y0 - 2) + 1);
         // ---- zero the ghost ring of the output state next to this strip (engine.cpp:1007) ----
@@ -500,10 +521,10 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
             for (int k = tid; k < w * (cy1 - cy0); k += MW) {
                 const int gx = cx0 + k % w, gy = cy0 + k / w;
                 if (gx >= 2 && gx < nx + 2 && gy >= 2 && gy < ny + 2) continue;
-                const size_t gz = size_t(gy) * P + gx;
+                float* gz = B + (size_t(gy) * P + gx);
                 for (int q = 0; q < 3; ++q) {
-                    B[size_t(3 * pa.out + q) * PL + gz] = 0.f;
-                    if (MIXED) B[size_t(9 + 3 * pa.out + q) * PL + gz] = 0.f;
+                    gz[oOUT + q * PL] = 0.f;
+                    if (MIXED) gz[oLO + q * PL] = 0.f;
                 }
             }
         }
