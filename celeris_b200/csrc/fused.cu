@@ -1003,6 +1003,8 @@ struct cel_batch {
     std::vector<void*> allocs;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t side = nullptr;       // second stream: the column solve runs beside the row solve
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cel::KernelTimer tm;
     cel::Scheme sch;      // shared pass sequence (all members use the same correction count)
     cel::Idx ix;
@@ -1106,21 +1108,27 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
         else
             k_march<false><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
     }
+    // the row (x) and column (y) solves are independent: fork the column solve onto the side
+    // stream and join before the boundaries (a fork/join pair inside the captured graph)
+    B_TRY(cudaEventRecord(b->ev_fork, b->stream));
+    B_TRY(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+    {
+        TimedLaunch t(&b->tm, b->side, "tridiag_cols");
+        if (b->cw == 16) {
+            if (b->mixed) k_cols<true, 16><<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+            else k_cols<false, 16><<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+        } else {
+            if (b->mixed) k_cols<true, 8><<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+            else k_cols<false, 8><<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+        }
+    }
     {
         TimedLaunch t(&b->tm, b->stream, "tridiag_rows");
         if (b->mixed) k_rows<true><<<b->grid_rows, NTR, b->smem_rows, b->stream>>>(b->ddev, b->rows, b->nrows, pa);
         else k_rows<false><<<b->grid_rows, NTR, b->smem_rows, b->stream>>>(b->ddev, b->rows, b->nrows, pa);
     }
-    {
-        TimedLaunch t(&b->tm, b->stream, "tridiag_cols");
-        if (b->cw == 16) {
-            if (b->mixed) k_cols<true, 16><<<b->grid_cols, NTC, b->smem_cols, b->stream>>>(b->ddev, b->bands, b->nbands, pa);
-            else k_cols<false, 16><<<b->grid_cols, NTC, b->smem_cols, b->stream>>>(b->ddev, b->bands, b->nbands, pa);
-        } else {
-            if (b->mixed) k_cols<true, 8><<<b->grid_cols, NTC, b->smem_cols, b->stream>>>(b->ddev, b->bands, b->nbands, pa);
-            else k_cols<false, 8><<<b->grid_cols, NTC, b->smem_cols, b->stream>>>(b->ddev, b->bands, b->nbands, pa);
-        }
-    }
+    B_TRY(cudaEventRecord(b->ev_join, b->side));
+    B_TRY(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
     for (int side : {1, 0, 3, 2}) {
         if (b->nbitems[side] == 0) continue;
         const int g = std::min(b->nbitems[side], b->sms * 8);
@@ -1252,7 +1260,13 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { err = "no CUDA device"; return nullptr; }
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { err = "stream creation failed"; return nullptr; }
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        err = "stream creation failed";
+        return nullptr;
+    }
     b->own_stream = true;
     b->mem.resize(n);
     b->hdev.resize(n);
@@ -1471,9 +1485,13 @@ void batch_destroy(cel_batch* b) {
     if (!b) return;
     free_graphs(b);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->side) cudaStreamSynchronize(b->side);
     for (void* a : b->allocs) cudaFree(a);
     if (b->dt_host) cudaFreeHost(b->dt_host);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
     delete b;
 }
 
