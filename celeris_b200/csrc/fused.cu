@@ -197,13 +197,14 @@ __device__ __forceinline__ float div_by_h_fast(float h, float eps) {
 __device__ __forceinline__ void numflux3(float ap, float am, const float Fp[3], const float Fm[3], const float dU[3],
                                          float out[3]) {
     const float den = ap - am;
-    const float inv = den != 0.f ? __frcp_rn(den) : 0.f;
+    const float inv = den != 0.f ? __fdividef(1.0f, den) : 0.f;
     const float apam = ap * am;
 #pragma unroll
     for (int k = 0; k < 3; ++k) out[k] = (ap * Fm[k] - am * Fp[k] + apam * dU[k]) * inv;
 }
 __device__ __forceinline__ float friction_fast(float hu, float hv, float h, float friction, int manning, float g,
                                               float eps) {
+    if (friction == 0.f) return 0.f;   // both friction laws vanish with a zero coefficient
     const float h2 = h * h, h4 = h2 * h2;
     const float dbh = 1.41421354f * h * rsqrtf(h4 + fmaxf(h4, eps));
     float f = friction;
@@ -212,6 +213,28 @@ __device__ __forceinline__ float friction_fast(float hu, float hv, float h, floa
 }
 
 struct Face { float hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, msd; };
+
+// Reconstruct with the breaking-indicator standard deviation, divisions by 3 as products
+__device__ __forceinline__ void reconstruct_sd_fast(float tt, float w, float c, float e, float& ow, float& oe, float& sd) {
+    const float z1 = tt * (c - w), z2 = e - w, z3 = tt * (e - c);
+    const float g2 = 0.25f * minmod3(z1, z2, z3);
+    const float mu = (0.5f / 3.0f) * (z1 + z2 + z3);
+    sd = sqrtf(((z1 - mu) * (z1 - mu) + (z2 - mu) * (z2 - mu) + (z3 - mu) * (z3 - mu)) * (1.0f / 3.0f));
+    oe = c + g2;
+    ow = c - g2;
+}
+
+// Kahan-compensated single-precision accumulator (statistics without per-cell FP64 work)
+struct Kahan {
+    float s = 0.f, c = 0.f;
+    __device__ __forceinline__ void add(float x) {
+        const float y = x - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return double(s) - double(c); }
+};
 
 // Ring layout: field f, slot s, column k at ring[f * FSTR + s * RSTR + k]; a "row base" is
 // s * RSTR + (this thread's column), so every access is base + compile-time offset.
@@ -228,8 +251,8 @@ __device__ __forceinline__ void faces_at(const float* __restrict__ ring, int bm,
     const float wc = W[b0], wl = W[b0 - 1], wr = W[b0 + 1], wd = W[bm], wu = W[bp];
     const float BN = BYr[b0], BE = BXr[b0], BS = BYr[bm], BW = BXr[b0 - 1];
     float wN, wE, wS, wW, huN, huE, huS, huW, hvN, hvE, hvS, hvW, sd1, sd2;
-    reconstruct_sd(c.two_theta, wl, wc, wr, wW, wE, sd1);
-    reconstruct_sd(c.two_theta, wd, wc, wu, wS, wN, sd2);
+    reconstruct_sd_fast(c.two_theta, wl, wc, wr, wW, wE, sd1);
+    reconstruct_sd_fast(c.two_theta, wd, wc, wu, wS, wN, sd2);
     const float huc = HU[b0], hvc = HV[b0];
     reconstruct(c.two_theta, HU[b0 - 1], huc, HU[b0 + 1], huW, huE);
     reconstruct(c.two_theta, HU[bm], huc, HU[bp], huS, huN);
@@ -311,7 +334,7 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
         };
         auto next_slot = [](int s) { return s + 1 == RING ? 0 : s + 1; };
 
-        double acc[6] = {0, 0, 0, 0, 0, 0};
+        Kahan acc[6];
         float mx[4] = {0.f, 0.f, 0.f, 0.f};
         bool bad = false;
         float nh = 0.f, nu = 0.f, nv = 0.f;       // north face of the previous row (this column)
@@ -492,15 +515,15 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
                 const float q = div_by_h_fast(h, c.epsilon);
                 const float u = q * huc, v = q * hvc;
                 if (xc < 2 + 4 * (nx / 4) && t < 2 + 4 * (ny / 4)) {
-                    acc[0] += h; acc[1] += double(h * (BAh + 0.5f * h)); acc[2] += huc; acc[3] += hvc;
-                    acc[4] += double(huc * u + hvc * v);
+                    acc[0].add(h); acc[1].add(h * (BAh + 0.5f * h)); acc[2].add(huc); acc[3].add(hvc);
+                    acc[4].add(huc * u + hvc * v);
                     const float u2v2 = u * u + v * v;
                     const float cc = sqrtf(c.g * h);
                     mx[0] = fmaxf(mx[0], u2v2); mx[1] = fmaxf(mx[1], h);
                     mx[2] = fmaxf(mx[2], fmaxf((fabsf(u) + cc) * c.one_over_dx, (fabsf(v) + cc) * c.one_over_dy));
                     mx[3] = fmaxf(mx[3], u2v2 * q);
                 }
-                acc[5] += h;
+                acc[5].add(h);
                 bad = bad || !(fabsf(wn) <= 3.0e38f) || !(fabsf(rhu) <= 3.0e38f) || !(fabsf(rhv) <= 3.0e38f);
             }
             ypv0 = yf[0]; ypv1 = yf[1]; ypv2 = yf[2];
@@ -531,7 +554,7 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
         // ---- strip statistics -> member accumulators ----
         {
             double sv[STATS_N];
-            for (int k = 0; k < 6; ++k) sv[k] = acc[k];
+            for (int k = 0; k < 6; ++k) sv[k] = acc[k].value();
             for (int k = 0; k < 4; ++k) sv[6 + k] = mx[k];
             sv[10] = bad ? 1.0 : 0.0;
             sv[11] = tma_late ? 1.0 : 0.0;
