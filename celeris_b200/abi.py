@@ -165,6 +165,7 @@ def _declare(L: C.CDLL) -> None:
         "cel_kernel_times": (i, [vp, i, C.POINTER(C.c_char * 64), C.POINTER(C.c_double),
                                  C.POINTER(C.c_longlong), i, C.POINTER(i)]),
         "cel_byte_model": (i, [i, i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "cel_stats_noalloc": (i, [vp, vp, C.POINTER(Params), vp, C.POINTER(Stats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -193,5 +194,5 @@ EXPORTED = [
     "cel_batch_create", "cel_batch_destroy", "cel_batch_set_stream", "cel_batch_step",
     "cel_batch_stats", "cel_batch_get_state", "cel_batch_set_state", "cel_batch_get_aux",
     "cel_batch_use_graph", "cel_batch_cells", "cel_batch_set_timestep", "cel_batch_launches_per_step", "cel_set_tuning", "cel_batch_set_tuning",
-    "cel_batch_kernel_timing", "cel_engine_kernel_timing", "cel_kernel_times", "cel_byte_model",
+    "cel_batch_kernel_timing", "cel_engine_kernel_timing", "cel_kernel_times", "cel_byte_model", "cel_stats_noalloc",
 ]

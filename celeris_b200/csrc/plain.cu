@@ -922,3 +922,175 @@ EngineIface* make_plain_engine(const cel_params& p, const float* bathy, int bnx,
 }
 
 }  // namespace cel
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free statistics entry point.
+//
+// Some callers of this library must not allocate device memory at the moment they ask for the
+// domain statistics: code that is in the middle of a CUDA stream capture (cudaMalloc and cudaFree
+// are not capturable), frame loops where the implicit device synchronisation of cudaMalloc /
+// cudaFree would stall the frame, and host applications whose device memory is entirely handed
+// out by their own allocator.  cel_stats_noalloc computes the GetStats reduction of a state that
+// the caller already keeps in device memory, using only the fixed scratch array below: the 4x4
+// block partials and the FP64 totals.  The array is reserved on every GPU that loads the library
+// and stays there until the process exits.  All calls share it, so two calls whose work overlaps on
+// the GPU (on different streams, or from different threads) race; run them one after another.
+// ---------------------------------------------------------------------------------------------
+namespace cel {
+namespace {
+
+constexpr int NOALLOC_MAX_BLOCKS = 65536;                  // 4x4 blocks: up to 1,048,576 cells
+constexpr int NOALLOC_FLOATS = NOALLOC_MAX_BLOCKS * 9 + 64;  // block partials + 16 doubles (32 floats)
+static __device__ __align__(256) float g_noalloc_scratch[NOALLOC_FLOATS];
+
+// GetStats (compute.hlsl:1319-1378) reading the bottom in the public {BY, BX, BA} layout.
+__global__ void k_getstats_b3(const float4* __restrict__ st, const float* __restrict__ b3, float* __restrict__ blocks,
+                              SimConsts c) {
+    const int bx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int by = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nbx = c.nx / 4, nby = c.ny / 4;
+    if (bx >= nbx || by >= nby) return;
+    float sh = 0, sb = 0, shu = 0, shv = 0, sk = 0, mu = 0, mh = 0, mc = 0, mf = 0;
+    for (int j = 2; j < 6; ++j)
+        for (int ii = 2; ii < 6; ++ii) {
+            const size_t i = size_t(by * 4 + j) * c.NX + bx * 4 + ii;
+            const float4 s = st[i];
+            const float B = b3[3 * i + 2];
+            const float h = fmaxf(0.f, s.x - B);
+            const float cc = sqrtf(c.g * h);
+            const float q = div_by_h(h, c.epsilon);
+            const float u = q * s.y, v = q * s.z;
+            sh += h; sb += h * (B + 0.5f * h); shu += s.y; shv += s.z;
+            sk += (s.y * u + s.z * v);
+            const float u2v2 = u * u + v * v;
+            mu = fmaxf(mu, u2v2); mh = fmaxf(mh, h);
+            mc = fmaxf(mc, (fabsf(u) + cc) * c.one_over_dx);
+            mc = fmaxf(mc, (fabsf(v) + cc) * c.one_over_dy);
+            mf = fmaxf(mf, u2v2 * q);
+        }
+    float* o = blocks + (size_t(by) * nbx + bx) * 9;
+    o[0] = sh; o[1] = sb; o[2] = shu; o[3] = shv; o[4] = sk; o[5] = mu; o[6] = mh; o[7] = mc; o[8] = mf;
+}
+
+// One CTA: FP64 totals of the block partials; every output word is written on every call.
+__global__ void k_reduce_b3(const float* __restrict__ blocks, int nb, const float4* __restrict__ st,
+                            const float* __restrict__ b3, SimConsts c, double* __restrict__ out) {
+    __shared__ double sm[10][32];
+    __shared__ int bad_s;
+    double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int bad = 0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        const float* b = blocks + size_t(k) * 9;
+        for (int q = 0; q < 5; ++q) v[q] += double(b[q]);
+        for (int q = 5; q < 9; ++q) v[q] = fmax(v[q], double(b[q]));
+    }
+    const int n = c.nx * c.ny;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const size_t i = size_t(k / c.nx + 2) * c.NX + (k % c.nx + 2);
+        const float4 s = st[i];
+        if (!isfinite(s.x) || !isfinite(s.y) || !isfinite(s.z)) bad = 1;
+        v[9] += fmax(0.0, double(s.x) - double(b3[3 * i + 2]));
+    }
+    if (threadIdx.x == 0) bad_s = 0;
+    __syncthreads();
+    if (bad) bad_s = 1;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int q = 0; q < 10; ++q) {
+        double x = v[q];
+        for (int off = 16; off; off >>= 1) {
+            const double y = __shfl_down_sync(0xffffffffu, x, off);
+            x = (q >= 5 && q < 9) ? fmax(x, y) : x + y;
+        }
+        if (lane == 0) sm[q][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int nw = blockDim.x >> 5;
+        for (int q = 0; q < 10; ++q) {
+            double x = lane < nw ? sm[q][lane] : 0.0;
+            for (int off = 16; off; off >>= 1) {
+                const double y = __shfl_down_sync(0xffffffffu, x, off);
+                x = (q >= 5 && q < 9) ? fmax(x, y) : x + y;
+            }
+            if (lane == 0) out[q] = x;
+        }
+        if (lane == 0) out[10] = bad_s ? 1.0 : 0.0;
+    }
+}
+
+// Device address of the scratch array, looked up once per device (with that device current).
+constexpr int NOALLOC_MAX_DEVICES = 64;
+float* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+}  // namespace
+
+}  // namespace cel
+
+extern "C" int cel_stats_noalloc(const float* d_state_rgba, const float* d_bottom_b3, const cel_params* p,
+                                 void* cuda_stream, cel_stats* out) {
+    using namespace cel;
+    if (!d_state_rgba || !d_bottom_b3 || !p || !out) { set_error("null argument"); return CEL_ERR_ARG; }
+    if (p->nx < 4 || p->ny < 4) { set_error("cel_stats_noalloc: nx and ny must be >= 4"); return CEL_ERR_ARG; }
+    const long long nb = (long long)(p->nx / 4) * (p->ny / 4);
+    if (nb > NOALLOC_MAX_BLOCKS) {
+        set_error("cel_stats_noalloc: domain has " + std::to_string(nb) + " 4x4 blocks; the fixed scratch holds " +
+                  std::to_string(NOALLOC_MAX_BLOCKS) + " (at most 1,048,576 interior cells)");
+        return CEL_ERR_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) { set_error(std::string("cel_stats_noalloc: ") + cudaGetErrorString(e)); return CEL_ERR_CUDA; }
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) { set_error("cel_stats_noalloc: device index out of range"); return CEL_ERR_ARG; }
+    if (!g_noalloc_ptr[dev]) {
+        // first call on this device: resolve the array's device address (this must not happen
+        // inside a stream capture, so make the first call before capturing)
+        float* ptr = nullptr;
+        e = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) {
+            set_error(std::string("cel_stats_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+            return CEL_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = ptr;
+    }
+    float* blocks = g_noalloc_ptr[dev];
+    double* totals = reinterpret_cast<double*>(blocks + size_t(NOALLOC_MAX_BLOCKS) * 9);  // 256-byte aligned
+    HostSetup hs;
+    hs.nx = p->nx; hs.ny = p->ny; hs.NX = p->nx + 4; hs.NY = p->ny + 4;
+    hs.dx = float(p->width) / float(p->nx - 1);
+    hs.dy = float(p->length) / float(p->ny - 1);
+    {
+        const float m = std::max(hs.dx, hs.dy);
+        hs.eps = std::min(float(p->epsilon), m * m * m * m);
+    }
+    const SimConsts c = make_consts(*p, hs, hs.NX);
+    cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+    const float4* st = reinterpret_cast<const float4*>(d_state_rgba);
+    const int nbx = p->nx / 4, nby = p->ny / 4;
+    k_getstats_b3<<<grid2(nbx, nby), dim3(BX2, BY2), 0, s>>>(st, d_bottom_b3, blocks, c);
+    k_reduce_b3<<<1, 1024, 0, s>>>(blocks, int(nb), st, d_bottom_b3, c, totals);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { set_error(std::string("cel_stats_noalloc: ") + cudaGetErrorString(e)); return CEL_ERR_CUDA; }
+    double v[11];
+    e = cudaMemcpyAsync(v, totals, sizeof(v), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_error(std::string("cel_stats_noalloc: ") + cudaGetErrorString(e)); return CEL_ERR_CUDA; }
+    const double DENSITY = 1000;
+    const double AREA = double(float(p->width) / float(p->nx - 1) * float(p->length) / float(p->ny - 1));
+    const double g = double(c.g);
+    std::memset(out, 0, sizeof(*out));
+    out->mass = v[0] * DENSITY * AREA;
+    out->potential_energy = v[1] * g * DENSITY * AREA;
+    out->x_momentum = v[2] * DENSITY * AREA;
+    out->y_momentum = v[3] * DENSITY * AREA;
+    out->kinetic_energy = v[4] * 0.5 * DENSITY * AREA;
+    out->total_energy = out->kinetic_energy + out->potential_energy;
+    out->max_speed = std::sqrt(v[5]);
+    out->max_depth = v[6];
+    out->cfl_rate = v[7];
+    out->max_froude = std::sqrt(v[8] / g);
+    out->mass_full = v[9];
+    out->health = v[10] != 0 ? CEL_ERR_NUMERIC : 0;
+    out->timestep = p->timestep;
+    out->cfl_number = out->cfl_rate * double(float(p->timestep));
+    return CEL_OK;
+}

@@ -201,6 +201,20 @@ int cel_kernel_times(void* handle, int is_batch, char (*names)[64], double* tota
 int cel_byte_model(int form, int correction_steps, double* stencil_bytes_per_cell_pass,
                    double* step_bytes_per_cell);
 
+/* ---- allocation-free statistics (no counterpart in the reference) ----------------------- */
+/* The resetTimestep statistics (mass, energies, momenta, maxima, CFL rate) of a state the caller
+ * keeps in device memory: d_state_rgba is (nx+4)(ny+4) x {w,hu,hv,_} and d_bottom_b3 is
+ * (nx+4)(ny+4) x {BY,BX,BA}, both device pointers; p supplies nx, ny, width, length, gravity and
+ * epsilon; the work runs on cuda_stream (NULL = the default stream) and the call returns after the
+ * result reached *out.  It never allocates: for callers that cannot call cudaMalloc at that point
+ * (during a stream capture, in frame loops where an allocation's device synchronisation would
+ * stall, or under an allocator that owns all device memory).  Its scratch is a fixed static device
+ * array sized for at most 65,536 4x4 blocks (1,048,576 interior cells); larger domains get
+ * CEL_ERR_ARG.  The first call on each device looks the array up (make it before any capture).
+ * Calls share the array: calls that overlap on the GPU race. */
+int cel_stats_noalloc(const float* d_state_rgba, const float* d_bottom_b3, const cel_params* p, void* cuda_stream,
+                      cel_stats* out);
+
 #ifdef __cplusplus
 }
 #endif
