@@ -85,6 +85,22 @@ __device__ __forceinline__ float friction_calc(float hu, float hv, float h, floa
     return f * sqrtf(hu * hu + hv * hv) * dbh * dbh;
 }
 
+// Source texel of a solid-wall ghost cell (compute.hlsl:985-1009).  The shaders mirror with
+// `4 - tex_idx` and `reflect - tex_idx` (reflect = 2n+2, engine.cpp:1308-1309) where tex_idx is
+// the interpolated pixel coordinate x + 0.5 (engine.cpp:579), and int3() truncates toward zero:
+// the west/south ghosts read 3 - x, the east/north ghosts read 2n + 1 - x.  A source outside the
+// texture reads zero.
+__host__ __device__ __forceinline__ int solid_mirror(int c, int x) {
+    return int(float(c) - (float(x) + 0.5f));
+}
+__host__ __device__ __forceinline__ void solid_source(int side, int x, int y, int nx, int ny, int& qx, int& qy) {
+    qx = x; qy = y;
+    if (side == 3) qx = solid_mirror(4, x);
+    else if (side == 1) qx = solid_mirror(2 * nx + 2, x);
+    else if (side == 2) qy = solid_mirror(4, y);
+    else qy = solid_mirror(2 * ny + 2, y);
+}
+
 // SpongeFunction (compute.hlsl:1056-1059)
 __device__ __forceinline__ float sponge_fn(float L, float x) {
     return 0.5f + 0.5f * t_cos(CEL_PI_F * fmaxf(L - x, 0.f) / L);

@@ -923,11 +923,8 @@ __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ 
         const double t64 = *M.time64;
         const float t32 = *M.time32;
         if (b.type == CEL_BC_SOLID) {
-            int qx = x, qy = y;
-            if (side == 3) qx = 4 - x;
-            else if (side == 1) qx = (2 * c.nx + 2) - x;
-            else if (side == 2) qy = 4 - y;
-            else qy = (2 * c.ny + 2) - y;
+            int qx, qy;
+            solid_source(side, x, y, c.nx, c.ny, qx, qy);
             float sw_ = 0.f, su = 0.f, sv = 0.f, lw_ = 0.f, lu_ = 0.f, lv_ = 0.f;
             if (qx >= 0 && qy >= 0 && qx < NX && qy < NY) {
                 const size_t qi = size_t(qy) * P + qx;
@@ -1417,7 +1414,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
             }
             const int cellsn = (s == 0 || s == 2) ? NX * std::min(bb.width, NY) : std::min(bb.width, NX) * NY;
             for (int c0 = 0; c0 < cellsn; c0 += 256) bitems[s].push_back(make_int2(i, c0));
-            if (bb.type == CEL_BC_SOLID && bb.width >= 4) b->two_phase[s] = true;
+            // a solid strip wider than 2 reads ghost cells of its own strip: compute, then write
+            if (bb.type == CEL_BC_SOLID && bb.width >= 3) b->two_phase[s] = true;
         }
         {
             size_t strip = 0;

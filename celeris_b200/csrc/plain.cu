@@ -349,11 +349,8 @@ __global__ void k_boundary(const float4* __restrict__ st, const float4* __restri
     float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
     const float sl = b.sea_level;
     if (b.type == CEL_BC_SOLID) {
-        int qx = x, qy = y;
-        if (b.side == 3) qx = 4 - x;
-        else if (b.side == 1) qx = (2 * c.nx + 2) - x;
-        else if (b.side == 2) qy = 4 - y;
-        else qy = (2 * c.ny + 2) - y;
+        int qx, qy;
+        solid_source(b.side, x, y, c.nx, c.ny, qx, qy);
         float4 s = make_float4(0.f, 0.f, 0.f, 0.f);  // out-of-range texture loads read zero
         if (qx >= 0 && qy >= 0 && qx < NX && qy < NY) s = st[size_t(qy) * NX + qx];
         o.x = s.x;

@@ -411,7 +411,9 @@ public:
     R g_() const { return R(p.gravity); }
 
     // ---- Pass1 (compute.hlsl:380-458), region [1,nx+3) x [1,ny+3) -------------------------
-    void pass1(const std::vector<T4>& st) {
+    virtual ~Engine() = default;
+
+    virtual void pass1(const std::vector<T4>& st) {
         const R odx = R(1) / dx, ody = R(1) / dy;
         const R thr = R(p.dissipation_threshold);
 #pragma omp parallel for schedule(static)
@@ -448,7 +450,7 @@ public:
     }
 
     // ---- Pass2 (compute.hlsl:470-542), region [1,nx+2) x [1,ny+2) -------------------------
-    void pass2() {
+    virtual void pass2() {
         const R g = g_(), half_g = R(0.5) * g;
         const R decay = R(1) / (R(1) + R(2) * R(p.whitewater_decay));
         const R decay_dt = t_pow(std::abs(decay), dt_());
@@ -511,7 +513,7 @@ public:
     }
 
     // ---- Pass3Predictor (compute.hlsl:616-812), region [2,nx+2) x [2,ny+2) ----------------
-    void pass3(const std::vector<T4>& st, std::vector<T4>& out, std::vector<T4>& sgrad, std::vector<T4>& sfg) {
+    virtual void pass3(const std::vector<T4>& st, std::vector<T4>& out, std::vector<T4>& sgrad, std::vector<T4>& sfg) {
         const R g = g_();
         const R odx = R(1) / dx, ody = R(1) / dy;
         const R gdx = g / dx, gdy = g / dy;
@@ -616,7 +618,7 @@ public:
     }
 
     // ---- Cyclic reduction (compute.hlsl:835-947, engine.cpp:1060-1217) --------------------
-    void cr_solve_x(const std::vector<T4>& rhs) {
+    virtual void cr_solve_x(const std::vector<T4>& rhs) {
         // reduce: D1x[k] from level k-1 (level-0 RHS is the new-state texture .g)
         for (int k = 1; k < Kx; ++k) {
             const int Wp = (k == 1) ? NX : lenx[k - 1] + 4, Wk = lenx[k] + 4;
@@ -661,7 +663,7 @@ public:
                 }
         }
     }
-    void cr_solve_y(const std::vector<T4>& rhs) {
+    virtual void cr_solve_y(const std::vector<T4>& rhs) {
         for (int k = 1; k < Ky; ++k) {
             const std::vector<T4>& Dp = (k == 1) ? rhs : D1y[k - 1];
             const std::vector<T4>& Ap = ABCy[k - 1];
@@ -746,7 +748,7 @@ public:
 
     // One side: 0=N,1=E,2=S,3=W (engine.cpp:1339 naming).  Computes the strip from the state
     // as it is before this side (render-to-scratch), then writes the strip back.
-    void boundary_side(std::vector<T4>& st, int side) {
+    virtual void boundary_side(std::vector<T4>& st, int side) {
         const Boundary& b = side == 0 ? p.north : side == 1 ? p.east : side == 2 ? p.south : p.west;
         int x0, x1, y0, y1;
         if (side == 0) { x0 = 0; x1 = NX; y0 = NY - b.width; y1 = NY; }
@@ -768,11 +770,15 @@ public:
             for (int x = x0; x < x1; ++x) {
                 T4 o;
                 if (b.type == B_SOLID) {
+                    // compute.hlsl:985-1009: `4 - tex_idx` / `reflect - tex_idx` (reflect = 2n+2,
+                    // engine.cpp:1308) with tex_idx = x + 0.5 at the pixel centre (engine.cpp:579),
+                    // truncated toward zero by int3(): west/south read 3 - x, east/north 2n + 1 - x.
+                    auto mirror = [](int c, int q) { return int(float(c) - (float(q) + 0.5f)); };
                     int sx = x, sy = y;
-                    if (side == 3) sx = 4 - x;
-                    else if (side == 1) sx = (2 * nx + 2) - x;
-                    else if (side == 2) sy = 4 - y;
-                    else sy = (2 * ny + 2) - y;
+                    if (side == 3) sx = mirror(4, x);
+                    else if (side == 1) sx = mirror(2 * nx + 2, x);
+                    else if (side == 2) sy = mirror(4, y);
+                    else sy = mirror(2 * ny + 2, y);
                     T4 s;
                     if (inb(sx, sy, NX, NY)) s = st[at(sx, sy)];
                     o.r = s.r;
@@ -823,33 +829,43 @@ public:
             for (int x = x0; x < x1; ++x) st[at(x, y)] = strip[size_t(y - y0) * (x1 - x0) + (x - x0)];
     }
 
-    // ---- GetStats (compute.hlsl:1319-1378) + resetTimestep (engine.cpp:1536-1756) ---------
+    // ---- GetStats (compute.hlsl:1319-1378): one 4x4 block --------------------------------
+    // o = {sum h, sum h(B+h/2), sum hu, sum hv, sum (hu u + hv v), max u^2+v^2, max h, max cfl,
+    //      max (u^2+v^2)/h}
+    virtual void stats_block(const std::vector<T4>& st, int bx, int by, R o[9]) const {
+        const R g = g_(), odx = R(1) / dx, ody = R(1) / dy;
+        R sh = 0, sb = 0, shu = 0, shv = 0, sk = 0, mu = 0, mh = 0, mc = 0, mf2 = 0;
+        for (int j = 2; j < 6; ++j)
+            for (int i = 2; i < 6; ++i) {
+                const int x = bx * 4 + i, y = by * 4 + j;
+                const T4 s = st[at(x, y)];
+                const R B = BA[at(x, y)];
+                const R h = std::max(R(0), s.r - B);
+                const R c = std::sqrt(g * h);
+                const R q = div_by_h(h);
+                const R u = q * s.g, v = q * s.b;
+                sh += h; sb += h * (B + R(0.5) * h); shu += s.g; shv += s.b;
+                sk += (s.g * u + s.b * v);
+                const R u2v2 = u * u + v * v;
+                mu = std::max(mu, u2v2); mh = std::max(mh, h);
+                mc = std::max(mc, (std::abs(u) + c) * odx);
+                mc = std::max(mc, (std::abs(v) + c) * ody);
+                mf2 = std::max(mf2, u2v2 * q);
+            }
+        o[0] = sh; o[1] = sb; o[2] = shu; o[3] = shv; o[4] = sk; o[5] = mu; o[6] = mh; o[7] = mc; o[8] = mf2;
+    }
+
+    // ---- resetTimestep (engine.cpp:1536-1756) ----------------------------------------------
     Stats reset_timestep() {
         const std::vector<T4>& st = state[sim_idx];
-        const R g = g_(), odx = R(1) / dx, ody = R(1) / dy;
+        const R g = g_();
         R mass = 0, xm = 0, ym = 0, ke = 0, pe = 0, ms = 0, md = 0, cfl = 0, mf = 0;
         for (int by = 0; by < ny / 4; ++by)
             for (int bx = 0; bx < nx / 4; ++bx) {
-                R sh = 0, sb = 0, shu = 0, shv = 0, sk = 0, mu = 0, mh = 0, mc = 0, mf2 = 0;
-                for (int j = 2; j < 6; ++j)
-                    for (int i = 2; i < 6; ++i) {
-                        const int x = bx * 4 + i, y = by * 4 + j;
-                        const T4 s = st[at(x, y)];
-                        const R B = BA[at(x, y)];
-                        const R h = std::max(R(0), s.r - B);
-                        const R c = std::sqrt(g * h);
-                        const R q = div_by_h(h);
-                        const R u = q * s.g, v = q * s.b;
-                        sh += h; sb += h * (B + R(0.5) * h); shu += s.g; shv += s.b;
-                        sk += (s.g * u + s.b * v);
-                        const R u2v2 = u * u + v * v;
-                        mu = std::max(mu, u2v2); mh = std::max(mh, h);
-                        mc = std::max(mc, (std::abs(u) + c) * odx);
-                        mc = std::max(mc, (std::abs(v) + c) * ody);
-                        mf2 = std::max(mf2, u2v2 * q);
-                    }
-                mass += sh; pe += sb; xm += shu; ym += shv; ke += sk;
-                ms = std::max(ms, mu); md = std::max(md, mh); cfl = std::max(cfl, mc); mf = std::max(mf, mf2);
+                R o[9];
+                stats_block(st, bx, by, o);
+                mass += o[0]; pe += o[1]; xm += o[2]; ym += o[3]; ke += o[4];
+                ms = std::max(ms, o[5]); md = std::max(md, o[6]); cfl = std::max(cfl, o[7]); mf = std::max(mf, o[8]);
             }
         const R DENSITY = 1000;
         const R AREA = R(p.width) / R(nx - 1) * R(p.length) / R(ny - 1);
@@ -883,6 +899,17 @@ public:
         return out;
     }
 
+    // CopyFromXxAndXy (compute.hlsl:814-823) over the interior (engine.cpp:1219-1233)
+    virtual void copy_from(std::vector<T4>& new_state) {
+        for (int y = 2; y < ny + 2; ++y)
+            for (int x = 2; x < nx + 2; ++x) {
+                T4& s = new_state[at(x, y)];
+                s.g = D1xc[0][at(x, y)].g;
+                s.b = D1yc[0][at(x, y)].b;
+                s.a = 0;
+            }
+    }
+
     // ---- timestep() (engine.cpp:849-1522): one pass ------------------------------------------
     void timestep() {
         std::vector<T4>& old_state = state[sim_idx];
@@ -897,14 +924,7 @@ public:
         }
         cr_solve_x(new_state);
         cr_solve_y(new_state);
-        // CopyFromXxAndXy over the interior (engine.cpp:1219-1233)
-        for (int y = 2; y < ny + 2; ++y)
-            for (int x = 2; x < nx + 2; ++x) {
-                T4& s = new_state[at(x, y)];
-                s.g = D1xc[0][at(x, y)].g;
-                s.b = D1yc[0][at(x, y)].b;
-                s.a = 0;
-            }
+        copy_from(new_state);
         // Boundaries in the order East, North, West, South (engine.cpp:1342-1438)
         boundary_side(new_state, 1);
         boundary_side(new_state, 0);
@@ -946,7 +966,7 @@ public:
     }
 
     // AddSolitaryWave (compute.hlsl:949-976, engine.cpp:2154-2219); theta in degrees
-    void add_solitary_wave(double Hh, double theta_deg, double xc, double yc) {
+    virtual void add_solitary_wave(double Hh, double theta_deg, double xc, double yc) {
         std::vector<T4>& st = state[sim_idx];
         const std::vector<T4> copy = st;
         const R th = R(theta_deg) * PI_ / R(180);

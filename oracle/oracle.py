@@ -26,9 +26,15 @@ def build() -> None:
 
 def _lib(real: str) -> C.CDLL:
     if real not in _libs:
-        path = os.path.join(_HERE, "_build", f"liboracle_{real}.so")
-        if not os.path.exists(path):
-            build()
+        if real == "ref":
+            # the reference's own compute.hlsl driven by the oracle's schedule (ref_build.py)
+            path = os.path.join(_HERE, "_ref", "libref_shader.so")
+            if not os.path.exists(path):
+                raise FileNotFoundError("oracle/_ref/libref_shader.so is not built (python oracle/ref_build.py)")
+        else:
+            path = os.path.join(_HERE, "_build", f"liboracle_{real}.so")
+            if not os.path.exists(path):
+                build()
         L = C.CDLL(path)
         vp, i, dp = C.c_void_p, C.c_int, C.POINTER(C.c_double)
         fp = C.POINTER(C.c_float)

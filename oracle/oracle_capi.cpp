@@ -19,7 +19,13 @@
 #endif
 
 using Real = ORACLE_REAL;
+#ifdef ORACLE_REF_SHADER
+// The reference's shader code driven by the oracle's schedule (built by ref_build.py).
+#include "ref_engine.hpp"
+using Eng = refshader::RefEngine;
+#else
 using Eng = oracle::Engine<Real>;
+#endif
 
 namespace {
 
