@@ -248,12 +248,14 @@ def main():
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     except Exception:
         peak, peak_src = 6650.0, "fallback"
+    # DRAM bytes per cell of one stencil launch measured by ncu (dram__bytes_read.sum +
+    # dram__bytes_write.sum / cells) on the first 8 members of this ensemble, mixed form:
+    # predictor 116.6, corrector 143.7; scaled here to this launch's cells.
+    ncu_bytes_cell = {"mixed": (116.6, 143.7)}
     traffic = None
-    try:
-        tr = json.load(open(os.path.join(ROOT, "profiles", "stencil_traffic.json")))
-        traffic = tr["dram_bytes_per_cell"] * cells
-    except Exception:
-        pass
+    if args.form in ncu_bytes_cell:
+        pb, cbytes = ncu_bytes_cell[args.form]
+        traffic = (pb + N * cbytes) / (1 + N) * cells
     total_kernel_ms = sum(v[0] for v in kt.values())
     shares = {k: round(v[0] / total_kernel_ms, 4) for k, v in kt.items()} if total_kernel_ms > 0 else {}
     step_bytes = cb.byte_model(args.form, N)[1]

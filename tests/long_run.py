@@ -1,0 +1,156 @@
+"""Long-run accuracy of the CUDA forms against the FP64 oracle (a measurement, not a pytest test).
+
+The FP64 oracle at 1024^2 x 10,000 steps takes tens of CPU minutes, so the two sides run
+separately and meet in .npz files:
+
+  python tests/long_run.py oracle --case c3 --steps 10000 --out ref.npz   # CPU, FP64 oracle
+  python tests/long_run.py gpu    --case c3 --steps 10000 --out gpu.npz   # CUDA forms
+  python tests/long_run.py compare ref.npz gpu.npz                        # prints one JSON line
+
+Cases: ``c3`` (1024^2 solitary wave on the truncated cone, solid walls), ``c3wm`` (the same
+basin with the sinusoidal wave-maker), ``c1`` (512x64 flume with the sine wave-maker).  Every
+``--every`` steps the FP64 total water volume (mass_full) is recorded.
+
+Reported per form: eta RMS over the interior (m), max |eta error| (m), max run-up of each side
+and its difference (run-up = highest bed elevation among initially dry cells whose recorded
+maximum inundation depth exceeds 1e-3 m), relative mass difference from the FP64 oracle at the
+end, max over the record, and each side's closed-basin drift |M(t) - M(0)| / M(0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
+
+from celeris_b200 import cases  # noqa: E402
+
+
+def build_case(name: str, n: int | None):
+    if name == "c3":
+        return cases.config3(n or 1024, n or 1024)
+    if name == "c3wm":
+        return cases.config3(n or 1024, n or 1024, wavemaker=True)
+    if name == "c1":
+        return cases.config1()
+    raise KeyError(name)
+
+
+def run_oracle(args):
+    from oracle import Oracle
+    p, z, bnx, bny = build_case(args.case, args.n)
+    o = Oracle(p, z, bnx, bny, real="f64")
+    s0 = o.reset_timestep()
+    t0 = time.time()
+    masses = [s0["mass_full"]]
+    done = 0
+    while done < args.steps:
+        k = min(args.every, args.steps - done)
+        s = o.physical_steps(k)
+        done += k
+        masses.append(o.reset_timestep()["mass_full"])
+        print(f"oracle {done}/{args.steps} steps, {time.time() - t0:.0f} s", flush=True)
+    np.savez_compressed(args.out, bottom=o.bottom()[..., 2].astype(np.float32),
+                        state=o.state(), aux=o.aux(), mass=np.array(masses), every=args.every,
+                        form="fp64-oracle")
+
+
+def run_gpu(args):
+    import celeris_b200 as cb
+    p, z, bnx, bny = build_case(args.case, args.n)
+    out = {}
+    for form in args.forms.split(","):
+        t0 = time.time()
+        if form == "plain":
+            eng = cb.Engine(p, z, "plain")
+            masses = [eng.reset_timestep()["mass_full"]]
+            done = 0
+            while done < args.steps:
+                k = min(args.every, args.steps - done)
+                eng.physical_steps(k)
+                done += k
+                masses.append(eng.reset_timestep()["mass_full"])
+            st, aux = eng.state(), eng.aux()
+        else:
+            b = cb.Batch([(p, z)], form)
+            b.use_graph(True)
+            masses = [b.stats()[0]["mass_full"]]
+            done = 0
+            while done < args.steps:
+                k = min(args.every, args.steps - done)
+                b.step(k)
+                done += k
+                masses.append(b.stats()[0]["mass_full"])
+            st, aux = b.state(0), b.aux(0)
+        out[f"{form}/state"] = st
+        out[f"{form}/aux"] = aux
+        out[f"{form}/mass"] = np.array(masses)
+        print(f"{form}: {args.steps} steps in {time.time() - t0:.1f} s", flush=True)
+    np.savez_compressed(args.out, every=args.every, **out)
+
+
+def runup(bottom: np.ndarray, initial_dry: np.ndarray, maxdepth: np.ndarray) -> float:
+    wet = (maxdepth > 1e-3) & initial_dry
+    return float(bottom[wet].max()) if wet.any() else float("nan")
+
+
+def compare(args):
+    ref = np.load(args.ref)
+    gpu = np.load(args.gpu)
+    B = ref["bottom"].astype(np.float64)
+    I = (slice(2, -2), slice(2, -2))
+    swl = 0.0
+    initial_dry = B[I] > swl
+    eta_ref = ref["state"][..., 0][I] - swl
+    res = {"steps_per_record": int(ref["every"]), "records": int(len(ref["mass"]) - 1)}
+    m_ref = ref["mass"]
+    res["fp64_closed_basin_drift"] = float(np.max(np.abs(m_ref - m_ref[0])) / m_ref[0])
+    ru_ref = runup(B[I], initial_dry, ref["aux"][..., 0][I])
+    res["fp64_runup_m"] = ru_ref
+    forms = sorted({k.split("/")[0] for k in gpu.files if "/" in k})
+    for f in forms:
+        st = gpu[f"{f}/state"].astype(np.float64)
+        d = st[..., 0][I] - swl - eta_ref
+        m = gpu[f"{f}/mass"]
+        n = min(len(m), len(m_ref))
+        ru = runup(B[I], initial_dry, gpu[f"{f}/aux"][..., 0][I].astype(np.float64))
+        res[f] = {
+            "eta_rms_m": float(np.sqrt(np.mean(d * d))),
+            "eta_max_abs_m": float(np.max(np.abs(d))),
+            "runup_m": ru,
+            "runup_err_m": float(abs(ru - ru_ref)),
+            "mass_rel_diff_end": float(abs(m[n - 1] - m_ref[n - 1]) / m_ref[n - 1]),
+            "mass_rel_diff_max": float(np.max(np.abs(m[:n] - m_ref[:n]) / m_ref[:n])),
+            "closed_basin_drift": float(np.max(np.abs(m - m[0])) / m[0]),
+        }
+    print(json.dumps(res))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    for name in ("oracle", "gpu"):
+        s = sub.add_parser(name)
+        s.add_argument("--case", default="c3")
+        s.add_argument("--n", type=int, default=None)
+        s.add_argument("--steps", type=int, default=10000)
+        s.add_argument("--every", type=int, default=500)
+        s.add_argument("--out", required=True)
+        if name == "gpu":
+            s.add_argument("--forms", default="mixed,fused,plain")
+    c = sub.add_parser("compare")
+    c.add_argument("ref")
+    c.add_argument("gpu")
+    a = ap.parse_args()
+    {"oracle": run_oracle, "gpu": run_gpu, "compare": compare}[a.cmd](a)
+
+
+if __name__ == "__main__":
+    main()
