@@ -408,6 +408,9 @@ public:
         return 0;
     }
     R dt_() const { return current_timestep; }
+    // initSetting.timestep is a float (settings.hpp:318): every build, FP64 included, steps with
+    // the single-precision value of the configured time step
+    R dt_setting() const { return R(float(p.timestep)); }
     R g_() const { return R(p.gravity); }
 
     // ---- Pass1 (compute.hlsl:380-458), region [1,nx+3) x [1,ny+3) -------------------------
@@ -872,19 +875,19 @@ public:
         mass *= DENSITY * AREA; xm *= DENSITY * AREA; ym *= DENSITY * AREA;
         ke *= R(0.5) * DENSITY * AREA; pe *= g * DENSITY * AREA;
         ms = std::sqrt(ms); mf /= g; mf = std::sqrt(mf);
-        if (cfl > 0 && !target_cfl_set && p.adaptive) { target_cfl = double(R(p.timestep) * cfl); target_cfl_set = true; }
+        if (cfl > 0 && !target_cfl_set && p.adaptive) { target_cfl = double(dt_setting() * cfl); target_cfl_set = true; }
         if (!initialized_timesteps) {
-            current_timestep = R(p.timestep);
+            current_timestep = dt_setting();
             if (p.adaptive && !target_cfl_set) target_cfl = 0;
             cfl = (p.adaptive ? R(target_cfl) : R(0)) / current_timestep;
             old_old_timestep = current_timestep; old_timestep = current_timestep;
             initialized_timesteps = true;
         }
         if (time_scheme == PREDICTOR_ADAPTIVE) {
-            const R tgt = std::max(R(target_cfl) / cfl, R(p.timestep) * R(p.min_timestep_ratio));
+            const R tgt = std::max(R(target_cfl) / cfl, dt_setting() * R(float(p.min_timestep_ratio)));
             current_timestep = tgt > old_timestep ? R(p.ema_alpha) * tgt + (1 - R(p.ema_alpha)) * old_timestep : tgt;
         } else {
-            current_timestep = R(p.timestep);
+            current_timestep = dt_setting();
         }
         Stats out{};
         out.mass = double(mass); out.x_momentum = double(xm); out.y_momentum = double(ym);

@@ -58,8 +58,8 @@ def run_oracle(args):
         masses.append(o.reset_timestep()["mass_full"])
         print(f"oracle {done}/{args.steps} steps, {time.time() - t0:.0f} s", flush=True)
     np.savez_compressed(args.out, bottom=o.bottom()[..., 2].astype(np.float32),
-                        state=o.state(), aux=o.aux(), mass=np.array(masses), every=args.every,
-                        form="fp64-oracle")
+                        eta=o.state()[..., 0], maxdepth=o.aux()[..., 0], mass=np.array(masses),
+                        every=args.every, form="fp64-oracle")
 
 
 def run_gpu(args):
@@ -89,8 +89,8 @@ def run_gpu(args):
                 done += k
                 masses.append(b.stats()[0]["mass_full"])
             st, aux = b.state(0), b.aux(0)
-        out[f"{form}/state"] = st
-        out[f"{form}/aux"] = aux
+        out[f"{form}/eta"] = st[..., 0].astype(np.float32)        # w (sea level 0)
+        out[f"{form}/maxdepth"] = aux[..., 0].astype(np.float32)  # max inundated depth
         out[f"{form}/mass"] = np.array(masses)
         print(f"{form}: {args.steps} steps in {time.time() - t0:.1f} s", flush=True)
     np.savez_compressed(args.out, every=args.every, **out)
@@ -108,19 +108,18 @@ def compare(args):
     I = (slice(2, -2), slice(2, -2))
     swl = 0.0
     initial_dry = B[I] > swl
-    eta_ref = ref["state"][..., 0][I] - swl
+    eta_ref = ref["eta"][I] - swl
     res = {"steps_per_record": int(ref["every"]), "records": int(len(ref["mass"]) - 1)}
     m_ref = ref["mass"]
     res["fp64_closed_basin_drift"] = float(np.max(np.abs(m_ref - m_ref[0])) / m_ref[0])
-    ru_ref = runup(B[I], initial_dry, ref["aux"][..., 0][I])
+    ru_ref = runup(B[I], initial_dry, ref["maxdepth"][I])
     res["fp64_runup_m"] = ru_ref
     forms = sorted({k.split("/")[0] for k in gpu.files if "/" in k})
     for f in forms:
-        st = gpu[f"{f}/state"].astype(np.float64)
-        d = st[..., 0][I] - swl - eta_ref
+        d = gpu[f"{f}/eta"].astype(np.float64)[I] - swl - eta_ref
         m = gpu[f"{f}/mass"]
         n = min(len(m), len(m_ref))
-        ru = runup(B[I], initial_dry, gpu[f"{f}/aux"][..., 0][I].astype(np.float64))
+        ru = runup(B[I], initial_dry, gpu[f"{f}/maxdepth"][I].astype(np.float64))
         res[f] = {
             "eta_rms_m": float(np.sqrt(np.mean(d * d))),
             "eta_max_abs_m": float(np.max(np.abs(d))),
