@@ -191,8 +191,15 @@ class Batch:
         check(lib().cel_batch_step(self.h, n))
 
     def stats(self) -> list:
+        """Statistics of each member at the start of the most recent step (fused into that step)."""
         arr = (Stats * self.n)()
         check(lib().cel_batch_stats(self.h, arr))
+        return [arr[i].as_dict() for i in range(self.n)]
+
+    def stats_current(self) -> list:
+        """Statistics of each member's current state (an extra pass over the state)."""
+        arr = (Stats * self.n)()
+        check(lib().cel_batch_stats_current(self.h, arr))
         return [arr[i].as_dict() for i in range(self.n)]
 
     def state(self, i: int) -> np.ndarray:

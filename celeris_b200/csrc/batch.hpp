@@ -17,7 +17,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
 void batch_destroy(cel_batch* b);
 int batch_set_stream(cel_batch* b, cudaStream_t s, std::string& err);
 int batch_step(cel_batch* b, int nsteps, std::string& err);
-int batch_stats(cel_batch* b, cel_stats* out, std::string& err);
+int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err);
 int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err);
 int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err);
 int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err);

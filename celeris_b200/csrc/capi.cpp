@@ -305,7 +305,12 @@ int cel_batch_step(cel_batch* b, int n) {
 int cel_batch_stats(cel_batch* b, cel_stats* out) {
     BAT(b);
     if (!out) { set_error("null buffer"); return CEL_ERR_ARG; }
-    CEL_GUARD_BEGIN BRET(cel::batch_stats(b, out, err)); CEL_GUARD_END
+    CEL_GUARD_BEGIN BRET(cel::batch_stats(b, out, false, err)); CEL_GUARD_END
+}
+int cel_batch_stats_current(cel_batch* b, cel_stats* out) {
+    BAT(b);
+    if (!out) { set_error("null buffer"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN BRET(cel::batch_stats(b, out, true, err)); CEL_GUARD_END
 }
 int cel_batch_get_state(cel_batch* b, int i, float* rgba) {
     BAT(b);

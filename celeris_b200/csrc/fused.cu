@@ -63,9 +63,9 @@ struct MemberDev {
     const float* BX;
     const float* BA;
     float* R[2];            // increment right-hand sides for hu, hv
-    float* G[4][3];         // dU/dt history buffers
-    float* F[4][2];         // F*, G* history buffers
-    float* AUX[2];          // max inundated depth, breaking indicator
+    float4* HA[4];          // history slots: {dw/dt, dhu/dt, dhv/dt, F*}
+    float* HB[4];           // history slots: G*
+    float* AUX[2];          // {max inundated depth, breaking} as one float2 plane pair (AUX[0])
     const float* FX[3];     // x-systems: c', inv_den, m
     const float* FYF[3];    // y-systems: c', inv_den, m
     BoundaryDesc bd[4];     // N, E, S, W
@@ -83,6 +83,9 @@ struct PassArgs {
     int in, out, cur;
     int og, oog, scr, pred;
     int scheme;
+    int stats;          // accumulate GetStats of the input state (first pass of a physical step)
+    int friction;       // some member has a nonzero friction coefficient
+    double* late_flag;  // set when a bounded TMA wait gave up
 };
 
 __device__ __forceinline__ void two_sum_add(float& hi, float& lo, float d) {
@@ -214,10 +217,16 @@ __device__ __forceinline__ float friction_fast(float hu, float hv, float h, floa
 
 struct Face { float hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, msd; };
 
+// MinMod (compute.hlsl:292-296) without branches: all three positive <=> their minimum is
+// positive, all negative <=> their maximum is negative (identical results for finite inputs).
+__device__ __forceinline__ float minmod3_fast(float a, float b, float c) {
+    const float mn = fminf(fminf(a, b), c), mx = fmaxf(fmaxf(a, b), c);
+    return mn > 0.f ? mn : (mx < 0.f ? mx : 0.f);
+}
 // Reconstruct with the breaking-indicator standard deviation, divisions by 3 as products
 __device__ __forceinline__ void reconstruct_sd_fast(float tt, float w, float c, float e, float& ow, float& oe, float& sd) {
     const float z1 = tt * (c - w), z2 = e - w, z3 = tt * (e - c);
-    const float g2 = 0.25f * minmod3(z1, z2, z3);
+    const float g2 = 0.25f * minmod3_fast(z1, z2, z3);
     const float mu = (0.5f / 3.0f) * (z1 + z2 + z3);
     sd = sqrtf(((z1 - mu) * (z1 - mu) + (z2 - mu) * (z2 - mu) + (z3 - mu) * (z3 - mu)) * (1.0f / 3.0f));
     oe = c + g2;
@@ -239,6 +248,22 @@ struct Kahan {
 // Ring layout: field f, slot s, column k at ring[f * FSTR + s * RSTR + k]; a "row base" is
 // s * RSTR + (this thread's column), so every access is base + compile-time offset.
 constexpr int FSTR = RING * RSTR;
+constexpr int DSTR = RBOX;   // still-water depth ring: one row of RBOX columns per slot
+
+__device__ __forceinline__ void reconstruct_fast(float tt, float w, float c, float e, float& ow, float& oe) {
+    const float z1 = tt * (c - w), z2 = e - w, z3 = tt * (e - c);
+    const float g2 = 0.25f * minmod3_fast(z1, z2, z3);
+    oe = c + g2;
+    ow = c - g2;
+}
+// CorrectW (compute.hlsl:317-328) as selects
+__device__ __forceinline__ void correct_w_fast(float Bw, float Be, float wbar, float& ww, float& we) {
+    const bool c1 = we < Be, c2 = !c1 && (ww < Bw);
+    const float nwe = c1 ? Be : (c2 ? fmaxf(Be, 2.f * wbar - Bw) : we);
+    const float nww = c1 ? fmaxf(Bw, 2.f * wbar - Be) : (c2 ? Bw : ww);
+    we = nwe;
+    ww = nww;
+}
 
 // Pass1 at one cell: rows below / here / above given by their row bases.
 __device__ __forceinline__ void faces_at(const float* __restrict__ ring, int bm, int b0, int bp, const SimConsts& c,
@@ -254,12 +279,12 @@ __device__ __forceinline__ void faces_at(const float* __restrict__ ring, int bm,
     reconstruct_sd_fast(c.two_theta, wl, wc, wr, wW, wE, sd1);
     reconstruct_sd_fast(c.two_theta, wd, wc, wu, wS, wN, sd2);
     const float huc = HU[b0], hvc = HV[b0];
-    reconstruct(c.two_theta, HU[b0 - 1], huc, HU[b0 + 1], huW, huE);
-    reconstruct(c.two_theta, HU[bm], huc, HU[bp], huS, huN);
-    reconstruct(c.two_theta, HV[b0 - 1], hvc, HV[b0 + 1], hvW, hvE);
-    reconstruct(c.two_theta, HV[bm], hvc, HV[bp], hvS, hvN);
-    correct_w(BW, BE, wc, wW, wE);
-    correct_w(BS, BN, wc, wS, wN);
+    reconstruct_fast(c.two_theta, HU[b0 - 1], huc, HU[b0 + 1], huW, huE);
+    reconstruct_fast(c.two_theta, HU[bm], huc, HU[bp], huS, huN);
+    reconstruct_fast(c.two_theta, HV[b0 - 1], hvc, HV[b0 + 1], hvW, hvE);
+    reconstruct_fast(c.two_theta, HV[bm], hvc, HV[bp], hvS, hvN);
+    correct_w_fast(BW, BE, wc, wW, wE);
+    correct_w_fast(BS, BN, wc, wS, wN);
     f.hN = wN - BN; f.hE = wE - BE; f.hS = wS - BS; f.hW = wW - BW;
     float q;
     q = div_by_h_fast(f.hN, c.epsilon); f.uN = q * huN; f.vN = q * hvN;
@@ -269,16 +294,43 @@ __device__ __forceinline__ void faces_at(const float* __restrict__ ring, int bm,
     f.msd = fmaxf(sd1 * c.one_over_dx, sd2 * c.one_over_dy);
 }
 
+// KP07 flux through one face for the three equations, given the two face states (m: the side
+// with the lower index, p: the other); `xdir` selects the velocity normal to the face.
+__device__ __forceinline__ void face_flux(float hm, float um, float vm, float hp, float up, float vp, float g,
+                                          float hg, bool xdir, float out[3]) {
+    const float cm = sqrtf(g * hm), cpp = sqrtf(g * hp);
+    const float nm = xdir ? um : vm, np = xdir ? up : vp;
+    const float ap = fmaxf(fmaxf(nm + cm, np + cpp), 0.f);
+    const float am = fminf(fminf(nm - cm, np - cpp), 0.f);
+    const float qp = hp * np, qm = hm * nm;          // normal mass fluxes
+    float Fp[3], Fm[3], dU[3];
+    Fp[0] = qp; Fm[0] = qm; dU[0] = hp - hm;
+    if (xdir) {
+        Fp[1] = hp * (up * up + hg * hp); Fm[1] = hm * (um * um + hg * hm); dU[1] = hp * up - hm * um;
+        Fp[2] = qp * vp; Fm[2] = qm * vm; dU[2] = hp * vp - hm * vm;
+    } else {
+        Fp[1] = qp * up; Fm[1] = qm * um; dU[1] = hp * up - hm * um;
+        Fp[2] = hp * (vp * vp + hg * hp); Fm[2] = hm * (vm * vm + hg * hm); dU[2] = hp * vp - hm * vm;
+    }
+    numflux3(ap, am, Fp, Fm, dU, out);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Plane layout of a member (offsets in planes of P x NY floats):
+//   S: w, hu, hv for 3 buffers (9) | L: their low words (9, mixed form only) | BY BX BA | R0 R1 |
+//   H[s], s = 0..3: HA = float4 {dw/dt, dhu/dt, dhv/dt, F*} (4 planes) and HB = G* (1 plane) |
+//   AUX = float2 {max inundated depth, breaking} (2 planes) | FX (3) | FY (3)
+// ---------------------------------------------------------------------------------------------
 template <bool MIXED>
 __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
                                                  int ntiles, PassArgs pa) {
     __shared__ __align__(128) float ring[6 * FSTR];
+    __shared__ float dring[RING * DSTR];  // still-water depth max(0, sea level - BA) of each ring row
     __shared__ __align__(8) unsigned long long bars[RING];
-    __shared__ float fEW[2][6][MW];     // [row parity][hE,uE,vE,hW,uW,vW][thread]
-    __shared__ float xb[2][3][MW];      // [row parity][component][thread] x flux at the thread's east face
-    __shared__ double red[MW / 32][STATS_N];
-    constexpr int OFF = MIXED ? 18 : 9;  // plane layout: S(9) [L(9)] BY BX BA R0 R1 G(12) F(8) AUX(2) ...
-    constexpr int iR0 = OFF + 3, iG0 = OFF + 5, iF0 = OFF + 17, iAUX = OFF + 25;
+    __shared__ float fW[2][3][MW];       // [row parity][hW, uW, vW][thread]: west faces for the x flux
+    __shared__ float xb[3][MW];          // x flux at the thread's east face, this row
+    constexpr int OFF = MIXED ? 18 : 9;
+    constexpr int iR0 = OFF + 3, iH0 = OFF + 5, iAUX = OFF + 25;
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int k = 0; k < RING; ++k) mbar_init(&bars[k], 1);
@@ -293,6 +345,9 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
     const float* BAr = ring + 3 * FSTR;
     const float* BXr = ring + 4 * FSTR;
     const float* BYr = ring + 5 * FSTR;
+    const bool stats = pa.stats != 0;
+    const bool corr = pa.scheme == CEL_SCHEME_CORRECTOR;
+    const bool euler = pa.scheme == CEL_SCHEME_EULER;
 
     for (int it = blockIdx.x; it < ntiles; it += gridDim.x) {
         const int4 tl = tiles[it];
@@ -300,48 +355,66 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
         const SimConsts c = M.c;
         const int P = M.P, nx = c.nx, ny = c.ny;
         float* __restrict__ B = M.base;
-        const unsigned PL = unsigned(M.plane);
+        const size_t PL = M.plane;
         const CUtensorMap* tm = M.tmaps;
         const int x0 = tl.y, y0 = tl.z;
         const int xs = (x0 - 2) & ~3;          // TMA box start, 16-byte aligned
         const int xc = x0 - 1 + tid;           // this thread's column
-        const int rc = xc - xs;                // its ring column
+        const int rc0 = xc - xs;               // its ring column (1 .. 131)
+        // Pass3 of the halo threads (0 and MW-1) runs on a clamped column and stores nothing; their
+        // faces (needed by the neighbouring output columns) use the true column
+        const int rc = max(rc0, 2);
         const int yend = min(y0 + MH, ny + 2);
         const int last_row = yend + 1;
         const bool out_col = tid >= 1 && tid <= MO && xc < nx + 2;
         const float dtm = *M.dtp;
         const float decay = t_pow(fabsf(c.whitewater_decay_rate), dtm);
-        const bool corr = pa.scheme == CEL_SCHEME_CORRECTOR;
-        const bool euler = pa.scheme == CEL_SCHEME_EULER;
-        // warp-uniform plane offsets (in floats) for this pass
-        const unsigned oOG = unsigned(iG0 + 3 * pa.og) * PL, oOOG = unsigned(iG0 + 3 * pa.oog) * PL;
-        const unsigned oFO = unsigned(iF0 + 2 * pa.og) * PL, oFOO = unsigned(iF0 + 2 * pa.oog) * PL;
-        const unsigned oPR = unsigned(iG0 + 3 * pa.pred) * PL, oFP = unsigned(iF0 + 2 * pa.pred) * PL;
-        const unsigned oSCR = unsigned(iG0 + 3 * pa.scr) * PL, oFS = unsigned(iF0 + 2 * pa.scr) * PL;
-        const unsigned oOUT = unsigned(3 * pa.out) * PL, oCUR = unsigned(3 * pa.cur) * PL;
-        const unsigned oLB = unsigned(9 + 3 * (corr ? pa.cur : pa.in)) * PL, oLO = unsigned(9 + 3 * pa.out) * PL;
-        const unsigned oR = unsigned(iR0) * PL, oAUX = unsigned(iAUX) * PL;
+        const float sl = c.sea_level;
+        // per-plane bases of this pass
+        const float4* __restrict__ HAo = reinterpret_cast<const float4*>(B + (iH0 + 5 * pa.og) * PL);
+        const float4* __restrict__ HAoo = reinterpret_cast<const float4*>(B + (iH0 + 5 * pa.oog) * PL);
+        const float4* __restrict__ HAp = reinterpret_cast<const float4*>(B + (iH0 + 5 * pa.pred) * PL);
+        float4* __restrict__ HAs = reinterpret_cast<float4*>(B + (iH0 + 5 * pa.scr) * PL);
+        const float* __restrict__ HBo = B + (iH0 + 5 * pa.og + 4) * PL;
+        const float* __restrict__ HBoo = B + (iH0 + 5 * pa.oog + 4) * PL;
+        const float* __restrict__ HBp = B + (iH0 + 5 * pa.pred + 4) * PL;
+        float* __restrict__ HBs = B + (iH0 + 5 * pa.scr + 4) * PL;
+        float* __restrict__ Wout = B + (3 * pa.out) * PL;
+        const float* __restrict__ Wcur = B + (3 * pa.cur) * PL;
+        float* __restrict__ R0 = B + iR0 * PL;
+        float2* __restrict__ AUX = reinterpret_cast<float2*>(B + iAUX * PL);
+        const float* __restrict__ Lbase = B + (9 + 3 * (corr ? pa.cur : pa.in)) * PL;
+        float* __restrict__ Lout = B + (9 + 3 * pa.out) * PL;
 
-        auto issue = [&](int row, int sl) {    // one thread: request the 6 fields of a row into slot sl
-            mbar_expect_tx(&bars[sl], ROW_BYTES);
-            float* dst = ring + sl * RSTR;
-            tma_row(dst, tm + pa.in * 3 + 0, xs, row, &bars[sl]);
-            tma_row(dst + FSTR, tm + pa.in * 3 + 1, xs, row, &bars[sl]);
-            tma_row(dst + 2 * FSTR, tm + pa.in * 3 + 2, xs, row, &bars[sl]);
-            tma_row(dst + 3 * FSTR, tm + 9, xs, row, &bars[sl]);
-            tma_row(dst + 4 * FSTR, tm + 10, xs, row, &bars[sl]);
-            tma_row(dst + 5 * FSTR, tm + 11, xs, row, &bars[sl]);
+        auto issue = [&](int row, int sl_) {   // one thread: request the 6 fields of a row into slot sl_
+            mbar_expect_tx(&bars[sl_], ROW_BYTES);
+            float* dst = ring + sl_ * RSTR;
+            tma_row(dst, tm + pa.in * 3 + 0, xs, row, &bars[sl_]);
+            tma_row(dst + FSTR, tm + pa.in * 3 + 1, xs, row, &bars[sl_]);
+            tma_row(dst + 2 * FSTR, tm + pa.in * 3 + 2, xs, row, &bars[sl_]);
+            tma_row(dst + 3 * FSTR, tm + 9, xs, row, &bars[sl_]);
+            tma_row(dst + 4 * FSTR, tm + 10, xs, row, &bars[sl_]);
+            tma_row(dst + 5 * FSTR, tm + 11, xs, row, &bars[sl_]);
         };
         auto next_slot = [](int s) { return s + 1 == RING ? 0 : s + 1; };
+        // still-water depth of a ring row: thread k covers ring column rc0(thread 0) - 1 + k, and
+        // threads 0 and 1 also the two columns past the last thread (every column Pass3 reads)
+        const int dcol = rc0 - 1;
+        auto depth_row = [&](int slot) {
+            const float* ba = BAr + slot * RSTR;
+            float* dr = dring + slot * DSTR;
+            dr[dcol] = fmaxf(0.f, sl - ba[dcol]);
+            const int d2c = min(dcol + MW, RBOX - 1);
+            if (tid < 2) dr[d2c] = fmaxf(0.f, sl - ba[d2c]);
+        };
 
         Kahan acc[6];
         float mx[4] = {0.f, 0.f, 0.f, 0.f};
         bool bad = false;
         float nh = 0.f, nu = 0.f, nv = 0.f;       // north face of the previous row (this column)
+        float eh = 0.f, eu = 0.f, ev = 0.f;       // east face of row t (this column), from the last step
         float ypv0 = 0.f, ypv1 = 0.f, ypv2 = 0.f; // y flux below the current row
 
-        // Row r of this strip has sequence number seq0 + (r - (y0 - 2)), ring slot seq % RING and
-        // mbarrier phase parity (seq / RING) & 1.
         const unsigned seq0 = seq;
         const int sA = int(seq0 % RING), sB = next_slot(sA), sC = next_slot(sB);  // rows y0-2, y0-1, y0
 
@@ -350,38 +423,46 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
             fence_proxy_async();
             // rows y0-2 .. y0+PREFETCH-1 here; the loop requests row t+PREFETCH+2 at step t, so every
             // row is requested exactly once (one arrive per mbarrier phase)
-            int sl = sA;
-            for (int r = y0 - 2; r <= min(y0 + PREFETCH - 1, last_row); ++r) { issue(r, sl); sl = next_slot(sl); }
+            int sl_ = sA;
+            for (int r = y0 - 2; r <= min(y0 + PREFETCH - 1, last_row); ++r) { issue(r, sl_); sl_ = next_slot(sl_); }
         }
         {   // the first step also reads rows y0-2 and y0-1
             const unsigned pA = (seq0 / RING) & 1u, pB = ((seq0 + 1) / RING) & 1u;
             if (!mbar_wait_bounded(&bars[sA], pA, tma_late ? 1 : (1 << 22))) tma_late = true;
             if (!mbar_wait_bounded(&bars[sB], pB, tma_late ? 1 : (1 << 22))) tma_late = true;
+            depth_row(sA);
+            depth_row(sB);
         }
-        // window of rows t-2, t-1, t, t+1, t+2 at the first step (t = y0-2); the two rows below are
-        // not read before t = y0, by when the window has shifted onto loaded rows
         int s2m = sA, s1m = sA, s0 = sA, s1p = sB, s2p = sC;
         unsigned par2p = ((seq0 + 2) / RING) & 1u;            // phase parity of row t+2
         int sReq = int((seq0 + unsigned(PREFETCH) + 2) % RING);  // slot of row t+PREFETCH+2
 
         for (int t = y0 - 2; t < yend; ++t) {
+            const bool p3 = t >= y0;                   // Pass3 runs on this row (uniform)
+            const size_t e = size_t(t) * P + xc;       // this thread's cell of row t
+            // loads use a column inside the row (the halo thread past the last column reads a
+            // neighbour it never stores to)
+            const size_t el = size_t(t) * P + min(xc, c.NX - 1);
             // per-cell inputs of Pass3 at (xc, t), requested before the face work
-            const bool do3 = t >= y0 && out_col;
-            float* cp = B + (size_t(t) * P + xc);
-            float o0 = 0, o1 = 0, o2 = 0, q0 = 0, q1 = 0, q2 = 0, fo0 = 0, fo1 = 0, foo0 = 0, foo1 = 0;
-            float p0 = 0, p1 = 0, p2 = 0, fp0 = 0, fp1 = 0, wcur = 0, wlo = 0;
-            if (do3 && !euler) {
-                o0 = cp[oOG]; o1 = cp[oOG + PL]; o2 = cp[oOG + 2 * PL];
-                q0 = cp[oOOG]; q1 = cp[oOOG + PL]; q2 = cp[oOOG + 2 * PL];
-                fo0 = cp[oFO]; fo1 = cp[oFO + PL];
-                foo0 = cp[oFOO]; foo1 = cp[oFOO + PL];
-                if (corr) {
-                    p0 = cp[oPR]; p1 = cp[oPR + PL]; p2 = cp[oPR + 2 * PL];
-                    fp0 = cp[oFP]; fp1 = cp[oFP + PL];
-                    wcur = cp[oCUR];
+            float4 ho = make_float4(0.f, 0.f, 0.f, 0.f), hoo = ho, hp = ho;
+            float go = 0.f, goo = 0.f, gp = 0.f, wcur = 0.f, wlo = 0.f;
+            // aux texel of row t+1 owned by this strip (ghost texels x = 1 / y = 1 go with column /
+            // row 2), read-modify-written after the faces of row t+1
+            const int gy = t + 1;
+            const int cxa = xc < 2 ? 2 : xc, cya = gy < 2 ? 2 : gy;
+            const bool aux_ok = xc >= 1 && xc < nx + 2 && gy >= 1 && gy < ny + 2 && cxa >= x0 && cxa < x0 + MO &&
+                                cya >= y0 && cya < y0 + MH;
+            float2* a0 = AUX + (size_t(gy) * P + xc);
+            float2 aux_old = make_float2(0.f, 0.f);
+            if (aux_ok) aux_old = *a0;
+            if (p3) {
+                if (!euler) {
+                    ho = __ldg(HAo + el); hoo = __ldg(HAoo + el);
+                    go = __ldg(HBo + el); goo = __ldg(HBoo + el);
+                    if (corr) { hp = __ldg(HAp + el); gp = __ldg(HBp + el); wcur = __ldg(Wcur + el); }
                 }
+                if (MIXED) wlo = __ldg(Lbase + el);
             }
-            if (MIXED && do3) wlo = cp[oLB];
             __syncthreads();  // (A) the previous row step is complete: its oldest ring slot is free
             if (tid == 0 && t + PREFETCH + 2 <= last_row) {
                 fence_proxy_async();
@@ -389,97 +470,68 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
             }
             sReq = next_slot(sReq);
             if (!mbar_wait_bounded(&bars[s2p], par2p, tma_late ? 1 : (1 << 22))) tma_late = true;
-            const int bm = s0 * RSTR + rc, b0 = s1p * RSTR + rc, bp = s2p * RSTR + rc;  // rows t, t+1, t+2
+            depth_row(s2p);
+            const int bm = s0 * RSTR + rc0, b0 = s1p * RSTR + rc0, bp = s2p * RSTR + rc0;  // rows t, t+1, t+2
             // ---- faces of row t+1 (Pass1), aux of that row, y flux between rows t and t+1 ----
             Face f;
             faces_at(ring, bm, b0, bp, c, f);
             const int par1 = (t + 1) & 1;
-            fEW[par1][0][tid] = f.hE; fEW[par1][1][tid] = f.uE; fEW[par1][2][tid] = f.vE;
-            fEW[par1][3][tid] = f.hW; fEW[par1][4][tid] = f.uW; fEW[par1][5][tid] = f.vW;
-            {
-                const int gy = t + 1;
-                if (xc >= 1 && xc < nx + 2 && gy >= 1 && gy < ny + 2) {
-                    const int cx = xc < 2 ? 2 : xc, cy = gy < 2 ? 2 : gy;
-                    if (cx >= x0 && cx < x0 + MO && cy >= y0 && cy < y0 + MH) {
-                        float* a0 = B + (size_t(gy) * P + xc) + oAUX;
-                        const float md = fmaxf((f.hN + f.hE + f.hS + f.hW) * 0.25f, a0[0]);
-                        float bw = a0[PL];
-                        if (f.msd > M.tan_thr) bw = 1.0f;  // atan(msd) > threshold
-                        a0[0] = md;
-                        a0[PL] = bw * decay;
-                    }
-                }
+            fW[par1][0][tid] = f.hW; fW[par1][1][tid] = f.uW; fW[par1][2][tid] = f.vW;
+            if (aux_ok) {
+                const float md = fmaxf((f.hN + f.hE + f.hS + f.hW) * 0.25f, aux_old.x);
+                const float bw = (f.msd > M.tan_thr) ? 1.0f : aux_old.y;   // atan(msd) > threshold
+                *a0 = make_float2(md, bw * decay);
             }
             const float g = c.g, hg = c.half_g;
-            float yf[3];
-            {   // y flux at the north face of row t: north face of row t (carried) vs south face of row t+1
-                const float hN = nh, uN = nu, vN = nv;
-                const float hSn = f.hS, uSn = f.uS, vSn = f.vS;
-                const float cN = sqrtf(g * hN), cS = sqrtf(g * hSn);
-                const float bpl = fmaxf(fmaxf(vN + cN, vSn + cS), 0.f);
-                const float bmi = fminf(fminf(vN - cN, vSn - cS), 0.f);
-                const float Fp[3] = {hSn * vSn, hSn * uSn * vSn, hSn * (vSn * vSn + hg * hSn)};
-                const float Fm[3] = {hN * vN, hN * uN * vN, hN * (vN * vN + hg * hN)};
-                const float dU[3] = {hSn - hN, hSn * uSn - hN * uN, hSn * vSn - hN * vN};
-                numflux3(bpl, bmi, Fp, Fm, dU, yf);
-            }
-            // ---- x flux at the east face of (xc, t): faces of row t from the previous step ----
+            float yf[3];   // y flux at the north face of row t: north face of row t vs south face of row t+1
+            face_flux(nh, nu, nv, f.hS, f.uS, f.vS, g, hg, false, yf);
+            // ---- x flux at the east face of (xc, t): east face of row t (registers) vs west face of (xc+1, t)
             const int par = t & 1;
-            if (t >= y0 && tid < MW - 1) {
-                const float hE = fEW[par][0][tid], uE = fEW[par][1][tid], vE = fEW[par][2][tid];
-                const float hWe = fEW[par][3][tid + 1], uWe = fEW[par][4][tid + 1], vWe = fEW[par][5][tid + 1];
-                const float cE = sqrtf(g * hE), cW = sqrtf(g * hWe);
-                const float ap = fmaxf(fmaxf(uE + cE, uWe + cW), 0.f);
-                const float am = fminf(fminf(uE - cE, uWe - cW), 0.f);
-                const float Fp[3] = {hWe * uWe, hWe * (uWe * uWe + hg * hWe), hWe * uWe * vWe};
-                const float Fm[3] = {hE * uE, hE * (uE * uE + hg * hE), hE * uE * vE};
-                const float dU[3] = {hWe - hE, hWe * uWe - hE * uE, hWe * vWe - hE * vE};
+            {
+                const int tn = min(tid + 1, MW - 1);
                 float xo[3];
-                numflux3(ap, am, Fp, Fm, dU, xo);
-                xb[par][0][tid] = xo[0]; xb[par][1][tid] = xo[1]; xb[par][2][tid] = xo[2];
+                face_flux(eh, eu, ev, fW[par][0][tn], fW[par][1][tn], fW[par][2][tn], g, hg, true, xo);
+                xb[0][tid] = xo[0]; xb[1][tid] = xo[1]; xb[2][tid] = xo[2];
             }
             __syncthreads();  // (B)
             // ---- Pass3 at (xc, t) ----
-            if (do3) {
+            if (p3) {
                 const int c0 = s0 * RSTR + rc, cm = s1m * RSTR + rc, cpp1 = s1p * RSTR + rc;
                 const int cmm = s2m * RSTR + rc, cpp2 = s2p * RSTR + rc;   // rows t, t-1, t+1, t-2, t+2
-                const float sl = c.sea_level;
+                const int d0 = s0 * DSTR + rc;
                 const float wc = W[c0], huc = HU[c0], hvc = HV[c0];
                 const float BAh = BAr[c0], BXh = BXr[c0], BYh = BYr[c0];
                 const float BXw = BXr[c0 - 1], BYs = BYr[cm];
                 const float h = fmaxf(0.f, wc - BAh);
-                const float dh = fmaxf(0.f, sl - BAh), d2 = dh * dh, d3 = d2 * dh;
-                const float dl = fmaxf(0.f, sl - BAr[c0 - 1]), dr = fmaxf(0.f, sl - BAr[c0 + 1]);
-                const float ddn = fmaxf(0.f, sl - BAr[cm]), du = fmaxf(0.f, sl - BAr[cpp1]);
-                const float dll = fmaxf(0.f, sl - BAr[c0 - 2]), drr = fmaxf(0.f, sl - BAr[c0 + 2]);
-                const float ddd = fmaxf(0.f, sl - BAr[cmm]), duu = fmaxf(0.f, sl - BAr[cpp2]);
-                const float e0 = wc - sl;
-                const float el = W[c0 - 1] - sl, er = W[c0 + 1] - sl;
-                const float ed = W[cm] - sl, eu = W[cpp1] - sl;
-                const float ell = W[c0 - 2] - sl, err = W[c0 + 2] - sl;
-                const float edd = W[cmm] - sl, euu = W[cpp2] - sl;
-                const float eul = W[cpp1 - 1] - sl, eur = W[cpp1 + 1] - sl;
-                const float edl = W[cm - 1] - sl, edr = W[cm + 1] - sl;
+                const float dh = dring[d0], d2 = dh * dh, d3 = d2 * dh;
+                const float dl = dring[d0 - 1], dr = dring[d0 + 1], dll = dring[d0 - 2], drr = dring[d0 + 2];
+                const float ddn = dring[s1m * DSTR + rc], du = dring[s1p * DSTR + rc];
+                const float ddd = dring[s2m * DSTR + rc], duu = dring[s2p * DSTR + rc];
+                // eta = w - sea level enters only through differences, where the sea level cancels
+                const float e0 = wc, el_ = W[c0 - 1], er = W[c0 + 1], ed = W[cm], eu_ = W[cpp1];
+                const float ell = W[c0 - 2], err = W[c0 + 2], edd = W[cmm], euu = W[cpp2];
+                const float eul = W[cpp1 - 1], eur = W[cpp1 + 1], edl = W[cm - 1], edr = W[cm + 1];
                 const float odx = c.one_over_dx, ody = c.one_over_dy;
                 const float od2x = odx * odx, od3x = od2x * odx, od2y = ody * ody, od3y = od2y * ody;
                 const float ddx = (-drr + 8 * dr - 8 * dl + dll) * odx * (1.0f / 12.0f);
                 const float ddy = (-duu + 8 * du - 8 * ddn + ddd) * ody * (1.0f / 12.0f);
                 const float exy = (0.25f * odx * ody * (eur - edr - eul + edl));
-                const float exx = od2x * (er - 2 * e0 + el);
-                const float eyy = od2y * (eu - 2 * e0 + ed);
+                const float exx = od2x * (er - 2 * e0 + el_);
+                const float eyy = od2y * (eu_ - 2 * e0 + ed);
                 const float Bg = c.Bcoef_g;
-                const float P1x = Bg * (d3) * ((err - 2 * er + 2 * el - ell) * (0.5f * od3x) +
-                                               (eur - eul - 2 * er + 2 * el + edr - edl) * (0.5f * odx * od2y));
+                const float P1x = Bg * (d3) * ((err - 2 * er + 2 * el_ - ell) * (0.5f * od3x) +
+                                               (eur - eul - 2 * er + 2 * el_ + edr - edl) * (0.5f * odx * od2y));
                 const float P2x = Bg * (d2) * (ddx * (2 * exx + eyy) + ddy * exy);
-                const float P1y = Bg * (d3) * ((euu - 2 * eu + 2 * ed - edd) * (0.5f * od3y) +
-                                               (eur + eul - 2 * eu + 2 * ed - edr - edl) * (0.5f * ody * od2x));
+                const float P1y = Bg * (d3) * ((euu - 2 * eu_ + 2 * ed - edd) * (0.5f * od3y) +
+                                               (eur + eul - 2 * eu_ + 2 * ed - edr - edl) * (0.5f * ody * od2x));
                 const float P2y = Bg * (d2) * (ddy * (exx + 2 * eyy) + ddx * exy);
-                const float fr = friction_fast(huc, hvc, h, c.friction, c.is_manning, c.g, c.epsilon);
+                const float fr = pa.friction ? friction_fast(huc, hvc, h, c.friction, c.is_manning, c.g, c.epsilon) : 0.f;
                 const float s1 = -c.g_over_dx * h * (BXh - BXw) - huc * fr + (P1x + P2x);
                 const float s2 = -c.g_over_dy * h * (BYh - BYs) - hvc * fr + (P1y + P2y);
-                const float f0 = (xb[par][0][tid - 1] - xb[par][0][tid]) * odx + (ypv0 - yf[0]) * ody;
-                const float f1 = (xb[par][1][tid - 1] - xb[par][1][tid]) * odx + (ypv1 - yf[1]) * ody + s1;
-                const float f2 = (xb[par][2][tid - 1] - xb[par][2][tid]) * odx + (ypv2 - yf[2]) * ody + s2;
+                const int tw = max(tid - 1, 0);
+                const float f0 = (xb[0][tw] - xb[0][tid]) * odx + (ypv0 - yf[0]) * ody;
+                const float f1 = (xb[1][tw] - xb[1][tid]) * odx + (ypv1 - yf[1]) * ody + s1;
+                const float f2 = (xb[2][tw] - xb[2][tid]) * odx + (ypv2 - yf[2]) * ody + s2;
                 const float sixth = 1.0f / 6.0f;
                 const float Fs = (sixth * dh * (ddx * ((ody * 0.5f) * (HV[cpp1] - HV[cm])) +
                                                 (ddy * ((odx * 0.5f) * (HV[c0 + 1] - HV[c0 - 1])))));
@@ -492,42 +544,48 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
                     dw = dt * f0; rhu = dt * f1; rhv = dt * f2;
                 } else if (!corr) {
                     const float k12 = dt * (1.0f / 12.0f);
-                    dw = k12 * (23.0f * f0 - 16.0f * o0 + 5.0f * q0);
-                    rhu = k12 * (23.0f * f1 - 16.0f * o1 + 5.0f * q1) + (2.0f * Fs - 3.0f * fo0 + foo0);
-                    rhv = k12 * (23.0f * f2 - 16.0f * o2 + 5.0f * q2) + (2.0f * Gs - 3.0f * fo1 + foo1);
+                    dw = k12 * (23.0f * f0 - 16.0f * ho.x + 5.0f * hoo.x);
+                    rhu = k12 * (23.0f * f1 - 16.0f * ho.y + 5.0f * hoo.y) + (2.0f * Fs - 3.0f * ho.w + hoo.w);
+                    rhv = k12 * (23.0f * f2 - 16.0f * ho.z + 5.0f * hoo.z) + (2.0f * Gs - 3.0f * go + goo);
                 } else {
                     const float k24 = dt * (1.0f / 24.0f);
-                    dw = k24 * (9 * f0 + 19 * p0 - 5 * o0 + 1 * q0);
-                    rhu = k24 * (9 * f1 + 19 * p1 - 5 * o1 + 1 * q1) + Fs - fp0;
-                    rhv = k24 * (9 * f2 + 19 * p2 - 5 * o2 + 1 * q2) + Gs - fp1;
+                    dw = k24 * (9 * f0 + 19 * hp.x - 5 * ho.x + 1 * hoo.x);
+                    rhu = k24 * (9 * f1 + 19 * hp.y - 5 * ho.y + 1 * hoo.y) + Fs - hp.w;
+                    rhv = k24 * (9 * f2 + 19 * hp.z - 5 * ho.z + 1 * hoo.z) + Gs - gp;
                     wbase = wcur;
                 }
                 float wn = wbase, wl = wlo;
                 if (MIXED) two_sum_add(wn, wl, dw);
                 else wn = wbase + dw;
-                cp[oOUT] = wn;
-                if (MIXED) cp[oLO] = wl;
-                cp[oR] = rhu;
-                cp[oR + PL] = rhv;
-                cp[oSCR] = f0; cp[oSCR + PL] = f1; cp[oSCR + 2 * PL] = f2;
-                cp[oFS] = Fs; cp[oFS + PL] = Gs;
-                // GetStats (compute.hlsl:1319-1378) of the input state, FP64 accumulation
-                const float q = div_by_h_fast(h, c.epsilon);
-                const float u = q * huc, v = q * hvc;
-                if (xc < 2 + 4 * (nx / 4) && t < 2 + 4 * (ny / 4)) {
-                    acc[0].add(h); acc[1].add(h * (BAh + 0.5f * h)); acc[2].add(huc); acc[3].add(hvc);
-                    acc[4].add(huc * u + hvc * v);
+                if (out_col) {
+                    Wout[e] = wn;
+                    if (MIXED) Lout[e] = wl;
+                    R0[e] = rhu;
+                    R0[e + PL] = rhv;
+                    HAs[e] = make_float4(f0, f1, f2, Fs);
+                    HBs[e] = Gs;
+                }
+                if (stats) {   // GetStats (compute.hlsl:1319-1378) of the input state
+                    const float q = div_by_h_fast(h, c.epsilon);
+                    const float u = q * huc, v = q * hvc;
+                    // cells outside the 4x4 blocks (and the halo threads) contribute zeros; selects,
+                    // not products, so a halo value that is not finite cannot leak in
+                    const bool blk = out_col && xc < 2 + 4 * (nx / 4) && t < 2 + 4 * (ny / 4);
                     const float u2v2 = u * u + v * v;
                     const float cc = sqrtf(c.g * h);
-                    mx[0] = fmaxf(mx[0], u2v2); mx[1] = fmaxf(mx[1], h);
-                    mx[2] = fmaxf(mx[2], fmaxf((fabsf(u) + cc) * c.one_over_dx, (fabsf(v) + cc) * c.one_over_dy));
-                    mx[3] = fmaxf(mx[3], u2v2 * q);
+                    acc[0].add(blk ? h : 0.f); acc[1].add(blk ? h * (BAh + 0.5f * h) : 0.f);
+                    acc[2].add(blk ? huc : 0.f); acc[3].add(blk ? hvc : 0.f);
+                    acc[4].add(blk ? huc * u + hvc * v : 0.f);
+                    mx[0] = fmaxf(mx[0], blk ? u2v2 : 0.f); mx[1] = fmaxf(mx[1], blk ? h : 0.f);
+                    mx[2] = fmaxf(mx[2], blk ? fmaxf((fabsf(u) + cc) * odx, (fabsf(v) + cc) * ody) : 0.f);
+                    mx[3] = fmaxf(mx[3], blk ? u2v2 * q : 0.f);
+                    acc[5].add(out_col ? h : 0.f);
+                    bad = bad | (out_col & !(fabsf(wc) <= 3.0e38f && fabsf(huc) <= 3.0e38f && fabsf(hvc) <= 3.0e38f));
                 }
-                acc[5].add(h);
-                bad = bad || !(fabsf(wn) <= 3.0e38f) || !(fabsf(rhu) <= 3.0e38f) || !(fabsf(rhv) <= 3.0e38f);
             }
             ypv0 = yf[0]; ypv1 = yf[1]; ypv2 = yf[2];
             nh = f.hN; nu = f.uN; nv = f.vN;
+            eh = f.hE; eu = f.uE; ev = f.vE;
             // advance the ring window: rows t-1 .. t+3 become t-2 .. t+2
             s2m = s1m; s1m = s0; s0 = s1p; s1p = s2p;
             s2p = next_slot(s2p);
@@ -544,30 +602,34 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
             for (int k = tid; k < w * (cy1 - cy0); k += MW) {
                 const int gx = cx0 + k % w, gy = cy0 + k / w;
                 if (gx >= 2 && gx < nx + 2 && gy >= 2 && gy < ny + 2) continue;
-                float* gz = B + (size_t(gy) * P + gx);
+                const size_t gi = size_t(gy) * P + gx;
                 for (int q = 0; q < 3; ++q) {
-                    gz[oOUT + q * PL] = 0.f;
-                    if (MIXED) gz[oLO + q * PL] = 0.f;
+                    Wout[gi + q * PL] = 0.f;
+                    if (MIXED) Lout[gi + q * PL] = 0.f;
                 }
             }
         }
-        // ---- strip statistics -> member accumulators ----
-        {
+        // ---- strip statistics -> member accumulators (statistics pass only) ----
+        if (stats) {
             double sv[STATS_N];
             for (int k = 0; k < 6; ++k) sv[k] = acc[k].value();
             for (int k = 0; k < 4; ++k) sv[6 + k] = mx[k];
             sv[10] = bad ? 1.0 : 0.0;
-            sv[11] = tma_late ? 1.0 : 0.0;
+            sv[11] = 0.0;
             for (int off = 16; off; off >>= 1)
-                for (int k = 0; k < STATS_N; ++k) {
+                for (int k = 0; k < STATS_N - 1; ++k) {
                     const double o = __shfl_down_sync(0xffffffffu, sv[k], off);
                     sv[k] = (k >= 6) ? fmax(sv[k], o) : sv[k] + o;
                 }
+            // the reduction scratch reuses the ring: every row of this strip has been consumed and
+            // the next strip requests rows only after its opening barrier
+            double (*red)[STATS_N] = reinterpret_cast<double (*)[STATS_N]>(ring);
             const int lane = tid & 31, wid = tid >> 5;
-            if (lane == 0)
-                for (int k = 0; k < STATS_N; ++k) red[wid][k] = sv[k];
             __syncthreads();
-            if (tid < STATS_N) {
+            if (lane == 0)
+                for (int k = 0; k < STATS_N - 1; ++k) red[wid][k] = sv[k];
+            __syncthreads();
+            if (tid < STATS_N - 1) {
                 double a = red[0][tid];
                 for (int w = 1; w < MW / 32; ++w) a = (tid >= 6) ? fmax(a, red[w][tid]) : a + red[w][tid];
                 if (tid < 6) { if (a != 0.0) atomicAdd(M.stats + tid, a); }
@@ -575,6 +637,9 @@ __global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ m
             }
         }
     }
+    // a bounded TMA wait that gave up anywhere in this CTA marks the whole pass (the host reports
+    // it as a CUDA error of the batch)
+    if (__syncthreads_or(tma_late) && tid == 0) atomic_max_nonneg(pa.late_flag, 1.0);
 }
 
 // Stats of the current state only (resetTimestep on demand).
@@ -1035,8 +1100,12 @@ struct cel_batch {
     int2* bitems[4] = {nullptr, nullptr, nullptr, nullptr};
     int nbitems[4] = {0, 0, 0, 0};
     bool two_phase[4] = {false, false, false, false};
-    double* stats_all = nullptr;       // members * STATS_N (per pass, fused into the stencil)
-    double* stats_now_all = nullptr;
+    double* stats_all = nullptr;       // members * STATS_N, gathered by the first pass of each step
+    double* stats_now_all = nullptr;   // members * STATS_N, on-demand statistics of the current state
+    double* late_flag = nullptr;       // a bounded TMA wait gave up (sticky)
+    bool step_stats_valid = false;     // stats_all describes the start of the most recent step
+    std::vector<float> step_dt;        // the time step each member took in its most recent step
+    bool any_friction = false;
     float* dt_table = nullptr;         // per-member time step on the device
     float* dt_host = nullptr;          // pinned mirror of dt_table
     size_t smem_rows = 0, smem_cols = 0;
@@ -1102,6 +1171,7 @@ int dalloc(cel_batch* b, void** ptr, size_t bytes, std::string& err) {
     } while (0)
 
 int upload_state(cel_batch* b, int i, const float* rgba, std::string& err) {
+    b->step_stats_valid = false;
     Member& m = b->mem[i];
     const MemberDev& d = b->hdev[i];
     const int NX = m.hs.NX, NY = m.hs.NY;
@@ -1120,7 +1190,7 @@ int upload_state(cel_batch* b, int i, const float* rgba, std::string& err) {
 
 int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     const size_t nm = b->mem.size();
-    B_TRY(cudaMemsetAsync(b->stats_all, 0, nm * STATS_N * sizeof(double), b->stream));
+    if (pa.stats) B_TRY(cudaMemsetAsync(b->stats_all, 0, nm * STATS_N * sizeof(double), b->stream));
     {
         TimedLaunch t(&b->tm, b->stream, "fused_stencil");
         if (b->mixed)
@@ -1171,7 +1241,7 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
 }
 
 // One pass with the host state machine; updates the buffer indices.
-int run_pass(cel_batch* b, std::string& err) {
+int run_pass(cel_batch* b, bool first_of_step, std::string& err) {
     Scheme& s = b->sch;
     Idx& ix = b->ix;
     if (!s.initialized) s.choose_dt(0.f);
@@ -1188,7 +1258,14 @@ int run_pass(cel_batch* b, std::string& err) {
         pa.out = (ix.sin + 1) % 3;
     }
     pa.og = ix.og; pa.oog = ix.oog; pa.scr = ix.scr; pa.pred = ix.pred;
+    pa.stats = first_of_step ? 1 : 0;
+    pa.friction = b->any_friction ? 1 : 0;
+    pa.late_flag = b->late_flag;
     if (int e = launch_pass(b, pa, err)) return e;
+    if (first_of_step) {
+        b->step_stats_valid = true;
+        b->step_dt.assign(b->dt_host, b->dt_host + b->mem.size());
+    }
     const bool was_pred = s.is_predictor();
     const bool book = s.after_pass();
     if (book) {
@@ -1205,9 +1282,9 @@ int run_pass(cel_batch* b, std::string& err) {
 }
 
 int run_physical_step(cel_batch* b, std::string& err) {
-    if (int e = run_pass(b, err)) return e;
+    if (int e = run_pass(b, true, err)) return e;
     while (b->sch.time_scheme == CEL_SCHEME_CORRECTOR)
-        if (int e = run_pass(b, err)) return e;
+        if (int e = run_pass(b, false, err)) return e;
     return CEL_OK;
 }
 
@@ -1297,6 +1374,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         b->stats_all = static_cast<double*>(p);
         if (dalloc(b.get(), &p, size_t(n) * STATS_N * sizeof(double), err)) return nullptr;
         b->stats_now_all = static_cast<double*>(p);
+        if (dalloc(b.get(), &p, sizeof(double), err)) return nullptr;
+        b->late_flag = static_cast<double*>(p);
         if (dalloc(b.get(), &p, size_t(n) * sizeof(float), err)) return nullptr;
         b->dt_table = static_cast<float*>(p);
         if (cudaMallocHost(&p, size_t(n) * sizeof(float)) != cudaSuccess) { err = "cudaMallocHost failed"; return nullptr; }
@@ -1308,6 +1387,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     for (int i = 0; i < n; ++i) {
         Member& m = b->mem[i];
         m.p = *params[i];
+        if (m.p.friction != 0.0) b->any_friction = true;
         if (make_setup(m.p, bathy[i], bnx[i], bny[i], m.hs, err)) return nullptr;
         // the fused solver needs only the level-0 systems
         m.hs.ABCx.resize(1);
@@ -1341,9 +1421,12 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         float* by = next(); float* bx = next(); float* ba = next();
         d.BY = by; d.BX = bx; d.BA = ba;
         d.R[0] = next(); d.R[1] = next();
-        for (int s = 0; s < 4; ++s) for (int k = 0; k < 3; ++k) d.G[s][k] = next();
-        for (int s = 0; s < 4; ++s) for (int k = 0; k < 2; ++k) d.F[s][k] = next();
-        d.AUX[0] = next(); d.AUX[1] = next();
+        // history slots: HA (float4 {dw/dt, dhu/dt, dhv/dt, F*}, 4 planes) and HB (G*, 1 plane)
+        for (int s = 0; s < 4; ++s) {
+            d.HA[s] = reinterpret_cast<float4*>(q); q += 4 * m.plane;
+            d.HB[s] = next();
+        }
+        d.AUX[0] = next(); d.AUX[1] = next();   // one float2 plane pair
         float* fx[3]; float* fy[3];
         for (int k = 0; k < 3; ++k) fx[k] = next();
         for (int k = 0; k < 3; ++k) fy[k] = next();
@@ -1550,6 +1633,8 @@ int batch_step(cel_batch* b, int nsteps, std::string& err) {
                 ix.sin = out;
             } while (s.time_scheme == CEL_SCHEME_CORRECTOR);
             b->graph_pos = (b->graph_pos + 1) % int(b->graphs.size());
+            b->step_stats_valid = true;
+            b->step_dt.assign(b->dt_host, b->dt_host + b->mem.size());
         } else {
             if (int e = run_physical_step(b, err)) return e;
         }
@@ -1557,15 +1642,19 @@ int batch_step(cel_batch* b, int nsteps, std::string& err) {
     return CEL_OK;
 }
 
-int batch_stats(cel_batch* b, cel_stats* out, std::string& err) {
+int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
     const size_t n = b->mem.size();
-    B_TRY(cudaMemsetAsync(b->stats_now_all, 0, n * STATS_N * sizeof(double), b->stream));
-    k_stats_only<<<std::min(b->ntiles, b->sms * 8), 256, 0, b->stream>>>(b->ddev, b->tiles, b->ntiles, b->ix.sin);
-    B_TRY(cudaGetLastError());
-    std::vector<double> v(n * STATS_N), pass_stats(n * STATS_N);
-    B_TRY(cudaMemcpyAsync(v.data(), b->stats_now_all, v.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
-    B_TRY(cudaMemcpyAsync(pass_stats.data(), b->stats_all, pass_stats.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                          b->stream));
+    const bool at_step = !current && b->step_stats_valid;
+    if (!at_step) {
+        B_TRY(cudaMemsetAsync(b->stats_now_all, 0, n * STATS_N * sizeof(double), b->stream));
+        k_stats_only<<<std::min(b->ntiles, b->sms * 8), 256, 0, b->stream>>>(b->ddev, b->tiles, b->ntiles, b->ix.sin);
+        B_TRY(cudaGetLastError());
+    }
+    std::vector<double> v(n * STATS_N);
+    double late = 0.0;
+    B_TRY(cudaMemcpyAsync(v.data(), at_step ? b->stats_all : b->stats_now_all, v.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost, b->stream));
+    B_TRY(cudaMemcpyAsync(&late, b->late_flag, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     std::vector<double> t64(n);
     for (size_t i = 0; i < n; ++i)
         B_TRY(cudaMemcpyAsync(&t64[i], b->hdev[i].time64, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
@@ -1590,11 +1679,11 @@ int batch_stats(cel_batch* b, cel_stats* out, std::string& err) {
         o.cfl_rate = s[8];
         o.max_froude = std::sqrt(s[9] / g);
         o.health = s[10] != 0 ? CEL_ERR_NUMERIC : 0;
-        // a bounded TMA wait that gave up in the last pass (should never happen) is a CUDA error
-        if (pass_stats[i * STATS_N + 11] != 0) o.health = CEL_ERR_CUDA;
+        // a bounded TMA wait that gave up (should never happen) is a CUDA error of the batch
+        if (late != 0) o.health = CEL_ERR_CUDA;
         o.timestep = double(b->dt_host[i]);
         o.cfl_number = o.cfl_rate * o.timestep;
-        o.total_time = t64[i];
+        o.total_time = at_step ? t64[i] - double(b->step_dt[i]) : t64[i];
         o.time_scheme = b->sch.time_scheme;
     }
     return CEL_OK;
@@ -1634,15 +1723,16 @@ int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     Member& m = b->mem[i];
     const MemberDev& d = b->hdev[i];
-    std::vector<float> a0(m.plane), a1(m.plane);
-    B_TRY(cudaMemcpyAsync(a0.data(), d.AUX[0], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
-    B_TRY(cudaMemcpyAsync(a1.data(), d.AUX[1], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+    // AUX is one float2 plane pair: {max inundated depth, breaking indicator} per texel
+    std::vector<float> a(2 * m.plane);
+    B_TRY(cudaMemcpyAsync(a.data(), d.AUX[0], 2 * m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
     B_TRY(cudaStreamSynchronize(b->stream));
     const int NX = m.hs.NX, NY = m.hs.NY;
     for (int y = 0; y < NY; ++y)
         for (int x = 0; x < NX; ++x) {
             float* o = rgba + (size_t(y) * NX + x) * 4;
-            o[0] = a0[size_t(y) * m.P + x]; o[1] = 0.f; o[2] = 0.f; o[3] = a1[size_t(y) * m.P + x];
+            const size_t k = 2 * (size_t(y) * m.P + x);
+            o[0] = a[k]; o[1] = 0.f; o[2] = 0.f; o[3] = a[k + 1];
         }
     return CEL_OK;
 }
@@ -1719,15 +1809,16 @@ public:
     int reset_timestep(float, float, cel_stats* out) override {
         b->sch.choose_dt(0.f);
         if (!out) return CEL_OK;
-        return batch_stats(b, out, err);
+        return batch_stats(b, out, true, err);
     }
-    int timestep() override { return run_pass(b, err); }
+    int timestep() override { return run_pass(b, b->sch.time_scheme != CEL_SCHEME_CORRECTOR, err); }
     int timesteps(int n) override {
-        for (int i = 0; i < n; ++i) if (int e = run_pass(b, err)) return e;
+        for (int i = 0; i < n; ++i)
+            if (int e = run_pass(b, b->sch.time_scheme != CEL_SCHEME_CORRECTOR, err)) return e;
         return CEL_OK;
     }
     int physical_steps(int n) override { return batch_step(b, n, err); }
-    int get_stats(cel_stats* out) override { return batch_stats(b, out, err); }
+    int get_stats(cel_stats* out) override { return batch_stats(b, out, true, err); }
     int add_solitary_wave(double, double, double, double) override {
         err = "cel_add_solitary_wave is available on CEL_FORM_PLAIN engines";
         return CEL_ERR_STATE;

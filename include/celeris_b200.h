@@ -174,7 +174,13 @@ int cel_batch_create(int n, const cel_params* const* params, const float* const*
 int cel_batch_destroy(cel_batch* b);
 int cel_batch_set_stream(cel_batch* b, void* cuda_stream);
 int cel_batch_step(cel_batch* b, int nsteps);            /* physical steps, all members */
-int cel_batch_stats(cel_batch* b, cel_stats* out);        /* n entries */
+/* n entries: the GetStats totals (FP64) of each member's state at the start of the most recent
+ * step, gathered by that step's first pass as the reference's resetTimestep gathers them before a
+ * step (engine.cpp:1536-1756); total_time is that start time.  Before any step (or after
+ * cel_batch_set_state) they are computed from the current state. */
+int cel_batch_stats(cel_batch* b, cel_stats* out);
+/* n entries: the same totals computed now, from the current state (one extra pass over it). */
+int cel_batch_stats_current(cel_batch* b, cel_stats* out);
 int cel_batch_get_state(cel_batch* b, int i, float* rgba);
 int cel_batch_set_state(cel_batch* b, int i, const float* rgba);
 int cel_batch_get_aux(cel_batch* b, int i, float* rgba);

@@ -81,13 +81,13 @@ def run_gpu(args):
         else:
             b = cb.Batch([(p, z)], form)
             b.use_graph(True)
-            masses = [b.stats()[0]["mass_full"]]
+            masses = [b.stats_current()[0]["mass_full"]]
             done = 0
             while done < args.steps:
                 k = min(args.every, args.steps - done)
                 b.step(k)
                 done += k
-                masses.append(b.stats()[0]["mass_full"])
+                masses.append(b.stats_current()[0]["mass_full"])
             st, aux = b.state(0), b.aux(0)
         out[f"{form}/eta"] = st[..., 0].astype(np.float32)        # w (sea level 0)
         out[f"{form}/maxdepth"] = aux[..., 0].astype(np.float32)  # max inundated depth
