@@ -42,7 +42,6 @@ namespace cel {
 namespace {
 
 constexpr int TX = 32, TY = 16;
-constexpr int NTR = 256;                     // row-solver threads
 constexpr int NTC = 512;                     // column solver threads: CWT columns x (512/CWT) chunks
 constexpr int STATS_N = 12;
 
@@ -687,118 +686,157 @@ __device__ __forceinline__ Affine compose(const Affine& later, const Affine& ear
     return Affine{later.a * earlier.a, later.b + later.a * earlier.b};
 }
 
-// Exclusive scan of affine maps over the threads of a block in thread order; returns the carry
-// (the composition of all earlier maps applied to 0).
-template <int NT>
-__device__ float block_exclusive_carry(Affine mine, Affine* sw) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    Affine inc = mine;
-    for (int off = 1; off < 32; off <<= 1) {
-        Affine o;
-        o.a = __shfl_up_sync(0xffffffffu, inc.a, off);
-        o.b = __shfl_up_sync(0xffffffffu, inc.b, off);
-        if (lane >= off) inc = compose(inc, o);
-    }
-    if (lane == 31) sw[wid] = inc;
-    __syncthreads();
-    if (wid == 0) {
-        Affine v = lane < NT / 32 ? sw[lane] : Affine{1.f, 0.f};
-        for (int off = 1; off < 32; off <<= 1) {
-            Affine o;
-            o.a = __shfl_up_sync(0xffffffffu, v.a, off);
-            o.b = __shfl_up_sync(0xffffffffu, v.b, off);
-            if (lane >= off) v = compose(v, o);
-        }
-        if (lane < NT / 32) sw[32 + lane] = v;  // inclusive totals of warps
-    }
-    __syncthreads();
-    Affine before = wid > 0 ? sw[32 + wid - 1] : Affine{1.f, 0.f};
-    Affine exl;
-    {
-        Affine o;
-        o.a = __shfl_up_sync(0xffffffffu, inc.a, 1);
-        o.b = __shfl_up_sync(0xffffffffu, inc.b, 1);
-        exl = lane > 0 ? o : Affine{1.f, 0.f};
-    }
-    const Affine tot = compose(exl, before);
-    __syncthreads();
-    return tot.b;
+
+
+// Row (x) solves, one warp per row.  A row is swept in tiles of RT = 256 columns; lane j owns the
+// RK = 8 consecutive columns tile*256 + 8j .. +7 (two float4 loads per array, 16-byte aligned
+// since rows start on 128-byte boundaries).  Within a tile each lane runs the recurrence over its
+// 8 columns from zero, the lanes' affine transfer maps are combined by a warp shuffle scan, and
+// the tile's carry passes to the next tile.  Columns outside the interior [2, nx+2) are identity
+// rows (m = c' = 0, right-hand side 0).  The forward values are kept in shared memory for the
+// backward sweep, which walks the tiles in reverse with the mirrored scan and writes
+// hu = hu_base + x (two-sum into the low word in the mixed form).
+constexpr int RK = 8, RT = 32 * RK;
+
+__device__ __forceinline__ Affine shfl_up_affine(const Affine& v, int off) {
+    return Affine{__shfl_up_sync(0xffffffffu, v.a, off), __shfl_up_sync(0xffffffffu, v.b, off)};
+}
+__device__ __forceinline__ Affine shfl_down_affine(const Affine& v, int off) {
+    return Affine{__shfl_down_sync(0xffffffffu, v.a, off), __shfl_down_sync(0xffffffffu, v.b, off)};
+}
+__device__ __forceinline__ void load8(const float* __restrict__ p, int c, int ncol, float v[RK]) {
+    // columns c .. c+7 of a row; a float4 is loaded only when it starts inside [0, ncol) (then it
+    // lies inside the row, whose pitch is a multiple of 32 and at least ncol + 2)
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 a = c < ncol ? __ldg(reinterpret_cast<const float4*>(p + c)) : z;
+    const float4 b = c + 4 < ncol ? __ldg(reinterpret_cast<const float4*>(p + c + 4)) : z;
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
 }
 
-__host__ __device__ __forceinline__ int pidx(int i) { return i + (i >> 5); }
-
 template <bool MIXED>
-__global__ void __launch_bounds__(NTR) k_rows(const MemberDev* __restrict__ mems, const int2* __restrict__ rows,
-                                              int nrows, PassArgs pa) {
-    extern __shared__ float rs[];
-    __shared__ Affine sw[64];
-    for (int it = blockIdx.x; it < nrows; it += gridDim.x) {
+__global__ void __launch_bounds__(256) k_rows(const MemberDev* __restrict__ mems, const int2* __restrict__ rows,
+                                              int nrows, int rowbuf, PassArgs pa) {
+    extern __shared__ float4 rsm4[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    float* __restrict__ ybuf = reinterpret_cast<float*>(rsm4) + size_t(wid) * rowbuf;
+    const int base_buf = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
+    for (int it = blockIdx.x * nw + wid; it < nrows; it += gridDim.x * nw) {
         const int2 rw = rows[it];
         const MemberDev& M = mems[rw.x];
-        const int n = M.c.nx, P = M.P, y = rw.y;
-        const size_t row = size_t(y) * P + 2;
-        const float* r = M.R[0] + row;
-        const float* cp = M.FX[0] + row;
-        const float* inv = M.FX[1] + row;
-        const float* mm = M.FX[2] + row;
-        float* sy = rs;
-        float* sm = rs + pidx(n) + 1;
-        float* sc = sm + pidx(n) + 1;
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += NTR) {
-            sy[pidx(i)] = inv[i] * r[i];
-            sm[pidx(i)] = mm[i];
-            sc[pidx(i)] = cp[i];
+        const int nx = M.c.nx;
+        const size_t row = size_t(rw.y) * M.P;
+        const int ncol = nx + 2;                       // columns [0, nx+2) are swept
+        const int ntile = (ncol + RT - 1) / RT;
+        const float* __restrict__ r = M.R[0] + row;
+        const float* __restrict__ cpp = M.FX[0] + row;
+        const float* __restrict__ inv = M.FX[1] + row;
+        const float* __restrict__ mm = M.FX[2] + row;
+        // ---- forward: y_i = inv_i r_i + m_i y_{i-1} ----
+        float carry = 0.f;
+        for (int ti = 0; ti < ntile; ++ti) {
+            const int c0 = ti * RT + lane * RK;
+            float rv[RK], iv[RK], mv[RK], yv[RK];
+            load8(r, c0, ncol, rv);
+            load8(inv, c0, ncol, iv);
+            load8(mm, c0, ncol, mv);
+            float a = 1.f, b = 0.f;
+#pragma unroll
+            for (int k = 0; k < RK; ++k) {
+                const bool ok = c0 + k >= 2 && c0 + k < ncol;
+                const float m = ok ? mv[k] : 0.f;
+                b = (ok ? iv[k] * rv[k] : 0.f) + m * b;
+                a *= m;
+                yv[k] = b;
+                mv[k] = m;
+            }
+            Affine inc{a, b};
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const Affine o = shfl_up_affine(inc, off);
+                if (lane >= off) inc = compose(inc, o);
+            }
+            const Affine before = shfl_up_affine(inc, 1);
+            const float cin = lane > 0 ? before.b + before.a * carry : carry;
+            float pref = 1.f;
+#pragma unroll
+            for (int k = 0; k < RK; ++k) {
+                pref *= mv[k];
+                yv[k] += pref * cin;
+            }
+            float4* yb = reinterpret_cast<float4*>(ybuf + c0);
+            yb[0] = make_float4(yv[0], yv[1], yv[2], yv[3]);
+            yb[1] = make_float4(yv[4], yv[5], yv[6], yv[7]);
+            carry = __shfl_sync(0xffffffffu, inc.b + inc.a * carry, 31);
         }
-        __syncthreads();
-        const int mc = (n + NTR - 1) / NTR;
-        const int i0 = min(n, int(threadIdx.x) * mc), i1 = min(n, i0 + mc);
-        float yv = 0.f, pa_ = 1.f;
-        for (int i = i0; i < i1; ++i) {
-            const float m = sm[pidx(i)];
-            yv = sy[pidx(i)] + m * yv;
-            pa_ *= m;
-            sy[pidx(i)] = yv;
-        }
-        const float carry = block_exclusive_carry<NTR>(Affine{pa_, yv}, sw);
-        float pref = 1.f;
-        for (int i = i0; i < i1; ++i) {
-            pref *= sm[pidx(i)];
-            sy[pidx(i)] += pref * carry;
-        }
-        // backward: chunks in reverse order; thread j handles chunk NTR-1-j of the scan
-        float z = 0.f, qa = 1.f;
-        for (int i = i1 - 1; i >= i0; --i) {
-            const float cv = sc[pidx(i)];
-            z = sy[pidx(i)] - cv * z;
-            qa *= -cv;
-            sy[pidx(i)] = z;
-        }
-        // reverse scan: reuse the forward scan on reversed thread order via shared memory
-        __shared__ Affine rev[NTR];
-        rev[threadIdx.x] = Affine{qa, z};
-        __syncthreads();
-        const Affine mine = rev[NTR - 1 - threadIdx.x];
-        __syncthreads();
-        const float carry_r = block_exclusive_carry<NTR>(mine, sw);
-        __shared__ float carries[NTR];
-        carries[NTR - 1 - threadIdx.x] = carry_r;
-        __syncthreads();
-        const float cnext = carries[threadIdx.x];
-        float suf = 1.f;
-        const int out = pa.out, base = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
-        float* ohi = M.S[out][1] + row;
-        const float* bhi = M.S[base][1] + row;
-        for (int i = i1 - 1; i >= i0; --i) {
-            suf *= -sc[pidx(i)];
-            const float x = sy[pidx(i)] + suf * cnext;
-            if (MIXED) {
-                float hi = bhi[i], lo = (M.L[base][1] + row)[i];
-                two_sum_add(hi, lo, x);
-                ohi[i] = hi;
-                (M.L[out][1] + row)[i] = lo;
+        // ---- backward: x_i = y_i - c'_i x_{i+1}; hu = base + x (each lane reads back its own
+        // chunks of the forward buffer, so no synchronisation is needed) ----
+        float* __restrict__ ohi = M.S[pa.out][1] + row;
+        const float* __restrict__ bhi = M.S[base_buf][1] + row;
+        float* __restrict__ olo = MIXED ? M.L[pa.out][1] + row : nullptr;
+        const float* __restrict__ blo = MIXED ? M.L[base_buf][1] + row : nullptr;
+        float xcarry = 0.f;
+        for (int ti = ntile - 1; ti >= 0; --ti) {
+            const int c0 = ti * RT + lane * RK;
+            float cv[RK], yv[RK];
+            load8(cpp, c0, ncol, cv);
+            {
+                const float4* yb = reinterpret_cast<const float4*>(ybuf + c0);
+                const float4 p = yb[0], q = yb[1];
+                yv[0] = p.x; yv[1] = p.y; yv[2] = p.z; yv[3] = p.w; yv[4] = q.x; yv[5] = q.y; yv[6] = q.z; yv[7] = q.w;
+            }
+            float z = 0.f, qa = 1.f;
+#pragma unroll
+            for (int k = RK - 1; k >= 0; --k) {
+                const bool ok = c0 + k >= 2 && c0 + k < ncol;
+                const float cn = ok ? -cv[k] : 0.f;
+                z = yv[k] + cn * z;
+                qa *= cn;
+                yv[k] = z;
+                cv[k] = cn;
+            }
+            Affine inc{qa, z};
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const Affine o = shfl_down_affine(inc, off);
+                if (lane + off < 32) inc = compose(inc, o);
+            }
+            const Affine after = shfl_down_affine(inc, 1);
+            const float cnext = lane < 31 ? after.b + after.a * xcarry : xcarry;
+            float suf = 1.f;
+#pragma unroll
+            for (int k = RK - 1; k >= 0; --k) {
+                suf *= cv[k];
+                yv[k] += suf * cnext;
+            }
+            xcarry = __shfl_sync(0xffffffffu, inc.b + inc.a * xcarry, 0);
+            float bh[RK], bl[RK];
+            load8(bhi, c0, ncol, bh);
+            if (MIXED) load8(blo, c0, ncol, bl);
+            float oh[RK], ol[RK];
+#pragma unroll
+            for (int k = 0; k < RK; ++k) {
+                if (MIXED) {
+                    float hi = bh[k], lo = bl[k];
+                    two_sum_add(hi, lo, yv[k]);
+                    oh[k] = hi; ol[k] = lo;
+                } else {
+                    oh[k] = bh[k] + yv[k];
+                }
+            }
+            if (c0 >= 2 && c0 + RK <= ncol) {
+                reinterpret_cast<float4*>(ohi + c0)[0] = make_float4(oh[0], oh[1], oh[2], oh[3]);
+                reinterpret_cast<float4*>(ohi + c0)[1] = make_float4(oh[4], oh[5], oh[6], oh[7]);
+                if (MIXED) {
+                    reinterpret_cast<float4*>(olo + c0)[0] = make_float4(ol[0], ol[1], ol[2], ol[3]);
+                    reinterpret_cast<float4*>(olo + c0)[1] = make_float4(ol[4], ol[5], ol[6], ol[7]);
+                }
             } else {
-                ohi[i] = bhi[i] + x;
+#pragma unroll
+                for (int k = 0; k < RK; ++k)
+                    if (c0 + k >= 2 && c0 + k < ncol) {
+                        ohi[c0 + k] = oh[k];
+                        if (MIXED) olo[c0 + k] = ol[k];
+                    }
             }
         }
     }
@@ -1109,6 +1147,7 @@ struct cel_batch {
     float* dt_table = nullptr;         // per-member time step on the device
     float* dt_host = nullptr;          // pinned mirror of dt_table
     size_t smem_rows = 0, smem_cols = 0;
+    int rowbuf = 0, rows_threads = 256;   // row solver: floats of forward values per warp, threads per CTA
     int grid_stencil = 0, grid_rows = 0, grid_cols = 0;
     int sms = 148;
     bool use_graph = false;
@@ -1214,8 +1253,12 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     }
     {
         TimedLaunch t(&b->tm, b->stream, "tridiag_rows");
-        if (b->mixed) k_rows<true><<<b->grid_rows, NTR, b->smem_rows, b->stream>>>(b->ddev, b->rows, b->nrows, pa);
-        else k_rows<false><<<b->grid_rows, NTR, b->smem_rows, b->stream>>>(b->ddev, b->rows, b->nrows, pa);
+        if (b->mixed)
+            k_rows<true><<<b->grid_rows, b->rows_threads, b->smem_rows, b->stream>>>(b->ddev, b->rows, b->nrows,
+                                                                                    b->rowbuf, pa);
+        else
+            k_rows<false><<<b->grid_rows, b->rows_threads, b->smem_rows, b->stream>>>(b->ddev, b->rows, b->nrows,
+                                                                                     b->rowbuf, pa);
     }
     B_TRY(cudaEventRecord(b->ev_join, b->side));
     B_TRY(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
@@ -1551,9 +1594,17 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         b->ddev = static_cast<MemberDev*>(p);
         cudaMemcpy(b->ddev, b->hdev.data(), sizeof(MemberDev) * n, cudaMemcpyHostToDevice);
     }
-    b->smem_rows = sizeof(float) * 3 * (pidx(max_nx) + 1);
+    // row solver: one warp per row, each with a buffer of the row's forward values (whole tiles)
+    b->rowbuf = (max_nx + 2 + RT - 1) / RT * RT;
+    {
+        const size_t per_warp = sizeof(float) * size_t(b->rowbuf);
+        const int warps = int(std::min<size_t>(8, (200 * 1024) / per_warp));
+        if (warps < 1) { err = "domain too large for the fused solver"; return nullptr; }
+        b->rows_threads = 32 * warps;
+        b->smem_rows = per_warp * warps;
+    }
     b->smem_cols = sizeof(float) * size_t(max_ny) * b->cw;
-    if (b->smem_cols + 8192 > 227 * 1024 || b->smem_rows + 8192 > 227 * 1024) { err = "domain too large for the fused solver"; return nullptr; }
+    if (b->smem_cols + 8192 > 227 * 1024) { err = "domain too large for the fused solver"; return nullptr; }
     cudaFuncSetAttribute(k_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
     cudaFuncSetAttribute(k_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
     cudaFuncSetAttribute(k_cols<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
@@ -1564,8 +1615,9 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         int occ = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_march<true>, MW, 0);
         b->grid_stencil = std::max(1, std::min(b->nmtiles, b->sms * std::max(occ, 1)));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rows<false>, NTR, b->smem_rows);
-        b->grid_rows = std::max(1, std::min(b->nrows, b->sms * std::max(occ, 1) * 4));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rows<true>, b->rows_threads, b->smem_rows);
+        const int wpc = b->rows_threads / 32;
+        b->grid_rows = std::max(1, std::min((b->nrows + wpc - 1) / wpc, b->sms * std::max(occ, 1)));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cols<false, 16>, NTC, b->smem_cols);
         b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
     }
