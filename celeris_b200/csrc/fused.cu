@@ -845,7 +845,12 @@ __global__ void __launch_bounds__(256) k_rows(const MemberDev* __restrict__ mems
 template <bool MIXED, int CW>
 __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems, const int2* __restrict__ bands,
                                               int nbands, PassArgs pa) {
+    // Column (y) solves: a CTA takes a band of CW adjacent columns, thread (c, k) runs chunk k of
+    // column c; a half warp reads CW consecutive floats of one row.  Every loop over a chunk's rows
+    // issues the loads of CU rows before using them, so each thread keeps several rows of
+    // requests in flight (the recurrences themselves are serial).
     constexpr int NCH = NTC / CW;
+    constexpr int CU = 8;
     extern __shared__ float cs[];
     __shared__ float carP[NCH][CW], carY[NCH][CW], carry_in[NCH][CW];
     const int c = threadIdx.x % CW, k = threadIdx.x / CW;
@@ -857,19 +862,30 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
         const bool col_ok = gx >= 2 && gx < M.c.nx + 2;
         const int mc = (n + NCH - 1) / NCH;
         const int i0 = min(n, k * mc), i1 = min(n, i0 + mc);
-        const float* r = M.R[1];
-        const float* cp = M.FYF[0];
-        const float* inv = M.FYF[1];
-        const float* mm = M.FYF[2];
+        const float* __restrict__ r = M.R[1] + gx;
+        const float* __restrict__ cp = M.FYF[0] + gx;
+        const float* __restrict__ inv = M.FYF[1] + gx;
+        const float* __restrict__ mm = M.FYF[2] + gx;
+        auto at = [&](int i) { return size_t(i + 2) * P; };   // row offset of system element i
         __syncthreads();
         float yv = 0.f, pa_ = 1.f;
         if (col_ok)
-            for (int i = i0; i < i1; ++i) {
-                const size_t gi = size_t(i + 2) * P + gx;
-                const float m = mm[gi];
-                yv = inv[gi] * r[gi] + m * yv;
-                pa_ *= m;
-                cs[i * CW + c] = yv;
+            for (int i = i0; i < i1; i += CU) {
+                float mv[CU], iv[CU], rv[CU];
+#pragma unroll
+                for (int u = 0; u < CU; ++u) {
+                    const bool ok = i + u < i1;
+                    mv[u] = ok ? __ldg(mm + at(i + u)) : 0.f;
+                    iv[u] = ok ? __ldg(inv + at(i + u)) : 0.f;
+                    rv[u] = ok ? __ldg(r + at(i + u)) : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < CU; ++u)
+                    if (i + u < i1) {
+                        yv = iv[u] * rv[u] + mv[u] * yv;
+                        pa_ *= mv[u];
+                        cs[(i + u) * CW + c] = yv;
+                    }
             }
         carP[k][c] = pa_;
         carY[k][c] = yv;
@@ -886,17 +902,28 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
         if (col_ok) {
             const float cin = carry_in[k][c];
             float pref = 1.f;
-            for (int i = i0; i < i1; ++i) {
-                const size_t gi = size_t(i + 2) * P + gx;
-                pref *= mm[gi];
-                cs[i * CW + c] += pref * cin;
+            for (int i = i0; i < i1; i += CU) {
+                float mv[CU];
+#pragma unroll
+                for (int u = 0; u < CU; ++u) mv[u] = (i + u < i1) ? __ldg(mm + at(i + u)) : 0.f;
+#pragma unroll
+                for (int u = 0; u < CU; ++u)
+                    if (i + u < i1) {
+                        pref *= mv[u];
+                        cs[(i + u) * CW + c] += pref * cin;
+                    }
             }
-            for (int i = i1 - 1; i >= i0; --i) {
-                const size_t gi = size_t(i + 2) * P + gx;
-                const float cv = cp[gi];
-                z = cs[i * CW + c] - cv * z;
-                qa *= -cv;
-                cs[i * CW + c] = z;
+            for (int i = i1 - 1; i >= i0; i -= CU) {
+                float cv[CU];
+#pragma unroll
+                for (int u = 0; u < CU; ++u) cv[u] = (i - u >= i0) ? __ldg(cp + at(i - u)) : 0.f;
+#pragma unroll
+                for (int u = 0; u < CU; ++u)
+                    if (i - u >= i0) {
+                        z = cs[(i - u) * CW + c] - cv[u] * z;
+                        qa *= -cv[u];
+                        cs[(i - u) * CW + c] = z;
+                    }
             }
         }
         __syncthreads();
@@ -915,18 +942,33 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
             const float cnext = carry_in[k][c];
             float suf = 1.f;
             const int out = pa.out, base = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
-            for (int i = i1 - 1; i >= i0; --i) {
-                const size_t gi = size_t(i + 2) * P + gx;
-                suf *= -cp[gi];
-                const float x = cs[i * CW + c] + suf * cnext;
-                if (MIXED) {
-                    float hi = M.S[base][2][gi], lo = M.L[base][2][gi];
-                    two_sum_add(hi, lo, x);
-                    M.S[out][2][gi] = hi;
-                    M.L[out][2][gi] = lo;
-                } else {
-                    M.S[out][2][gi] = M.S[base][2][gi] + x;
+            const float* __restrict__ bhi = M.S[base][2] + gx;
+            float* __restrict__ ohi = M.S[out][2] + gx;
+            const float* __restrict__ blo = MIXED ? M.L[base][2] + gx : nullptr;
+            float* __restrict__ olo = MIXED ? M.L[out][2] + gx : nullptr;
+            for (int i = i1 - 1; i >= i0; i -= CU) {
+                float cv[CU], bh[CU], bl[CU];
+#pragma unroll
+                for (int u = 0; u < CU; ++u) {
+                    const bool ok = i - u >= i0;
+                    cv[u] = ok ? __ldg(cp + at(i - u)) : 0.f;
+                    bh[u] = ok ? bhi[at(i - u)] : 0.f;
+                    bl[u] = (MIXED && ok) ? blo[at(i - u)] : 0.f;
                 }
+#pragma unroll
+                for (int u = 0; u < CU; ++u)
+                    if (i - u >= i0) {
+                        suf *= -cv[u];
+                        const float x = cs[(i - u) * CW + c] + suf * cnext;
+                        if (MIXED) {
+                            float hi = bh[u], lo = bl[u];
+                            two_sum_add(hi, lo, x);
+                            ohi[at(i - u)] = hi;
+                            olo[at(i - u)] = lo;
+                        } else {
+                            ohi[at(i - u)] = bh[u] + x;
+                        }
+                    }
             }
         }
     }
