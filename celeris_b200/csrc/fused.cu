@@ -731,14 +731,23 @@ __global__ void __launch_bounds__(256) k_rows(const MemberDev* __restrict__ mems
         const float* __restrict__ cpp = M.FX[0] + row;
         const float* __restrict__ inv = M.FX[1] + row;
         const float* __restrict__ mm = M.FX[2] + row;
-        // ---- forward: y_i = inv_i r_i + m_i y_{i-1} ----
+        // ---- forward: y_i = inv_i r_i + m_i y_{i-1}; the next tile's loads are issued before the
+        // current tile is computed ----
         float carry = 0.f;
+        float rn[RK], in_[RK], mn[RK];
+        load8(r, lane * RK, ncol, rn);
+        load8(inv, lane * RK, ncol, in_);
+        load8(mm, lane * RK, ncol, mn);
         for (int ti = 0; ti < ntile; ++ti) {
             const int c0 = ti * RT + lane * RK;
             float rv[RK], iv[RK], mv[RK], yv[RK];
-            load8(r, c0, ncol, rv);
-            load8(inv, c0, ncol, iv);
-            load8(mm, c0, ncol, mv);
+#pragma unroll
+            for (int k = 0; k < RK; ++k) { rv[k] = rn[k]; iv[k] = in_[k]; mv[k] = mn[k]; }
+            if (ti + 1 < ntile) {
+                load8(r, c0 + RT, ncol, rn);
+                load8(inv, c0 + RT, ncol, in_);
+                load8(mm, c0 + RT, ncol, mn);
+            }
             float a = 1.f, b = 0.f;
 #pragma unroll
             for (int k = 0; k < RK; ++k) {
@@ -775,10 +784,23 @@ __global__ void __launch_bounds__(256) k_rows(const MemberDev* __restrict__ mems
         float* __restrict__ olo = MIXED ? M.L[pa.out][1] + row : nullptr;
         const float* __restrict__ blo = MIXED ? M.L[base_buf][1] + row : nullptr;
         float xcarry = 0.f;
+        float cn_[RK], bhn[RK], bln[RK];
+        {
+            const int cl = (ntile - 1) * RT + lane * RK;
+            load8(cpp, cl, ncol, cn_);
+            load8(bhi, cl, ncol, bhn);
+            if (MIXED) load8(blo, cl, ncol, bln);
+        }
         for (int ti = ntile - 1; ti >= 0; --ti) {
             const int c0 = ti * RT + lane * RK;
-            float cv[RK], yv[RK];
-            load8(cpp, c0, ncol, cv);
+            float cv[RK], yv[RK], bh[RK], bl[RK];
+#pragma unroll
+            for (int k = 0; k < RK; ++k) { cv[k] = cn_[k]; bh[k] = bhn[k]; bl[k] = MIXED ? bln[k] : 0.f; }
+            if (ti > 0) {
+                load8(cpp, c0 - RT, ncol, cn_);
+                load8(bhi, c0 - RT, ncol, bhn);
+                if (MIXED) load8(blo, c0 - RT, ncol, bln);
+            }
             {
                 const float4* yb = reinterpret_cast<const float4*>(ybuf + c0);
                 const float4 p = yb[0], q = yb[1];
@@ -809,9 +831,6 @@ __global__ void __launch_bounds__(256) k_rows(const MemberDev* __restrict__ mems
                 yv[k] += suf * cnext;
             }
             xcarry = __shfl_sync(0xffffffffu, inc.b + inc.a * xcarry, 0);
-            float bh[RK], bl[RK];
-            load8(bhi, c0, ncol, bh);
-            if (MIXED) load8(blo, c0, ncol, bl);
             float oh[RK], ol[RK];
 #pragma unroll
             for (int k = 0; k < RK; ++k) {
@@ -850,6 +869,8 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
     // issues the loads of CU rows before using them, so each thread keeps several rows of
     // requests in flight (the recurrences themselves are serial).
     constexpr int NCH = NTC / CW;
+    constexpr int G = NCH / 32;   // chunks per lane in the carry scans (one warp per column)
+    static_assert(NCH % 32 == 0 && CW <= NTC / 32, "carry scans: one warp per column, G chunks per lane");
     constexpr int CU = 8;
     extern __shared__ float cs[];
     __shared__ float carP[NCH][CW], carY[NCH][CW], carry_in[NCH][CW];
@@ -890,11 +911,24 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
         carP[k][c] = pa_;
         carY[k][c] = yv;
         __syncthreads();
-        if (k == 0) {
-            float cur = 0.f;
-            for (int q = 0; q < NCH; ++q) {
-                carry_in[q][c] = cur;
-                cur = carY[q][c] + carP[q][c] * cur;
+        // carries into the chunks of each column: warp w < CW scans column w's 32 chunk maps
+        if (threadIdx.x < 32 * CW) {
+            const int col = threadIdx.x >> 5, q = threadIdx.x & 31;
+            Affine loc{1.f, 0.f};
+#pragma unroll
+            for (int g = 0; g < G; ++g) loc = compose(Affine{carP[q * G + g][col], carY[q * G + g][col]}, loc);
+            Affine inc = loc;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const Affine o = Affine{__shfl_up_sync(0xffffffffu, inc.a, off), __shfl_up_sync(0xffffffffu, inc.b, off)};
+                if (q >= off) inc = compose(inc, o);
+            }
+            const float before = __shfl_up_sync(0xffffffffu, inc.b, 1);
+            float cur = q > 0 ? before : 0.f;
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                carry_in[q * G + g][col] = cur;
+                cur = carY[q * G + g][col] + carP[q * G + g][col] * cur;
             }
         }
         __syncthreads();
@@ -930,11 +964,24 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
         carP[k][c] = qa;
         carY[k][c] = z;
         __syncthreads();
-        if (k == 0) {
-            float cur = 0.f;
-            for (int q = NCH - 1; q >= 0; --q) {
-                carry_in[q][c] = cur;
-                cur = carY[q][c] + carP[q][c] * cur;
+        // carries from the chunks below (higher rows) in the backward sweep: the mirrored scan
+        if (threadIdx.x < 32 * CW) {
+            const int col = threadIdx.x >> 5, q = threadIdx.x & 31;
+            Affine loc{1.f, 0.f};
+#pragma unroll
+            for (int g = G - 1; g >= 0; --g) loc = compose(Affine{carP[q * G + g][col], carY[q * G + g][col]}, loc);
+            Affine inc = loc;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const Affine o = Affine{__shfl_down_sync(0xffffffffu, inc.a, off), __shfl_down_sync(0xffffffffu, inc.b, off)};
+                if (q + off < 32) inc = compose(inc, o);
+            }
+            const float after = __shfl_down_sync(0xffffffffu, inc.b, 1);
+            float cur = q < 31 ? after : 0.f;
+#pragma unroll
+            for (int g = G - 1; g >= 0; --g) {
+                carry_in[q * G + g][col] = cur;
+                cur = carY[q * G + g][col] + carP[q * G + g][col] * cur;
             }
         }
         __syncthreads();
