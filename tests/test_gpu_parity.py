@@ -128,3 +128,35 @@ def test_flume_config1_plain_1000_steps(celeris):
     s_gpu = eng.reset_timestep()
     s_ref = ref.reset_timestep()
     assert abs(s_gpu["mass_full"] - s_ref["mass_full"]) <= 1e-6 * s_ref["mass_full"]
+
+
+def test_tall_domain_narrow_column_bands(celeris):
+    """ny above ~3,500 rows makes the column solver use 8-column bands (64 chunks per column)."""
+    p, z, bnx, bny = cases.small_case(36, 3700, "solid", correction_steps=1)
+    ref = O.Oracle(p, z, bnx, bny, "f64")
+    b = celeris.Batch([(p, z)], "mixed")
+    ref.physical_steps(60)
+    b.step(60)
+    a = b.state(0)
+    assert np.isfinite(a).all()
+    assert eta_rms(a, ref.state()) <= 1e-4
+
+
+def test_batch_stats_describe_the_start_of_the_last_step(celeris):
+    """cel_batch_stats (gathered by the first pass of a step) equals the statistics of the state
+    the step started from (cel_batch_stats_current one step earlier)."""
+    members = [_case(k, nx=48, ny=32, N=1)[:4] for k in ["mixed", "sponge"]]
+    b1 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    b2 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    b1.step(11)
+    before = b1.stats_current()
+    b2.step(12)
+    fused = b2.stats()
+    for s, f in zip(before, fused):
+        # sums of depth agree to the FP64 reduction order; velocity-derived totals also carry the
+        # FP32 difference between the stencil's reciprocal square root and a division
+        for k in ("mass", "mass_full", "potential_energy", "max_depth"):
+            assert f[k] == pytest.approx(s[k], rel=1e-9, abs=1e-12), k
+        for k in ("kinetic_energy", "max_speed", "cfl_rate"):
+            assert f[k] == pytest.approx(s[k], rel=1e-6, abs=1e-12), k
+        assert f["total_time"] == pytest.approx(s["total_time"], rel=1e-12)
