@@ -56,7 +56,9 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         objs.append(o)
         if os.path.exists(o) and os.path.getmtime(o) > max(os.path.getmtime(s), hdr_mtime) and not ptxas_info:
             continue
-        cmd = [nvcc(), *_host_compiler(), *ARCH, *COMMON, *extra, "-I", inc, "-c", s, "-o", o]
+        # CEL_NVCC_FLAGS: extra nvcc flags for the CUDA units (tuning builds, e.g. -DCEL_MARCH_MIN_CTAS=5)
+        tune = os.environ.get("CEL_NVCC_FLAGS", "").split() if src.endswith(".cu") else []
+        cmd = [nvcc(), *_host_compiler(), *ARCH, *COMMON, *extra, *tune, "-I", inc, "-c", s, "-o", o]
         if ptxas_info and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
         if verbose:

@@ -145,6 +145,11 @@ __device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h,
 // registers (the north face of row t becomes the south side of the y flux), east/west faces and
 // the x fluxes are exchanged through shared memory.  Two barriers per row.
 // ---------------------------------------------------------------------------------------------
+// CTAs per SM the stencil's register budget is sized for (65,536 / (128 x this) registers a thread)
+#ifndef CEL_MARCH_MIN_CTAS
+#define CEL_MARCH_MIN_CTAS 5
+#endif
+constexpr int MARCH_MIN_CTAS = CEL_MARCH_MIN_CTAS;
 constexpr int MW = 128;          // threads = columns with faces per row
 constexpr int MO = MW - 2;       // output columns per strip
 constexpr int MH = 64;           // rows per strip
@@ -321,7 +326,7 @@ __device__ __forceinline__ void face_flux(float hm, float um, float vm, float hp
 //   AUX = float2 {max inundated depth, breaking} (2 planes) | FX (3) | FY (3)
 // ---------------------------------------------------------------------------------------------
 template <bool MIXED>
-__global__ void __launch_bounds__(MW, 6) k_march(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
+__global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
                                                  int ntiles, PassArgs pa) {
     __shared__ __align__(128) float ring[6 * FSTR];
     __shared__ float dring[RING * DSTR];  // still-water depth max(0, sea level - BA) of each ring row
