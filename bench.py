@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the per-domain plain FP32 comparison")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="0 skips the CPU baseline")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA graphs (profiling)")
+    ap.add_argument("--tune-steps", type=int, default=6, help="steps per autotuner candidate (0 keeps the defaults)")
     return ap.parse_args()
 
 
@@ -175,10 +176,13 @@ def main():
     batch = cb.Batch([(m[0], m[1]) for m in members], args.form)
     stream = torch.cuda.Stream()
     batch.set_stream(stream.cuda_stream)
-    batch.use_graph(not args.no_graph)
     cells = batch.cells
     N = members[0][0].correction_steps
     with torch.cuda.stream(stream):
+        # the autotuner times each (band width, strip height) candidate for a few steps; those
+        # steps are warm-up too and lie outside the timed region
+        batch.use_graph(not args.no_graph)
+        tuned = batch.autotune(args.tune_steps) if args.tune_steps > 0 else None
         batch.step(max(3, args.warmup))
     torch.cuda.synchronize()
 
@@ -296,7 +300,10 @@ def main():
                        "cells_per_gpu": cells, "correction_steps": N, "cuda_graph": not args.no_graph,
                        "l2": "working set (%.1f GB) larger than L2 (126 MB); no flush" % (
                            cells * 4 * (42 + (9 if args.form == "mixed" else 0)) / 1e9),
-                       "parallelism": f"ensemble sharded by domain over {world} GPU(s)"},
+                       "parallelism": f"ensemble sharded by domain over {world} GPU(s)",
+                       "tuning": {"column_band_width": batch.tuning[0], "strip_height": batch.tuning[1],
+                                  "autotuned": tuned is not None,
+                                  "pcr_switch": "none (Thomas factors + scans; no cyclic-reduction stage)"}},
             "e2e": {"value": e2e_value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

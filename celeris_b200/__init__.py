@@ -216,6 +216,22 @@ class Batch:
         check(lib().cel_batch_get_aux(self.h, i, _fp(out)))
         return out
 
+    def set_tuning(self, band_width: int = 0, strip_height: int = 0):
+        """Column-solver band width (8/16/32) and stencil strip height (0 keeps the current value)."""
+        check(lib().cel_batch_set_tuning(self.h, band_width, strip_height, 0))
+
+    @property
+    def tuning(self) -> tuple:
+        tx, ty = C.c_int(), C.c_int()
+        check(lib().cel_batch_get_tuning(self.h, C.byref(tx), C.byref(ty)))
+        return tx.value, ty.value
+
+    def autotune(self, steps: int = 5) -> dict:
+        """Times each candidate for `steps` steps and keeps the fastest (the members advance)."""
+        tx, ty, ms = C.c_int(), C.c_int(), C.c_double()
+        check(lib().cel_batch_autotune(self.h, steps, C.byref(tx), C.byref(ty), C.byref(ms)))
+        return {"band_width": tx.value, "strip_height": ty.value, "ms_per_step": ms.value}
+
     def kernel_timing(self, enable: bool = True):
         check(lib().cel_batch_kernel_timing(self.h, int(enable)))
 

@@ -339,6 +339,14 @@ int cel_batch_set_tuning(cel_batch* b, int tx, int ty, int pcr) {
     BAT(b);
     CEL_GUARD_BEGIN BRET(cel::batch_set_tuning(b, tx, ty, pcr, err)); CEL_GUARD_END
 }
+int cel_batch_get_tuning(const cel_batch* b, int* tx, int* ty) {
+    if (!b) { set_error("null batch"); return CEL_ERR_ARG; }
+    return cel::batch_get_tuning(b, tx, ty);
+}
+int cel_batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* ms) {
+    BAT(b);
+    CEL_GUARD_BEGIN BRET(cel::batch_autotune(b, steps, tx, ty, ms, err)); CEL_GUARD_END
+}
 int cel_batch_kernel_timing(cel_batch* b, int enable) {
     BAT(b);
     cel::batch_timer(b)->enabled = enable != 0;

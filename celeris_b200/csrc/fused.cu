@@ -152,7 +152,7 @@ __device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h,
 constexpr int MARCH_MIN_CTAS = CEL_MARCH_MIN_CTAS;
 constexpr int MW = 128;          // threads = columns with faces per row
 constexpr int MO = MW - 2;       // output columns per strip
-constexpr int MH = 64;           // rows per strip
+constexpr int MH_DEFAULT = 64;   // rows per strip unless tuned (each work item carries its height)
 constexpr int RING = 7;          // state / bottom rows resident in shared memory (PREFETCH + 5)
 constexpr int RBOX = 136;        // TMA box width in floats (covers columns x0-2 .. x0+127)
 constexpr int RSTR = 160;        // ring row stride in floats (640 B, a multiple of 128 B)
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
         float* __restrict__ B = M.base;
         const size_t PL = M.plane;
         const CUtensorMap* tm = M.tmaps;
-        const int x0 = tl.y, y0 = tl.z;
+        const int x0 = tl.y, y0 = tl.z, MH = tl.w;   // strip: columns x0 .. x0+MO-1, rows y0 .. y0+MH-1
         const int xs = (x0 - 2) & ~3;          // TMA box start, 16-byte aligned
         const int xc = x0 - 1 + tid;           // this thread's column
         const int rc0 = xc - xs;               // its ring column (1 .. 131)
@@ -874,8 +874,10 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
     // issues the loads of CU rows before using them, so each thread keeps several rows of
     // requests in flight (the recurrences themselves are serial).
     constexpr int NCH = NTC / CW;
-    constexpr int G = NCH / 32;   // chunks per lane in the carry scans (one warp per column)
-    static_assert(NCH % 32 == 0 && CW <= NTC / 32, "carry scans: one warp per column, G chunks per lane");
+    // carry scans: one warp per column; each of the first LN lanes holds G consecutive chunks
+    constexpr int G = NCH >= 32 ? NCH / 32 : 1;
+    constexpr int LN = NCH >= 32 ? 32 : NCH;
+    static_assert(NCH % LN == 0, "carry scan layout");
     constexpr int CU = 8;
     extern __shared__ float cs[];
     __shared__ float carP[NCH][CW], carY[NCH][CW], carry_in[NCH][CW];
@@ -917,11 +919,13 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
         carY[k][c] = yv;
         __syncthreads();
         // carries into the chunks of each column: warp w < CW scans column w's 32 chunk maps
-        if (threadIdx.x < 32 * CW) {
-            const int col = threadIdx.x >> 5, q = threadIdx.x & 31;
+        for (int col = threadIdx.x >> 5; col < CW; col += NTC / 32) {   // warp-uniform loop
+            const int q = threadIdx.x & 31;
             Affine loc{1.f, 0.f};
+            if (q < LN) {
 #pragma unroll
-            for (int g = 0; g < G; ++g) loc = compose(Affine{carP[q * G + g][col], carY[q * G + g][col]}, loc);
+                for (int g = 0; g < G; ++g) loc = compose(Affine{carP[q * G + g][col], carY[q * G + g][col]}, loc);
+            }
             Affine inc = loc;
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
@@ -930,10 +934,12 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
             }
             const float before = __shfl_up_sync(0xffffffffu, inc.b, 1);
             float cur = q > 0 ? before : 0.f;
+            if (q < LN) {
 #pragma unroll
-            for (int g = 0; g < G; ++g) {
-                carry_in[q * G + g][col] = cur;
-                cur = carY[q * G + g][col] + carP[q * G + g][col] * cur;
+                for (int g = 0; g < G; ++g) {
+                    carry_in[q * G + g][col] = cur;
+                    cur = carY[q * G + g][col] + carP[q * G + g][col] * cur;
+                }
             }
         }
         __syncthreads();
@@ -970,11 +976,13 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
         carY[k][c] = z;
         __syncthreads();
         // carries from the chunks below (higher rows) in the backward sweep: the mirrored scan
-        if (threadIdx.x < 32 * CW) {
-            const int col = threadIdx.x >> 5, q = threadIdx.x & 31;
+        for (int col = threadIdx.x >> 5; col < CW; col += NTC / 32) {   // warp-uniform loop
+            const int q = threadIdx.x & 31;
             Affine loc{1.f, 0.f};
+            if (q < LN) {
 #pragma unroll
-            for (int g = G - 1; g >= 0; --g) loc = compose(Affine{carP[q * G + g][col], carY[q * G + g][col]}, loc);
+                for (int g = G - 1; g >= 0; --g) loc = compose(Affine{carP[q * G + g][col], carY[q * G + g][col]}, loc);
+            }
             Affine inc = loc;
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
@@ -983,10 +991,12 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
             }
             const float after = __shfl_down_sync(0xffffffffu, inc.b, 1);
             float cur = q < 31 ? after : 0.f;
+            if (q < LN) {
 #pragma unroll
-            for (int g = G - 1; g >= 0; --g) {
-                carry_in[q * G + g][col] = cur;
-                cur = carY[q * G + g][col] + carP[q * G + g][col] * cur;
+                for (int g = G - 1; g >= 0; --g) {
+                    carry_in[q * G + g][col] = cur;
+                    cur = carY[q * G + g][col] + carP[q * G + g][col] * cur;
+                }
             }
         }
         __syncthreads();
@@ -1249,8 +1259,9 @@ struct cel_batch {
     std::vector<cel::Idx> graph_idx;   // index state at the start of each captured step
     int graph_pos = 0;
     long long cells = 0;
-    int tile_x = cel::TX, tile_y = cel::TY, pcr_switch = 0;
-    int cw = 16;
+    int cw = 16;                        // column solver band width (columns per CTA)
+    int mh = cel::MH_DEFAULT;           // stencil strip height (rows per CTA work item)
+    int max_nx = 0, max_ny = 0;
 };
 
 namespace cel {
@@ -1321,6 +1332,13 @@ int upload_state(cel_batch* b, int i, const float* rgba, std::string& err) {
     return CEL_OK;
 }
 
+using ColsKernel = void (*)(const MemberDev*, const int2*, int, PassArgs);
+ColsKernel cols_kernel(bool mixed, int cw) {
+    if (cw == 32) return mixed ? k_cols<true, 32> : k_cols<false, 32>;
+    if (cw == 16) return mixed ? k_cols<true, 16> : k_cols<false, 16>;
+    return mixed ? k_cols<true, 8> : k_cols<false, 8>;
+}
+
 int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     const size_t nm = b->mem.size();
     if (pa.stats) B_TRY(cudaMemsetAsync(b->stats_all, 0, nm * STATS_N * sizeof(double), b->stream));
@@ -1337,13 +1355,8 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     B_TRY(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     {
         TimedLaunch t(&b->tm, b->side, "tridiag_cols");
-        if (b->cw == 16) {
-            if (b->mixed) k_cols<true, 16><<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
-            else k_cols<false, 16><<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
-        } else {
-            if (b->mixed) k_cols<true, 8><<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
-            else k_cols<false, 8><<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
-        }
+        auto* kc = cols_kernel(b->mixed, b->cw);
+        kc<<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
     }
     {
         TimedLaunch t(&b->tm, b->stream, "tridiag_rows");
@@ -1479,6 +1492,51 @@ void byte_model(int form, int N, double& stencil, double& step) {
     step = (st_pred + tri) + N * (st_corr + tri);
 }
 
+// (Re)builds the stencil strips (height mh) and the column bands (width cw) of a batch, sizes the
+// column solver's shared memory and grids, and drops captured graphs (they hold the old lists).
+int configure_work(cel_batch* b, int cw, int mh, std::string& err) {
+    if (cw != 8 && cw != 16 && cw != 32) { err = "column band width must be 8, 16 or 32"; return CEL_ERR_ARG; }
+    if (mh < 8 || mh > 1024) { err = "strip height must be in [8, 1024]"; return CEL_ERR_ARG; }
+    const size_t smem_cols = sizeof(float) * size_t(b->max_ny) * cw;
+    if (smem_cols + 8192 > 227 * 1024) { err = "column band too wide for the tallest member (shared memory)"; return CEL_ERR_ARG; }
+    std::vector<int4> mt;
+    std::vector<int2> bd;
+    for (int i = 0; i < int(b->mem.size()); ++i) {
+        const HostSetup& hs = b->mem[i].hs;
+        for (int y0 = 2; y0 < hs.ny + 2; y0 += mh)
+            for (int x0 = 2; x0 < hs.nx + 2; x0 += MO) mt.push_back(make_int4(i, x0, y0, mh));
+        // bands start on multiples of the band width so column loads are sector aligned
+        for (int x0 = 0; x0 < hs.nx + 2; x0 += cw) bd.push_back(make_int2(i, x0));
+    }
+    free_graphs(b);
+    B_TRY(cudaStreamSynchronize(b->stream));
+    B_TRY(cudaStreamSynchronize(b->side));
+    for (void* p : {static_cast<void*>(b->mtiles), static_cast<void*>(b->bands)})
+        if (p) { cudaFree(p); b->allocs.erase(std::remove(b->allocs.begin(), b->allocs.end(), p), b->allocs.end()); }
+    b->mtiles = nullptr;
+    b->bands = nullptr;
+    void* p = nullptr;
+    if (dalloc(b, &p, mt.size() * sizeof(int4), err)) return CEL_ERR_CUDA;
+    b->mtiles = static_cast<int4*>(p);
+    if (dalloc(b, &p, bd.size() * sizeof(int2), err)) return CEL_ERR_CUDA;
+    b->bands = static_cast<int2*>(p);
+    B_TRY(cudaMemcpy(b->mtiles, mt.data(), mt.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    B_TRY(cudaMemcpy(b->bands, bd.data(), bd.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    b->nmtiles = int(mt.size());
+    b->nbands = int(bd.size());
+    b->cw = cw;
+    b->mh = mh;
+    b->smem_cols = smem_cols;
+    ColsKernel kc = cols_kernel(b->mixed, cw);
+    B_TRY(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_cols)));
+    int occ = 1;
+    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc, NTC, smem_cols));
+    b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
+    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->mixed ? k_march<true> : k_march<false>, MW, 0));
+    b->grid_stencil = std::max(1, std::min(b->nmtiles, b->sms * std::max(occ, 1)));
+    return CEL_OK;
+}
+
 cel_batch* batch_create(int n, const cel_params* const* params, const float* const* bathy, const int* bnx,
                         const int* bny, int form, std::string& err) {
     std::unique_ptr<cel_batch> b(new cel_batch());
@@ -1518,8 +1576,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         if (cudaMallocHost(&p, size_t(n) * sizeof(float)) != cudaSuccess) { err = "cudaMallocHost failed"; return nullptr; }
         b->dt_host = static_cast<float*>(p);
     }
-    std::vector<int4> tiles, mtiles;
-    std::vector<int2> rows, bands, bitems[4];
+    std::vector<int4> tiles;
+    std::vector<int2> rows, bitems[4];
     int max_nx = 0, max_ny = 0;
     for (int i = 0; i < n; ++i) {
         Member& m = b->mem[i];
@@ -1650,16 +1708,10 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         // work lists
         for (int y0 = 2; y0 < m.hs.ny + 2; y0 += TY)
             for (int x0 = 2; x0 < m.hs.nx + 2; x0 += TX) tiles.push_back(make_int4(i, x0, y0, 0));
-        for (int y0 = 2; y0 < m.hs.ny + 2; y0 += MH)
-            for (int x0 = 2; x0 < m.hs.nx + 2; x0 += MO) mtiles.push_back(make_int4(i, x0, y0, 0));
         for (int y = 2; y < m.hs.ny + 2; ++y) rows.push_back(make_int2(i, y));
     }
-    // column bands: 16 columns per CTA, or 8 for tall domains (shared-memory capacity)
-    b->cw = (size_t(max_ny) * 16 * sizeof(float) + 8192 <= 227 * 1024) ? 16 : 8;
-    for (int i = 0; i < n; ++i) {
-        // bands start on multiples of the band width so column loads are sector aligned
-        for (int x0 = 0; x0 < b->mem[i].hs.nx + 2; x0 += b->cw) bands.push_back(make_int2(i, x0));
-    }
+    b->max_nx = max_nx;
+    b->max_ny = max_ny;
     {
         void* wp = nullptr;
         if (waves.empty()) waves.push_back(make_float4(0, 0, 0, 0));
@@ -1676,10 +1728,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         *dst = static_cast<std::remove_reference_t<decltype(**dst)>*>(p);
         return CEL_OK;
     };
-    if (upload_list(tiles, &b->tiles, b->ntiles) || upload_list(mtiles, &b->mtiles, b->nmtiles) ||
-        upload_list(rows, &b->rows, b->nrows) ||
-        upload_list(bands, &b->bands, b->nbands))
-        return nullptr;
+    if (upload_list(tiles, &b->tiles, b->ntiles) || upload_list(rows, &b->rows, b->nrows)) return nullptr;
     for (int s = 0; s < 4; ++s)
         if (upload_list(bitems[s], &b->bitems[s], b->nbitems[s])) return nullptr;
     {
@@ -1697,23 +1746,17 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         b->rows_threads = 32 * warps;
         b->smem_rows = per_warp * warps;
     }
-    b->smem_cols = sizeof(float) * size_t(max_ny) * b->cw;
-    if (b->smem_cols + 8192 > 227 * 1024) { err = "domain too large for the fused solver"; return nullptr; }
     cudaFuncSetAttribute(k_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
     cudaFuncSetAttribute(k_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
-    cudaFuncSetAttribute(k_cols<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
-    cudaFuncSetAttribute(k_cols<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
-    cudaFuncSetAttribute(k_cols<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
-    cudaFuncSetAttribute(k_cols<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cols));
     {
         int occ = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_march<true>, MW, 0);
-        b->grid_stencil = std::max(1, std::min(b->nmtiles, b->sms * std::max(occ, 1)));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rows<true>, b->rows_threads, b->smem_rows);
         const int wpc = b->rows_threads / 32;
         b->grid_rows = std::max(1, std::min((b->nrows + wpc - 1) / wpc, b->sms * std::max(occ, 1)));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cols<false, 16>, NTC, b->smem_cols);
-        b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
+    }
+    {   // column bands of 16 columns (8 for tall domains: shared-memory capacity), strips of 64 rows
+        const int cw = (size_t(max_ny) * 16 * sizeof(float) + 8192 <= 227 * 1024) ? 16 : 8;
+        if (configure_work(b.get(), cw, MH_DEFAULT, err)) return nullptr;
     }
     b->sch.reset(*params[0]);
     cudaMemcpy(b->dt_table, b->dt_host, sizeof(float) * n, cudaMemcpyHostToDevice);
@@ -1904,8 +1947,50 @@ int batch_set_timestep(cel_batch* b, const float* dt, std::string& err) {
 }
 
 int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err) {
-    (void)err;
-    b->tile_x = tx; b->tile_y = ty; b->pcr_switch = pcr;
+    (void)pcr;   // the solves have no cyclic-reduction stage to hand over from (Thomas factors + scans)
+    return configure_work(b, tx > 0 ? tx : b->cw, ty > 0 ? ty : b->mh, err);
+}
+
+int batch_get_tuning(const cel_batch* b, int* tx, int* ty) {
+    if (tx) *tx = b->cw;
+    if (ty) *ty = b->mh;
+    return CEL_OK;
+}
+
+// Times `steps` physical steps for every candidate (band width, strip height), in the launch mode
+// the batch is set to (graph replay or direct), two rounds in turn, and keeps the fastest by its
+// better round.  The ensemble advances by every step taken here.
+int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, std::string& err) {
+    if (steps < 1) { err = "autotune needs at least one step per candidate"; return CEL_ERR_ARG; }
+    std::vector<int2> cand;
+    for (int cw : {8, 16, 32})
+        if (sizeof(float) * size_t(b->max_ny) * cw + 8192 <= 227 * 1024)
+            for (int mh : {32, 64, 128}) cand.push_back(make_int2(cw, mh));
+    std::vector<double> best(cand.size(), 1e300);
+    cudaEvent_t e0, e1;
+    B_TRY(cudaEventCreate(&e0));
+    B_TRY(cudaEventCreate(&e1));
+    int rc = CEL_OK;
+    for (int round = 0; round < 2 && !rc; ++round)
+        for (size_t k = 0; k < cand.size() && !rc; ++k) {
+            if ((rc = configure_work(b, cand[k].x, cand[k].y, err))) break;
+            if ((rc = batch_step(b, 2, err))) break;   // warm-up (captures the graphs in graph mode)
+            cudaEventRecord(e0, b->stream);
+            if ((rc = batch_step(b, steps, err))) break;
+            cudaEventRecord(e1, b->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            best[k] = std::min(best[k], double(ms) / steps);
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    const size_t kb = size_t(std::min_element(best.begin(), best.end()) - best.begin());
+    if ((rc = configure_work(b, cand[kb].x, cand[kb].y, err))) return rc;
+    if (tx) *tx = cand[kb].x;
+    if (ty) *ty = cand[kb].y;
+    if (best_ms) *best_ms = best[kb];
     return CEL_OK;
 }
 

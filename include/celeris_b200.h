@@ -193,9 +193,16 @@ int cel_batch_set_timestep(cel_batch* b, const float* dt);
 int cel_batch_launches_per_step(const cel_batch* b);
 
 /* ---- tuning and measurement ------------------------------------------------------------- */
-/* tile_x, tile_y: stencil tile; pcr_switch: system length at which PCR hands over to Thomas */
+/* Fused forms.  tile_x: column-solver band width (8, 16 or 32 columns per CTA); tile_y: stencil
+ * strip height (rows a CTA marches, 8..1024); 0 keeps the current value.  pcr_switch is accepted
+ * and ignored: the tridiagonal solves here factor each system once (Thomas) and run the sweeps as
+ * scans, with no cyclic-reduction stage to hand over from.  Plain engines ignore the call. */
 int cel_set_tuning(cel_engine* h, int tile_x, int tile_y, int pcr_switch);
 int cel_batch_set_tuning(cel_batch* b, int tile_x, int tile_y, int pcr_switch);
+int cel_batch_get_tuning(const cel_batch* b, int* tile_x, int* tile_y);
+/* Times `steps` physical steps for each candidate (band width x strip height) and keeps the
+ * fastest; writes the choice and its ms per step.  The members advance by every timed step. */
+int cel_batch_autotune(cel_batch* b, int steps, int* tile_x, int* tile_y, double* ms_per_step);
 /* Per-kernel CUDA-event timing on the launching stream (off by default). */
 int cel_batch_kernel_timing(cel_batch* b, int enable);
 int cel_engine_kernel_timing(cel_engine* h, int enable);

@@ -160,3 +160,26 @@ def test_batch_stats_describe_the_start_of_the_last_step(celeris):
         for k in ("kinetic_energy", "max_speed", "cfl_rate"):
             assert f[k] == pytest.approx(s[k], rel=1e-6, abs=1e-12), k
         assert f["total_time"] == pytest.approx(s["total_time"], rel=1e-12)
+
+
+def test_tuning_changes_decomposition_not_results(celeris):
+    """Band width and strip height only change how the work is split: the fields agree to FP32
+    rounding (the column scans group their additions differently)."""
+    members = [_case(k, nx=150 + 10 * i, ny=70 + 30 * i, N=1)[:4] for i, k in enumerate(["mixed", "sponge", "irregular"])]
+    ref = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    ref.step(30)
+    for bw, sh in [(32, 32), (8, 128), (16, 8)]:
+        b = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+        b.set_tuning(bw, sh)
+        assert b.tuning == (bw, sh)
+        b.step(30)
+        for i in range(len(members)):
+            errs = field_errors(b.state(i), ref.state(i))
+            assert rel_ok(errs, 1e-5, 1e-9), (bw, sh, errs)
+    t = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    got = t.autotune(2)
+    assert got["band_width"] in (8, 16, 32) and got["strip_height"] in (32, 64, 128) and got["ms_per_step"] > 0
+    assert t.tuning == (got["band_width"], got["strip_height"])
+    t.use_graph(True)
+    t.step(5)
+    assert np.isfinite(t.state(0)).all()
