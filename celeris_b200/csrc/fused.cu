@@ -1036,6 +1036,76 @@ __global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems
     }
 }
 
+// Column (y) solves, one thread per column: the thread runs the forward recurrence down its whole
+// column and the backward one up it.  A warp covers 32 adjacent columns, so every row access is a
+// coalesced 128-byte segment, and each thread issues the loads of CS rows before using them.  The
+// forward values overwrite the right-hand side in place (the same thread reads them back in the
+// backward sweep, mostly from L2), so the kernel needs no shared memory.
+constexpr int CS = 16;
+
+template <bool MIXED>
+__global__ void __launch_bounds__(128) k_cols_serial(const MemberDev* __restrict__ mems, const int2* __restrict__ cols,
+                                                     int ncols, PassArgs pa) {
+    const int it = blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= ncols) return;
+    const int2 cl = cols[it];
+    if (cl.y < 0) return;   // padding that keeps each warp on 32 aligned columns
+    const MemberDev& M = mems[cl.x];
+    const int n = M.c.ny, P = M.P, gx = cl.y;
+    float* __restrict__ rr = M.R[1] + gx;              // right-hand side, then the forward values
+    const float* __restrict__ cp = M.FYF[0] + gx;
+    const float* __restrict__ inv = M.FYF[1] + gx;
+    const float* __restrict__ mm = M.FYF[2] + gx;
+    auto at = [&](int i) { return size_t(i + 2) * P; };   // row offset of system element i
+    float y = 0.f;
+    for (int i = 0; i < n; i += CS) {
+        float mv[CS], iv[CS], rv[CS];
+#pragma unroll
+        for (int u = 0; u < CS; ++u) {
+            const bool ok = i + u < n;
+            mv[u] = ok ? __ldg(mm + at(i + u)) : 0.f;
+            iv[u] = ok ? __ldg(inv + at(i + u)) : 0.f;
+            rv[u] = ok ? rr[at(i + u)] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < CS; ++u)
+            if (i + u < n) {
+                y = iv[u] * rv[u] + mv[u] * y;
+                rr[at(i + u)] = y;
+            }
+    }
+    const int base = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
+    const float* __restrict__ bhi = M.S[base][2] + gx;
+    float* __restrict__ ohi = M.S[pa.out][2] + gx;
+    const float* __restrict__ blo = MIXED ? M.L[base][2] + gx : nullptr;
+    float* __restrict__ olo = MIXED ? M.L[pa.out][2] + gx : nullptr;
+    float x = 0.f;
+    for (int i = n - 1; i >= 0; i -= CS) {
+        float cv[CS], yv[CS], bh[CS], bl[CS];
+#pragma unroll
+        for (int u = 0; u < CS; ++u) {
+            const bool ok = i - u >= 0;
+            cv[u] = ok ? __ldg(cp + at(i - u)) : 0.f;
+            yv[u] = ok ? rr[at(i - u)] : 0.f;
+            bh[u] = ok ? bhi[at(i - u)] : 0.f;
+            bl[u] = (MIXED && ok) ? blo[at(i - u)] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < CS; ++u)
+            if (i - u >= 0) {
+                x = yv[u] - cv[u] * x;
+                if (MIXED) {
+                    float hi = bh[u], lo = bl[u];
+                    two_sum_add(hi, lo, x);
+                    ohi[at(i - u)] = hi;
+                    olo[at(i - u)] = lo;
+                } else {
+                    ohi[at(i - u)] = bh[u] + x;
+                }
+            }
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Boundary strips (compute.hlsl:985-1309), one side per launch over every member.
 // work item: {member, first strip cell}; 256 strip cells per item.
@@ -1355,8 +1425,13 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     B_TRY(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     {
         TimedLaunch t(&b->tm, b->side, "tridiag_cols");
-        auto* kc = cols_kernel(b->mixed, b->cw);
-        kc<<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+        if (b->cw == 1) {
+            if (b->mixed) k_cols_serial<true><<<b->grid_cols, 128, 0, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+            else k_cols_serial<false><<<b->grid_cols, 128, 0, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+        } else {
+            auto* kc = cols_kernel(b->mixed, b->cw);
+            kc<<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+        }
     }
     {
         TimedLaunch t(&b->tm, b->stream, "tridiag_rows");
@@ -1495,9 +1570,9 @@ void byte_model(int form, int N, double& stencil, double& step) {
 // (Re)builds the stencil strips (height mh) and the column bands (width cw) of a batch, sizes the
 // column solver's shared memory and grids, and drops captured graphs (they hold the old lists).
 int configure_work(cel_batch* b, int cw, int mh, std::string& err) {
-    if (cw != 8 && cw != 16 && cw != 32) { err = "column band width must be 8, 16 or 32"; return CEL_ERR_ARG; }
+    if (cw != 1 && cw != 8 && cw != 16 && cw != 32) { err = "column band width must be 1, 8, 16 or 32"; return CEL_ERR_ARG; }
     if (mh < 8 || mh > 1024) { err = "strip height must be in [8, 1024]"; return CEL_ERR_ARG; }
-    const size_t smem_cols = sizeof(float) * size_t(b->max_ny) * cw;
+    const size_t smem_cols = cw == 1 ? 0 : sizeof(float) * size_t(b->max_ny) * cw;
     if (smem_cols + 8192 > 227 * 1024) { err = "column band too wide for the tallest member (shared memory)"; return CEL_ERR_ARG; }
     std::vector<int4> mt;
     std::vector<int2> bd;
@@ -1505,8 +1580,15 @@ int configure_work(cel_batch* b, int cw, int mh, std::string& err) {
         const HostSetup& hs = b->mem[i].hs;
         for (int y0 = 2; y0 < hs.ny + 2; y0 += mh)
             for (int x0 = 2; x0 < hs.nx + 2; x0 += MO) mt.push_back(make_int4(i, x0, y0, mh));
-        // bands start on multiples of the band width so column loads are sector aligned
-        for (int x0 = 0; x0 < hs.nx + 2; x0 += cw) bd.push_back(make_int2(i, x0));
+        if (cw == 1) {
+            // one entry per column; columns 0, 1 and past nx+1 are padding (-1) so that each warp
+            // covers 32 columns starting on a 128-byte boundary
+            const int w = (hs.nx + 2 + 31) / 32 * 32;
+            for (int x = 0; x < w; ++x) bd.push_back(make_int2(i, (x >= 2 && x < hs.nx + 2) ? x : -1));
+        } else {
+            // bands start on multiples of the band width so column loads are sector aligned
+            for (int x0 = 0; x0 < hs.nx + 2; x0 += cw) bd.push_back(make_int2(i, x0));
+        }
     }
     free_graphs(b);
     B_TRY(cudaStreamSynchronize(b->stream));
@@ -1527,11 +1609,15 @@ int configure_work(cel_batch* b, int cw, int mh, std::string& err) {
     b->cw = cw;
     b->mh = mh;
     b->smem_cols = smem_cols;
-    ColsKernel kc = cols_kernel(b->mixed, cw);
-    B_TRY(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_cols)));
     int occ = 1;
-    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc, NTC, smem_cols));
-    b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
+    if (cw == 1) {
+        b->grid_cols = (b->nbands + 127) / 128;
+    } else {
+        ColsKernel kc = cols_kernel(b->mixed, cw);
+        B_TRY(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_cols)));
+        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc, NTC, smem_cols));
+        b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
+    }
     B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->mixed ? k_march<true> : k_march<false>, MW, 0));
     b->grid_stencil = std::max(1, std::min(b->nmtiles, b->sms * std::max(occ, 1)));
     return CEL_OK;
@@ -1963,8 +2049,8 @@ int batch_get_tuning(const cel_batch* b, int* tx, int* ty) {
 int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, std::string& err) {
     if (steps < 1) { err = "autotune needs at least one step per candidate"; return CEL_ERR_ARG; }
     std::vector<int2> cand;
-    for (int cw : {8, 16, 32})
-        if (sizeof(float) * size_t(b->max_ny) * cw + 8192 <= 227 * 1024)
+    for (int cw : {1, 8, 16, 32})
+        if (cw == 1 || sizeof(float) * size_t(b->max_ny) * cw + 8192 <= 227 * 1024)
             for (int mh : {32, 64, 128}) cand.push_back(make_int2(cw, mh));
     std::vector<double> best(cand.size(), 1e300);
     cudaEvent_t e0, e1;

@@ -193,7 +193,8 @@ int cel_batch_set_timestep(cel_batch* b, const float* dt);
 int cel_batch_launches_per_step(const cel_batch* b);
 
 /* ---- tuning and measurement ------------------------------------------------------------- */
-/* Fused forms.  tile_x: column-solver band width (8, 16 or 32 columns per CTA); tile_y: stencil
+/* Fused forms.  tile_x: column-solver band width (8, 16 or 32 columns per CTA, chunked scans; or 1:
+ * one thread per column, serial sweeps, forward values kept in the right-hand-side plane); tile_y: stencil
  * strip height (rows a CTA marches, 8..1024); 0 keeps the current value.  pcr_switch is accepted
  * and ignored: the tridiagonal solves here factor each system once (Thomas) and run the sweeps as
  * scans, with no cyclic-reduction stage to hand over from.  Plain engines ignore the call. */

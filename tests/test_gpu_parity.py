@@ -168,7 +168,7 @@ def test_tuning_changes_decomposition_not_results(celeris):
     members = [_case(k, nx=150 + 10 * i, ny=70 + 30 * i, N=1)[:4] for i, k in enumerate(["mixed", "sponge", "irregular"])]
     ref = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
     ref.step(30)
-    for bw, sh in [(32, 32), (8, 128), (16, 8)]:
+    for bw, sh in [(32, 32), (8, 128), (16, 8), (1, 64)]:
         b = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
         b.set_tuning(bw, sh)
         assert b.tuning == (bw, sh)
@@ -178,7 +178,7 @@ def test_tuning_changes_decomposition_not_results(celeris):
             assert rel_ok(errs, 1e-5, 1e-9), (bw, sh, errs)
     t = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
     got = t.autotune(2)
-    assert got["band_width"] in (8, 16, 32) and got["strip_height"] in (32, 64, 128) and got["ms_per_step"] > 0
+    assert got["band_width"] in (1, 8, 16, 32) and got["strip_height"] in (32, 64, 128) and got["ms_per_step"] > 0
     assert t.tuning == (got["band_width"], got["strip_height"])
     t.use_graph(True)
     t.step(5)
