@@ -252,7 +252,7 @@ struct Kahan {
 // Ring layout: field f, slot s, column k at ring[f * FSTR + s * RSTR + k]; a "row base" is
 // s * RSTR + (this thread's column), so every access is base + compile-time offset.
 constexpr int FSTR = RING * RSTR;
-constexpr int DSTR = RBOX;   // still-water depth ring: one row of RBOX columns per slot
+constexpr int DSTR = RSTR;   // still-water depth ring: the ring's row stride, so one offset serves both
 
 __device__ __forceinline__ void reconstruct_fast(float tt, float w, float c, float e, float& ow, float& oe) {
     const float z1 = tt * (c - w), z2 = e - w, z3 = tt * (e - c);
@@ -404,9 +404,9 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
         // still-water depth of a ring row: thread k covers ring column rc0(thread 0) - 1 + k, and
         // threads 0 and 1 also the two columns past the last thread (every column Pass3 reads)
         const int dcol = rc0 - 1;
-        auto depth_row = [&](int slot) {
-            const float* ba = BAr + slot * RSTR;
-            float* dr = dring + slot * DSTR;
+        auto depth_row = [&](int off) {   // off = slot * RSTR
+            const float* ba = BAr + off;
+            float* dr = dring + off;
             dr[dcol] = fmaxf(0.f, sl - ba[dcol]);
             const int d2c = min(dcol + MW, RBOX - 1);
             if (tid < 2) dr[d2c] = fmaxf(0.f, sl - ba[d2c]);
@@ -434,19 +434,23 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
             const unsigned pA = (seq0 / RING) & 1u, pB = ((seq0 + 1) / RING) & 1u;
             if (!mbar_wait_bounded(&bars[sA], pA, tma_late ? 1 : (1 << 22))) tma_late = true;
             if (!mbar_wait_bounded(&bars[sB], pB, tma_late ? 1 : (1 << 22))) tma_late = true;
-            depth_row(sA);
-            depth_row(sB);
+            depth_row(sA * RSTR);
+            depth_row(sB * RSTR);
         }
-        int s2m = sA, s1m = sA, s0 = sA, s1p = sB, s2p = sC;
+        int s2p = sC;                                          // slot of row t+2 (mbarrier index)
+        // ring-row offsets (slot * RSTR) of rows t-2 .. t+2, rotated as the window moves
+        int o2m = sA * RSTR, o1m = sA * RSTR, o0 = sA * RSTR, o1p = sB * RSTR, o2p = sC * RSTR;
         unsigned par2p = ((seq0 + 2) / RING) & 1u;            // phase parity of row t+2
         int sReq = int((seq0 + unsigned(PREFETCH) + 2) % RING);  // slot of row t+PREFETCH+2
+        size_t erow = size_t(y0 - 2) * P;                     // first cell of row t
+        const int xl = min(xc, c.NX - 1);
 
         for (int t = y0 - 2; t < yend; ++t) {
             const bool p3 = t >= y0;                   // Pass3 runs on this row (uniform)
-            const size_t e = size_t(t) * P + xc;       // this thread's cell of row t
+            const size_t e = erow + size_t(xc);        // this thread's cell of row t
             // loads use a column inside the row (the halo thread past the last column reads a
             // neighbour it never stores to)
-            const size_t el = size_t(t) * P + min(xc, c.NX - 1);
+            const size_t el = erow + size_t(xl);
             // per-cell inputs of Pass3 at (xc, t), requested before the face work
             float4 ho = make_float4(0.f, 0.f, 0.f, 0.f), hoo = ho, hp = ho;
             float go = 0.f, goo = 0.f, gp = 0.f, wcur = 0.f, wlo = 0.f;
@@ -474,8 +478,8 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
             }
             sReq = next_slot(sReq);
             if (!mbar_wait_bounded(&bars[s2p], par2p, tma_late ? 1 : (1 << 22))) tma_late = true;
-            depth_row(s2p);
-            const int bm = s0 * RSTR + rc0, b0 = s1p * RSTR + rc0, bp = s2p * RSTR + rc0;  // rows t, t+1, t+2
+            depth_row(o2p);
+            const int bm = o0 + rc0, b0 = o1p + rc0, bp = o2p + rc0;  // rows t, t+1, t+2
             // ---- faces of row t+1 (Pass1), aux of that row, y flux between rows t and t+1 ----
             Face f;
             faces_at(ring, bm, b0, bp, c, f);
@@ -500,17 +504,17 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
             __syncthreads();  // (B)
             // ---- Pass3 at (xc, t) ----
             if (p3) {
-                const int c0 = s0 * RSTR + rc, cm = s1m * RSTR + rc, cpp1 = s1p * RSTR + rc;
-                const int cmm = s2m * RSTR + rc, cpp2 = s2p * RSTR + rc;   // rows t, t-1, t+1, t-2, t+2
-                const int d0 = s0 * DSTR + rc;
+                const int c0 = o0 + rc, cm = o1m + rc, cpp1 = o1p + rc;
+                const int cmm = o2m + rc, cpp2 = o2p + rc;   // rows t, t-1, t+1, t-2, t+2
+                const int d0 = c0;
                 const float wc = W[c0], huc = HU[c0], hvc = HV[c0];
                 const float BAh = BAr[c0], BXh = BXr[c0], BYh = BYr[c0];
                 const float BXw = BXr[c0 - 1], BYs = BYr[cm];
                 const float h = fmaxf(0.f, wc - BAh);
                 const float dh = dring[d0], d2 = dh * dh, d3 = d2 * dh;
                 const float dl = dring[d0 - 1], dr = dring[d0 + 1], dll = dring[d0 - 2], drr = dring[d0 + 2];
-                const float ddn = dring[s1m * DSTR + rc], du = dring[s1p * DSTR + rc];
-                const float ddd = dring[s2m * DSTR + rc], duu = dring[s2p * DSTR + rc];
+                const float ddn = dring[cm], du = dring[cpp1];
+                const float ddd = dring[cmm], duu = dring[cpp2];
                 // eta = w - sea level enters only through differences, where the sea level cancels
                 const float e0 = wc, el_ = W[c0 - 1], er = W[c0 + 1], ed = W[cm], eu_ = W[cpp1];
                 const float ell = W[c0 - 2], err = W[c0 + 2], edd = W[cmm], euu = W[cpp2];
@@ -591,9 +595,11 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
             nh = f.hN; nu = f.uN; nv = f.vN;
             eh = f.hE; eu = f.uE; ev = f.vE;
             // advance the ring window: rows t-1 .. t+3 become t-2 .. t+2
-            s2m = s1m; s1m = s0; s0 = s1p; s1p = s2p;
+            o2m = o1m; o1m = o0; o0 = o1p; o1p = o2p;
+            o2p = (o2p + RSTR == RING * RSTR) ? 0 : o2p + RSTR;
             s2p = next_slot(s2p);
             if (s2p == 0) par2p ^= 1u;
+            erow += size_t(P);
         }
         seq = seq0 + unsigned(last_row - (y0 - 2) + 1);
         // ---- zero the ghost ring of the output state next to this strip (engine.cpp:1007) ----
