@@ -302,6 +302,7 @@ def main():
                            cells * 4 * (42 + (9 if args.form == "mixed" else 0)) / 1e9),
                        "parallelism": f"ensemble sharded by domain over {world} GPU(s)",
                        "tuning": {"column_band_width": batch.tuning[0], "strip_height": batch.tuning[1],
+                                  "stencil_rows_per_step": batch.stencil_rows,
                                   "autotuned": tuned is not None,
                                   "pcr_switch": "none (Thomas factors + scans; no cyclic-reduction stage)"}},
             "e2e": {"value": e2e_value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": h2d,

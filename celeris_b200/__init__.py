@@ -222,9 +222,20 @@ class Batch:
 
     @property
     def tuning(self) -> tuple:
-        tx, ty = C.c_int(), C.c_int()
-        check(lib().cel_batch_get_tuning(self.h, C.byref(tx), C.byref(ty)))
+        """(column band width, strip height)."""
+        tx, ty, rp = C.c_int(), C.c_int(), C.c_int()
+        check(lib().cel_batch_get_tuning(self.h, C.byref(tx), C.byref(ty), C.byref(rp)))
         return tx.value, ty.value
+
+    @property
+    def stencil_rows(self) -> int:
+        tx, ty, rp = C.c_int(), C.c_int(), C.c_int()
+        check(lib().cel_batch_get_tuning(self.h, C.byref(tx), C.byref(ty), C.byref(rp)))
+        return rp.value
+
+    def set_stencil_rows(self, rows_per_step: int):
+        """1: one row per stencil step; 2: two rows as paired f32x2 arithmetic."""
+        check(lib().cel_batch_set_stencil_rows(self.h, rows_per_step))
 
     def autotune(self, steps: int = 5) -> dict:
         """Times each candidate for `steps` steps and keeps the fastest (the members advance)."""

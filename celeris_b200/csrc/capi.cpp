@@ -339,9 +339,13 @@ int cel_batch_set_tuning(cel_batch* b, int tx, int ty, int pcr) {
     BAT(b);
     CEL_GUARD_BEGIN BRET(cel::batch_set_tuning(b, tx, ty, pcr, err)); CEL_GUARD_END
 }
-int cel_batch_get_tuning(const cel_batch* b, int* tx, int* ty) {
+int cel_batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rows_per_step) {
     if (!b) { set_error("null batch"); return CEL_ERR_ARG; }
-    return cel::batch_get_tuning(b, tx, ty);
+    return cel::batch_get_tuning(b, tx, ty, rows_per_step);
+}
+int cel_batch_set_stencil_rows(cel_batch* b, int rows_per_step) {
+    BAT(b);
+    CEL_GUARD_BEGIN BRET(cel::batch_set_stencil_rows(b, rows_per_step, err)); CEL_GUARD_END
 }
 int cel_batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* ms) {
     BAT(b);

@@ -150,6 +150,10 @@ __device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h,
 #define CEL_MARCH_MIN_CTAS 5
 #endif
 constexpr int MARCH_MIN_CTAS = CEL_MARCH_MIN_CTAS;
+#ifndef CEL_MARCH2_MIN_CTAS
+#define CEL_MARCH2_MIN_CTAS 3
+#endif
+constexpr int MARCH2_MIN_CTAS = CEL_MARCH2_MIN_CTAS;   // the paired-row stencil (49.6 KB smem, 166 registers)
 constexpr int MW = 128;          // threads = columns with faces per row
 constexpr int MO = MW - 2;       // output columns per strip
 constexpr int MH_DEFAULT = 64;   // rows per strip unless tuned (each work item carries its height)
@@ -649,6 +653,548 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
     }
     // a bounded TMA wait that gave up anywhere in this CTA marks the whole pass (the host reports
     // it as a CUDA error of the batch)
+    if (__syncthreads_or(tma_late) && tid == 0) atomic_max_nonneg(pa.late_flag, 1.0);
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_march2: the passes of k_march on two rows per step.  Every per-cell quantity is a pair
+// (row t, row t+1) held in a float2, and arithmetic on pairs uses the paired single-precision
+// instructions of sm_100 (__fadd2_rn, __fmul2_rn, __ffma2_rn): one instruction does the work of
+// two cells.  The per-step bookkeeping (barriers, TMA requests, ring rotation, addressing) is paid
+// once per two rows.  The faces run one step ahead of Pass3: step j computes the faces of rows
+// t+2 and t+3 and uses those of rows t and t+1 from step j-1.  Ring: RING2 = 9 rows, the window
+// t-2 .. t+4 plus the two rows requested one step ahead.
+// ---------------------------------------------------------------------------------------------
+constexpr int RING2 = 9;
+constexpr int FSTR2 = RING2 * RSTR;
+constexpr size_t MARCH2_DYN_SMEM = sizeof(float) * 6 * FSTR2;   // the 9-row TMA ring
+
+typedef float2 f2;
+__device__ __forceinline__ f2 P2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ f2 S2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 max2(f2 a, f2 b) { return P2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+__device__ __forceinline__ f2 min2(f2 a, f2 b) { return P2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+
+__device__ __forceinline__ void recon2(f2 tt, f2 w, f2 c, f2 e, f2& ow, f2& oe) {
+    const f2 z1 = mul2(tt, sub2(c, w)), z2 = sub2(e, w), z3 = mul2(tt, sub2(e, c));
+    const f2 g2 = mul2(S2(0.25f), P2(minmod3_fast(z1.x, z2.x, z3.x), minmod3_fast(z1.y, z2.y, z3.y)));
+    oe = add2(c, g2);
+    ow = sub2(c, g2);
+}
+__device__ __forceinline__ void recon_sd2(f2 tt, f2 w, f2 c, f2 e, f2& ow, f2& oe, f2& sd) {
+    const f2 z1 = mul2(tt, sub2(c, w)), z2 = sub2(e, w), z3 = mul2(tt, sub2(e, c));
+    const f2 g2 = mul2(S2(0.25f), P2(minmod3_fast(z1.x, z2.x, z3.x), minmod3_fast(z1.y, z2.y, z3.y)));
+    const f2 mu = mul2(S2(0.5f / 3.0f), add2(add2(z1, z2), z3));
+    const f2 d1 = sub2(z1, mu), d2 = sub2(z2, mu), d3 = sub2(z3, mu);
+    const f2 v = mul2(fma2(d1, d1, fma2(d2, d2, mul2(d3, d3))), S2(1.0f / 3.0f));
+    sd = P2(sqrtf(v.x), sqrtf(v.y));
+    oe = add2(c, g2);
+    ow = sub2(c, g2);
+}
+__device__ __forceinline__ void correct_w2(f2 Bw, f2 Be, f2 wbar, f2& ww, f2& we) {
+    float a = ww.x, b = we.x, c = ww.y, d = we.y;
+    correct_w_fast(Bw.x, Be.x, wbar.x, a, b);
+    correct_w_fast(Bw.y, Be.y, wbar.y, c, d);
+    ww = P2(a, c);
+    we = P2(b, d);
+}
+__device__ __forceinline__ f2 div_by_h2(f2 h, float eps) {
+    const f2 h2 = mul2(h, h), h4 = mul2(h2, h2);
+    const f2 t = add2(h4, max2(h4, S2(eps)));
+    return mul2(mul2(S2(1.41421354f), h), P2(rsqrtf(t.x), rsqrtf(t.y)));
+}
+
+struct Face2 { f2 hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, msd; };
+// what the next step needs of a pair's faces: north and east faces of both rows, south face of
+// the second row
+struct Carry2 {
+    f2 hN, uN, vN, hE, uE, vE;
+    float hS1, uS1, vS1;
+    __device__ __forceinline__ void set(const Face2& f) {
+        hN = f.hN; uN = f.uN; vN = f.vN; hE = f.hE; uE = f.uE; vE = f.vE;
+        hS1 = f.hS.y; uS1 = f.uS.y; vS1 = f.vS.y;
+    }
+};
+
+// Pass1 on rows r and r+1 of one column: ring-row offsets of rows r-1, r, r+1, r+2 and the column.
+__device__ __forceinline__ void faces_at2(const float* __restrict__ ring, int om1, int o0, int o1, int o2, int col,
+                                          const SimConsts& c, Face2& f) {
+    const float* W = ring;
+    const float* HU = ring + FSTR2;
+    const float* HV = ring + 2 * FSTR2;
+    const float* BXr = ring + 4 * FSTR2;
+    const float* BYr = ring + 5 * FSTR2;
+    const int a0 = o0 + col, a1 = o1 + col;
+    const f2 tt = S2(c.two_theta);
+    const f2 wc = P2(W[a0], W[a1]), wl = P2(W[a0 - 1], W[a1 - 1]), wr = P2(W[a0 + 1], W[a1 + 1]);
+    const f2 wd = P2(W[om1 + col], W[a0]), wu = P2(W[a1], W[o2 + col]);
+    const f2 BN = P2(BYr[a0], BYr[a1]), BE = P2(BXr[a0], BXr[a1]);
+    const f2 BS = P2(BYr[om1 + col], BYr[a0]), BW = P2(BXr[a0 - 1], BXr[a1 - 1]);
+    f2 wN, wE, wS, wW, huN, huE, huS, huW, hvN, hvE, hvS, hvW, sd1, sd2;
+    recon_sd2(tt, wl, wc, wr, wW, wE, sd1);
+    recon_sd2(tt, wd, wc, wu, wS, wN, sd2);
+    const f2 huc = P2(HU[a0], HU[a1]), hvc = P2(HV[a0], HV[a1]);
+    recon2(tt, P2(HU[a0 - 1], HU[a1 - 1]), huc, P2(HU[a0 + 1], HU[a1 + 1]), huW, huE);
+    recon2(tt, P2(HU[om1 + col], HU[a0]), huc, P2(HU[a1], HU[o2 + col]), huS, huN);
+    recon2(tt, P2(HV[a0 - 1], HV[a1 - 1]), hvc, P2(HV[a0 + 1], HV[a1 + 1]), hvW, hvE);
+    recon2(tt, P2(HV[om1 + col], HV[a0]), hvc, P2(HV[a1], HV[o2 + col]), hvS, hvN);
+    correct_w2(BW, BE, wc, wW, wE);
+    correct_w2(BS, BN, wc, wS, wN);
+    f.hN = sub2(wN, BN); f.hE = sub2(wE, BE); f.hS = sub2(wS, BS); f.hW = sub2(wW, BW);
+    f2 q;
+    q = div_by_h2(f.hN, c.epsilon); f.uN = mul2(q, huN); f.vN = mul2(q, hvN);
+    q = div_by_h2(f.hE, c.epsilon); f.uE = mul2(q, huE); f.vE = mul2(q, hvE);
+    q = div_by_h2(f.hS, c.epsilon); f.uS = mul2(q, huS); f.vS = mul2(q, hvS);
+    q = div_by_h2(f.hW, c.epsilon); f.uW = mul2(q, huW); f.vW = mul2(q, hvW);
+    f.msd = max2(mul2(sd1, S2(c.one_over_dx)), mul2(sd2, S2(c.one_over_dy)));
+}
+
+// KP07 fluxes through a pair of faces (m: lower-index side, p: the other); xdir selects the normal.
+__device__ __forceinline__ void face_flux2(f2 hm, f2 um, f2 vm, f2 hp, f2 up, f2 vp, float g, float hg, bool xdir,
+                                           f2 out[3]) {
+    const f2 cm = P2(sqrtf(g * hm.x), sqrtf(g * hm.y)), cpp = P2(sqrtf(g * hp.x), sqrtf(g * hp.y));
+    const f2 nm = xdir ? um : vm, np = xdir ? up : vp;
+    const f2 ap = max2(max2(add2(nm, cm), add2(np, cpp)), S2(0.f));
+    const f2 am = min2(min2(sub2(nm, cm), sub2(np, cpp)), S2(0.f));
+    const f2 qp = mul2(hp, np), qm = mul2(hm, nm);
+    const f2 hgv = S2(hg);
+    f2 Fp[3], Fm[3], dU[3];
+    Fp[0] = qp; Fm[0] = qm; dU[0] = sub2(hp, hm);
+    if (xdir) {
+        Fp[1] = mul2(hp, fma2(hgv, hp, mul2(up, up))); Fm[1] = mul2(hm, fma2(hgv, hm, mul2(um, um)));
+        dU[1] = sub2(mul2(hp, up), mul2(hm, um));
+        Fp[2] = mul2(qp, vp); Fm[2] = mul2(qm, vm); dU[2] = sub2(mul2(hp, vp), mul2(hm, vm));
+    } else {
+        Fp[1] = mul2(qp, up); Fm[1] = mul2(qm, um); dU[1] = sub2(mul2(hp, up), mul2(hm, um));
+        Fp[2] = mul2(hp, fma2(hgv, hp, mul2(vp, vp))); Fm[2] = mul2(hm, fma2(hgv, hm, mul2(vm, vm)));
+        dU[2] = sub2(mul2(hp, vp), mul2(hm, vm));
+    }
+    const f2 den = sub2(ap, am);
+    const f2 inv = P2(den.x != 0.f ? __fdividef(1.0f, den.x) : 0.f, den.y != 0.f ? __fdividef(1.0f, den.y) : 0.f);
+    const f2 apam = mul2(ap, am);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = mul2(fma2(apam, dU[k], sub2(mul2(ap, Fm[k]), mul2(am, Fp[k]))), inv);
+}
+
+// Kahan accumulation of a pair of rows
+struct Kahan2 {
+    f2 s = make_float2(0.f, 0.f), c = make_float2(0.f, 0.f);
+    __device__ __forceinline__ void add(f2 x) {
+        const f2 y = sub2(x, c);
+        const f2 t = add2(s, y);
+        c = sub2(sub2(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double(s.x) - double(c.x)) + (double(s.y) - double(c.y)); }
+};
+
+template <bool MIXED>
+__global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev* __restrict__ mems,
+                                                               const int4* __restrict__ tiles, int ntiles, PassArgs pa) {
+    extern __shared__ __align__(128) float ring[];   // 6 * FSTR2 floats (dynamic: the total passes 48 KB)
+    __shared__ float dring[RING2 * RSTR];   // still-water depth of each ring row (same stride as the ring)
+    __shared__ __align__(8) unsigned long long bars[RING2];
+    __shared__ float fW[2][2][3][MW];       // [step parity][row of the pair][hW, uW, vW][thread]
+    __shared__ float xb[2][3][MW];          // [row of the pair][component][thread]
+    constexpr int OFF = MIXED ? 18 : 9;
+    constexpr int iR0 = OFF + 3, iH0 = OFF + 5, iAUX = OFF + 25;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int k = 0; k < RING2; ++k) mbar_init(&bars[k], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    unsigned seq = 0;          // rows requested by this CTA so far (the same value in every thread)
+    bool tma_late = false;
+    const float* W = ring;
+    const float* HU = ring + FSTR2;
+    const float* HV = ring + 2 * FSTR2;
+    const float* BAr = ring + 3 * FSTR2;
+    const float* BXr = ring + 4 * FSTR2;
+    const float* BYr = ring + 5 * FSTR2;
+    const bool stats = pa.stats != 0;
+    const bool corr = pa.scheme == CEL_SCHEME_CORRECTOR;
+    const bool euler = pa.scheme == CEL_SCHEME_EULER;
+
+    for (int it = blockIdx.x; it < ntiles; it += gridDim.x) {
+        const int4 tl = tiles[it];
+        const MemberDev& M = mems[tl.x];
+        const SimConsts c = M.c;
+        const int P = M.P, nx = c.nx, ny = c.ny, NYm1 = c.NY - 1;
+        float* __restrict__ B = M.base;
+        const size_t PL = M.plane;
+        const CUtensorMap* tm = M.tmaps;
+        const int x0 = tl.y, y0 = tl.z, MH = tl.w;
+        const int xs = (x0 - 2) & ~3;          // TMA box start, 16-byte aligned
+        const int xc = x0 - 1 + tid;           // this thread's column
+        const int rc0 = xc - xs;               // its ring column (1 .. 131)
+        const int rc = max(rc0, 2);            // Pass3 column (clamped for the halo thread 0)
+        const int yend = min(y0 + MH, ny + 2);
+        const int nsteps = (yend - y0 + 1) / 2;             // output row pairs of this strip
+        const int last_row = y0 + 2 * (nsteps - 1) + 4;     // last row any step reads
+        const bool out_col = tid >= 1 && tid <= MO && xc < nx + 2;
+        const int xl = min(xc, c.NX - 1);
+        const float dtm = *M.dtp;
+        const float decay = t_pow(fabsf(c.whitewater_decay_rate), dtm);
+        const float sl = c.sea_level;
+        const float4* __restrict__ HAo = reinterpret_cast<const float4*>(B + (iH0 + 5 * pa.og) * PL);
+        const float4* __restrict__ HAoo = reinterpret_cast<const float4*>(B + (iH0 + 5 * pa.oog) * PL);
+        const float4* __restrict__ HAp = reinterpret_cast<const float4*>(B + (iH0 + 5 * pa.pred) * PL);
+        float4* __restrict__ HAs = reinterpret_cast<float4*>(B + (iH0 + 5 * pa.scr) * PL);
+        const float* __restrict__ HBo = B + (iH0 + 5 * pa.og + 4) * PL;
+        const float* __restrict__ HBoo = B + (iH0 + 5 * pa.oog + 4) * PL;
+        const float* __restrict__ HBp = B + (iH0 + 5 * pa.pred + 4) * PL;
+        float* __restrict__ HBs = B + (iH0 + 5 * pa.scr + 4) * PL;
+        float* __restrict__ Wout = B + (3 * pa.out) * PL;
+        const float* __restrict__ Wcur = B + (3 * pa.cur) * PL;
+        float* __restrict__ R0 = B + iR0 * PL;
+        float2* __restrict__ AUX = reinterpret_cast<float2*>(B + iAUX * PL);
+        const float* __restrict__ Lbase = B + (9 + 3 * (corr ? pa.cur : pa.in)) * PL;
+        float* __restrict__ Lout = B + (9 + 3 * pa.out) * PL;
+
+        // row r of the strip has sequence number seq0 + (r - (y0 - 2)): slot seq % RING2, mbarrier
+        // phase parity (seq / RING2) & 1
+        const unsigned seq0 = seq;
+        auto slot_of = [&](int r) { return int((seq0 + unsigned(r - (y0 - 2))) % RING2); };
+        auto par_of = [&](int r) { return ((seq0 + unsigned(r - (y0 - 2))) / RING2) & 1u; };
+        auto issue = [&](int row) {   // one thread: request the 6 fields of a row into its slot
+            const int sl_ = slot_of(row);
+            const int ry = min(row, NYm1);          // rows past the domain are never used; load the last
+            mbar_expect_tx(&bars[sl_], ROW_BYTES);
+            float* dst = ring + sl_ * RSTR;
+            tma_row(dst, tm + pa.in * 3 + 0, xs, ry, &bars[sl_]);
+            tma_row(dst + FSTR2, tm + pa.in * 3 + 1, xs, ry, &bars[sl_]);
+            tma_row(dst + 2 * FSTR2, tm + pa.in * 3 + 2, xs, ry, &bars[sl_]);
+            tma_row(dst + 3 * FSTR2, tm + 9, xs, ry, &bars[sl_]);
+            tma_row(dst + 4 * FSTR2, tm + 10, xs, ry, &bars[sl_]);
+            tma_row(dst + 5 * FSTR2, tm + 11, xs, ry, &bars[sl_]);
+        };
+        auto wait_row = [&](int row) {
+            if (!mbar_wait_bounded(&bars[slot_of(row)], par_of(row), tma_late ? 1 : (1 << 22))) tma_late = true;
+        };
+        // still-water depth of a ring row: thread k covers ring column rc0(thread 0) - 1 + k, and
+        // threads 0 and 1 also the two columns past the last thread
+        const int dcol = rc0 - 1;
+        auto depth_row = [&](int row) {
+            const int off = slot_of(row) * RSTR;
+            const float* ba = BAr + off;
+            float* dr = dring + off;
+            dr[dcol] = fmaxf(0.f, sl - ba[dcol]);
+            const int d2c = min(dcol + MW, RBOX - 1);
+            if (tid < 2) dr[d2c] = fmaxf(0.f, sl - ba[d2c]);
+        };
+
+        Kahan2 acc[6];
+        f2 mx[4] = {S2(0.f), S2(0.f), S2(0.f), S2(0.f)};
+        bool bad = false;
+
+        __syncthreads();  // the previous strip is done with shared memory
+        if (tid == 0) {
+            fence_proxy_async();
+            for (int r = y0 - 2; r <= min(y0 + 2, last_row); ++r) issue(r);   // rows of the prologue and step -1
+        }
+        // prologue: faces of rows y0-2 and y0-1 (row y0-3's slot holds stale data: only row y0-2's
+        // faces read it, and those are never used)
+        wait_row(y0 - 2); wait_row(y0 - 1); wait_row(y0);
+        depth_row(y0 - 2); depth_row(y0 - 1); depth_row(y0);
+        Carry2 fp;   // faces of the previous step's rows (t, t+1 of the coming step)
+        float ypv[3] = {0.f, 0.f, 0.f};   // y flux through the south face of row t (per component)
+        {
+        Face2 fq;
+        faces_at2(ring, slot_of(y0 - 3) * RSTR, slot_of(y0 - 2) * RSTR, slot_of(y0 - 1) * RSTR, slot_of(y0) * RSTR,
+                  rc0, c, fq);
+        {
+            const int pp = 1;   // parity of step -1
+            fW[pp][0][0][tid] = fq.hW.x; fW[pp][0][1][tid] = fq.uW.x; fW[pp][0][2][tid] = fq.vW.x;
+            fW[pp][1][0][tid] = fq.hW.y; fW[pp][1][1][tid] = fq.uW.y; fW[pp][1][2][tid] = fq.vW.y;
+        }
+        {   // aux of row y0-1 (the ghost row y = 1 belongs to the first strip)
+            const int gy = y0 - 1;
+            const int cxa = xc < 2 ? 2 : xc, cya = gy < 2 ? 2 : gy;
+            if (xc >= 1 && xc < nx + 2 && gy >= 1 && cxa >= x0 && cxa < x0 + MO && cya >= y0 && cya < y0 + MH) {
+                float2* a = AUX + (size_t(gy) * P + xc);
+                const float2 old = *a;
+                const float md = (((fq.hN.y + fq.hE.y) + (fq.hS.y + fq.hW.y)) * 0.25f);
+                const float bw = (fq.msd.y > M.tan_thr) ? 1.0f : old.y;
+                *a = make_float2(fmaxf(md, old.x), bw * decay);
+            }
+        }
+        fp.set(fq);
+        }
+
+        for (int j = -1; j < nsteps; ++j) {
+            const int t = y0 + 2 * j;
+            const bool p3 = j >= 0;
+            const bool row1 = t + 1 < yend;                  // the second row of the pair exists
+            const size_t e0 = size_t(t) * P + xc, e1 = e0 + P;
+            const size_t l0 = size_t(t) * P + xl, l1 = l0 + P;
+            // Pass3 inputs of rows t and t+1
+            float4 ho0 = make_float4(0.f, 0.f, 0.f, 0.f), ho1 = ho0, hoo0 = ho0, hoo1 = ho0, hp0 = ho0, hp1 = ho0;
+            f2 go = S2(0.f), goo = go, gp = go, wcur = go, wlo = go;
+            if (p3) {
+                if (!euler) {
+                    ho0 = __ldg(HAo + l0); ho1 = __ldg(HAo + l1);
+                    hoo0 = __ldg(HAoo + l0); hoo1 = __ldg(HAoo + l1);
+                    go = P2(__ldg(HBo + l0), __ldg(HBo + l1));
+                    goo = P2(__ldg(HBoo + l0), __ldg(HBoo + l1));
+                    if (corr) {
+                        hp0 = __ldg(HAp + l0); hp1 = __ldg(HAp + l1);
+                        gp = P2(__ldg(HBp + l0), __ldg(HBp + l1));
+                        wcur = P2(__ldg(Wcur + l0), __ldg(Wcur + l1));
+                    }
+                }
+                if (MIXED) wlo = P2(__ldg(Lbase + l0), __ldg(Lbase + l1));
+            }
+            // aux texels of rows t+2 and t+3 owned by this strip, read-modify-written after their faces
+            bool aux_ok[2];
+            float2* ap[2];
+            float2 aux_old[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int gy = t + 2 + k;
+                const int cxa = xc < 2 ? 2 : xc, cya = gy < 2 ? 2 : gy;
+                aux_ok[k] = xc >= 1 && xc < nx + 2 && gy >= 1 && gy < ny + 2 && cxa >= x0 && cxa < x0 + MO &&
+                            cya >= y0 && cya < y0 + MH;
+                ap[k] = AUX + (size_t(min(gy, NYm1)) * P + xc);
+                aux_old[k] = aux_ok[k] ? *ap[k] : make_float2(0.f, 0.f);
+            }
+            __syncthreads();  // (A) the previous step is complete: ring slots of rows t-4, t-3 are free
+            if (tid == 0) {
+                fence_proxy_async();
+                if (t + 5 <= last_row) issue(t + 5);
+                if (t + 6 <= last_row) issue(t + 6);
+            }
+            wait_row(t + 3);
+            wait_row(t + 4);
+            depth_row(t + 3);
+            depth_row(t + 4);
+            const int om2 = slot_of(t - 2) * RSTR, om1 = slot_of(t - 1) * RSTR, o0 = slot_of(t) * RSTR;
+            const int o1 = slot_of(t + 1) * RSTR, o2 = slot_of(t + 2) * RSTR, o3 = slot_of(t + 3) * RSTR;
+            const int o4 = slot_of(t + 4) * RSTR;
+            // ---- faces of rows t+2, t+3 (Pass1), their aux, and the y fluxes of rows t, t+1 ----
+            Face2 f;
+            faces_at2(ring, o1, o2, o3, o4, rc0, c, f);
+            const int npar = (j + 1) & 1, par = j & 1;
+            fW[npar][0][0][tid] = f.hW.x; fW[npar][0][1][tid] = f.uW.x; fW[npar][0][2][tid] = f.vW.x;
+            fW[npar][1][0][tid] = f.hW.y; fW[npar][1][1][tid] = f.uW.y; fW[npar][1][2][tid] = f.vW.y;
+            {
+                const f2 md = mul2(add2(add2(f.hN, f.hE), add2(f.hS, f.hW)), S2(0.25f));
+                if (aux_ok[0]) {
+                    const float bw = (f.msd.x > M.tan_thr) ? 1.0f : aux_old[0].y;   // atan(msd) > threshold
+                    *ap[0] = make_float2(fmaxf(md.x, aux_old[0].x), bw * decay);
+                }
+                if (aux_ok[1]) {
+                    const float bw = (f.msd.y > M.tan_thr) ? 1.0f : aux_old[1].y;
+                    *ap[1] = make_float2(fmaxf(md.y, aux_old[1].x), bw * decay);
+                }
+            }
+            const float g = c.g, hg = c.half_g;
+            f2 yf[3];   // north faces of rows t, t+1: (N(t) vs S(t+1)), (N(t+1) vs S(t+2))
+            face_flux2(fp.hN, fp.uN, fp.vN, P2(fp.hS1, f.hS.x), P2(fp.uS1, f.uS.x), P2(fp.vS1, f.vS.x), g, hg,
+                       false, yf);
+            {   // x fluxes of rows t, t+1 at this thread's east face
+                const int tn = min(tid + 1, MW - 1);
+                f2 xo[3];
+                face_flux2(fp.hE, fp.uE, fp.vE, P2(fW[par][0][0][tn], fW[par][1][0][tn]),
+                           P2(fW[par][0][1][tn], fW[par][1][1][tn]), P2(fW[par][0][2][tn], fW[par][1][2][tn]), g,
+                           hg, true, xo);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) { xb[0][k][tid] = xo[k].x; xb[1][k][tid] = xo[k].y; }
+            }
+            __syncthreads();  // (B)
+            // ---- Pass3 at (xc, t) and (xc, t+1) ----
+            if (p3) {
+                const int am2 = om2 + rc, am1 = om1 + rc, a0 = o0 + rc, a1 = o1 + rc, a2 = o2 + rc, a3 = o3 + rc;
+                // rows t, t+1 as pairs; "d" = the row below, "u" = the row above
+                const f2 wc = P2(W[a0], W[a1]);
+                const f2 huc = P2(HU[a0], HU[a1]), hvc = P2(HV[a0], HV[a1]);
+                const f2 BAh = P2(BAr[a0], BAr[a1]), BXh = P2(BXr[a0], BXr[a1]), BYh = P2(BYr[a0], BYr[a1]);
+                const f2 BXw = P2(BXr[a0 - 1], BXr[a1 - 1]), BYs = P2(BYr[am1], BYr[a0]);
+                const f2 h = max2(S2(0.f), sub2(wc, BAh));
+                const f2 dh = P2(dring[a0], dring[a1]), d2 = mul2(dh, dh), d3 = mul2(d2, dh);
+                const f2 dl = P2(dring[a0 - 1], dring[a1 - 1]), dr = P2(dring[a0 + 1], dring[a1 + 1]);
+                const f2 dll = P2(dring[a0 - 2], dring[a1 - 2]), drr = P2(dring[a0 + 2], dring[a1 + 2]);
+                const f2 ddn = P2(dring[am1], dring[a0]), du = P2(dring[a1], dring[a2]);
+                const f2 ddd = P2(dring[am2], dring[am1]), duu = P2(dring[a2], dring[a3]);
+                // eta = w - sea level enters only through differences, where the sea level cancels
+                const f2 ec = wc, el_ = P2(W[a0 - 1], W[a1 - 1]), er = P2(W[a0 + 1], W[a1 + 1]);
+                const f2 ed = P2(W[am1], W[a0]), eu_ = P2(W[a1], W[a2]);
+                const f2 ell = P2(W[a0 - 2], W[a1 - 2]), err = P2(W[a0 + 2], W[a1 + 2]);
+                const f2 edd = P2(W[am2], W[am1]), euu = P2(W[a2], W[a3]);
+                const f2 eul = P2(W[a1 - 1], W[a2 - 1]), eur = P2(W[a1 + 1], W[a2 + 1]);
+                const f2 edl = P2(W[am1 - 1], W[a0 - 1]), edr = P2(W[am1 + 1], W[a0 + 1]);
+                const float odx = c.one_over_dx, ody = c.one_over_dy;
+                const float od2x = odx * odx, od3x = od2x * odx, od2y = ody * ody, od3y = od2y * ody;
+                const f2 two = S2(2.f), eight = S2(8.f);
+                // (-r2 + 8 r1 - 8 l1 + l2) / 12 per unit length
+                const f2 ddx = mul2(add2(sub2(fma2(eight, dr, P2(-drr.x, -drr.y)), mul2(eight, dl)), dll),
+                                    S2(odx * (1.0f / 12.0f)));
+                const f2 ddy = mul2(add2(sub2(fma2(eight, du, P2(-duu.x, -duu.y)), mul2(eight, ddn)), ddd),
+                                    S2(ody * (1.0f / 12.0f)));
+                const f2 exy = mul2(S2(0.25f * odx * ody), add2(sub2(sub2(eur, edr), eul), edl));
+                const f2 exx = mul2(S2(od2x), add2(fma2(S2(-2.f), ec, er), el_));
+                const f2 eyy = mul2(S2(od2y), add2(fma2(S2(-2.f), ec, eu_), ed));
+                const f2 Bg = S2(c.Bcoef_g);
+                const f2 P1x = mul2(mul2(Bg, d3),
+                    fma2(sub2(fma2(two, el_, fma2(S2(-2.f), er, err)), ell), S2(0.5f * od3x),
+                         mul2(sub2(add2(fma2(two, el_, fma2(S2(-2.f), er, sub2(eur, eul))), edr), edl),
+                              S2(0.5f * odx * od2y))));
+                const f2 P2x = mul2(mul2(Bg, d2), fma2(ddx, fma2(two, exx, eyy), mul2(ddy, exy)));
+                const f2 P1y = mul2(mul2(Bg, d3),
+                    fma2(sub2(fma2(two, ed, fma2(S2(-2.f), eu_, euu)), edd), S2(0.5f * od3y),
+                         mul2(sub2(sub2(fma2(two, ed, fma2(S2(-2.f), eu_, add2(eur, eul))), edr), edl),
+                              S2(0.5f * ody * od2x))));
+                const f2 P2y = mul2(mul2(Bg, d2), fma2(ddy, fma2(two, eyy, exx), mul2(ddx, exy)));
+                f2 fr = S2(0.f);
+                if (pa.friction)
+                    fr = P2(friction_fast(huc.x, hvc.x, h.x, c.friction, c.is_manning, c.g, c.epsilon),
+                            friction_fast(huc.y, hvc.y, h.y, c.friction, c.is_manning, c.g, c.epsilon));
+                const f2 s1 = add2(sub2(mul2(mul2(S2(-c.g_over_dx), h), sub2(BXh, BXw)), mul2(huc, fr)), add2(P1x, P2x));
+                const f2 s2 = add2(sub2(mul2(mul2(S2(-c.g_over_dy), h), sub2(BYh, BYs)), mul2(hvc, fr)), add2(P1y, P2y));
+                const int tw = max(tid - 1, 0);
+                f2 fl[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    // x fluxes: west face (the neighbour's east face) minus east face; y fluxes: the
+                    // south faces of rows t, t+1 are the north faces of rows t-1, t
+                    const f2 xw = P2(xb[0][k][tw], xb[1][k][tw]), xh = P2(xb[0][k][tid], xb[1][k][tid]);
+                    const f2 ys = P2(ypv[k], yf[k].x);
+                    fl[k] = fma2(sub2(xw, xh), S2(odx), mul2(sub2(ys, yf[k]), S2(ody)));
+                }
+                const f2 f0 = fl[0], f1 = add2(fl[1], s1), f2v = add2(fl[2], s2);
+                const f2 sixth = S2(1.0f / 6.0f);
+                const f2 Fs = mul2(mul2(sixth, dh),
+                                   fma2(ddx, mul2(S2(ody * 0.5f), sub2(P2(HV[a1], HV[a2]), P2(HV[am1], HV[a0]))),
+                                        mul2(ddy, mul2(S2(odx * 0.5f), sub2(P2(HV[a0 + 1], HV[a1 + 1]), P2(HV[a0 - 1], HV[a1 - 1]))))));
+                const f2 Gs = mul2(mul2(sixth, dh),
+                                   fma2(ddx, mul2(S2(ody * 0.5f), sub2(P2(HU[a1], HU[a2]), P2(HU[am1], HU[a0]))),
+                                        mul2(ddy, mul2(S2(odx * 0.5f), sub2(P2(HU[a0 + 1], HU[a1 + 1]), P2(HU[a0 - 1], HU[a1 - 1]))))));
+                const f2 dt = S2(dtm);
+                f2 dw, rhu, rhv;
+                f2 wbase = wc;
+                if (euler) {
+                    dw = mul2(dt, f0); rhu = mul2(dt, f1); rhv = mul2(dt, f2v);
+                } else if (!corr) {
+                    const f2 k12 = S2(dtm * (1.0f / 12.0f));
+                    const f2 o_x = P2(ho0.x, ho1.x), o_y = P2(ho0.y, ho1.y), o_z = P2(ho0.z, ho1.z), o_w = P2(ho0.w, ho1.w);
+                    const f2 q_x = P2(hoo0.x, hoo1.x), q_y = P2(hoo0.y, hoo1.y), q_z = P2(hoo0.z, hoo1.z), q_w = P2(hoo0.w, hoo1.w);
+                    const f2 c23 = S2(23.0f), c16 = S2(-16.0f), c5 = S2(5.0f);
+                    dw = mul2(k12, fma2(c5, q_x, fma2(c16, o_x, mul2(c23, f0))));
+                    rhu = fma2(k12, fma2(c5, q_y, fma2(c16, o_y, mul2(c23, f1))), add2(fma2(S2(-3.f), o_w, mul2(two, Fs)), q_w));
+                    rhv = fma2(k12, fma2(c5, q_z, fma2(c16, o_z, mul2(c23, f2v))), add2(fma2(S2(-3.f), go, mul2(two, Gs)), goo));
+                } else {
+                    const f2 k24 = S2(dtm * (1.0f / 24.0f));
+                    const f2 o_x = P2(ho0.x, ho1.x), o_y = P2(ho0.y, ho1.y), o_z = P2(ho0.z, ho1.z);
+                    const f2 q_x = P2(hoo0.x, hoo1.x), q_y = P2(hoo0.y, hoo1.y), q_z = P2(hoo0.z, hoo1.z);
+                    const f2 p_x = P2(hp0.x, hp1.x), p_y = P2(hp0.y, hp1.y), p_z = P2(hp0.z, hp1.z), p_w = P2(hp0.w, hp1.w);
+                    const f2 c9 = S2(9.f), c19 = S2(19.f), c5 = S2(-5.f);
+                    dw = mul2(k24, add2(fma2(c5, o_x, fma2(c19, p_x, mul2(c9, f0))), q_x));
+                    rhu = add2(fma2(k24, add2(fma2(c5, o_y, fma2(c19, p_y, mul2(c9, f1))), q_y), Fs), P2(-p_w.x, -p_w.y));
+                    rhv = add2(fma2(k24, add2(fma2(c5, o_z, fma2(c19, p_z, mul2(c9, f2v))), q_z), Gs), P2(-gp.x, -gp.y));
+                    wbase = wcur;
+                }
+                f2 wn = wbase, wl = wlo;
+                if (MIXED) {
+                    float a = wn.x, b = wl.x, cc = wn.y, d = wl.y;
+                    two_sum_add(a, b, dw.x);
+                    two_sum_add(cc, d, dw.y);
+                    wn = P2(a, cc); wl = P2(b, d);
+                } else {
+                    wn = add2(wbase, dw);
+                }
+                if (out_col) {
+                    Wout[e0] = wn.x;
+                    if (MIXED) Lout[e0] = wl.x;
+                    R0[e0] = rhu.x;
+                    R0[e0 + PL] = rhv.x;
+                    HAs[e0] = make_float4(f0.x, f1.x, f2v.x, Fs.x);
+                    HBs[e0] = Gs.x;
+                    if (row1) {
+                        Wout[e1] = wn.y;
+                        if (MIXED) Lout[e1] = wl.y;
+                        R0[e1] = rhu.y;
+                        R0[e1 + PL] = rhv.y;
+                        HAs[e1] = make_float4(f0.y, f1.y, f2v.y, Fs.y);
+                        HBs[e1] = Gs.y;
+                    }
+                }
+                if (stats) {   // GetStats (compute.hlsl:1319-1378) of the input state
+                    const f2 q = div_by_h2(h, c.epsilon);
+                    const f2 u = mul2(q, huc), v = mul2(q, hvc);
+                    const bool in_cols = out_col && xc < 2 + 4 * (nx / 4);
+                    const bool b0 = in_cols && t < 2 + 4 * (ny / 4), b1 = in_cols && row1 && t + 1 < 2 + 4 * (ny / 4);
+                    const bool a0_ = out_col, a1_ = out_col && row1;
+                    auto pick = [](bool k0, bool k1, f2 v_) { return P2(k0 ? v_.x : 0.f, k1 ? v_.y : 0.f); };
+                    const f2 u2v2 = fma2(u, u, mul2(v, v));
+                    const f2 cc = P2(sqrtf(c.g * h.x), sqrtf(c.g * h.y));
+                    acc[0].add(pick(b0, b1, h));
+                    acc[1].add(pick(b0, b1, mul2(h, fma2(S2(0.5f), h, BAh))));
+                    acc[2].add(pick(b0, b1, huc));
+                    acc[3].add(pick(b0, b1, hvc));
+                    acc[4].add(pick(b0, b1, fma2(huc, u, mul2(hvc, v))));
+                    mx[0] = max2(mx[0], pick(b0, b1, u2v2));
+                    mx[1] = max2(mx[1], pick(b0, b1, h));
+                    const f2 cx = mul2(add2(P2(fabsf(u.x), fabsf(u.y)), cc), S2(odx));
+                    const f2 cy = mul2(add2(P2(fabsf(v.x), fabsf(v.y)), cc), S2(ody));
+                    mx[2] = max2(mx[2], pick(b0, b1, max2(cx, cy)));
+                    mx[3] = max2(mx[3], pick(b0, b1, mul2(u2v2, q)));
+                    acc[5].add(pick(a0_, a1_, h));
+                    const bool nb0 = !(fabsf(wc.x) <= 3.0e38f && fabsf(huc.x) <= 3.0e38f && fabsf(hvc.x) <= 3.0e38f);
+                    const bool nb1 = !(fabsf(wc.y) <= 3.0e38f && fabsf(huc.y) <= 3.0e38f && fabsf(hvc.y) <= 3.0e38f);
+                    bad = bad | (a0_ & nb0) | (a1_ & nb1);
+                }
+            }
+            // the y flux through the north face of row t+1 is the south flux of the next pair's first row
+            ypv[0] = yf[0].y; ypv[1] = yf[1].y; ypv[2] = yf[2].y;
+            fp.set(f);
+        }
+        seq = seq0 + unsigned(last_row - (y0 - 2) + 1);
+        // ---- zero the ghost ring of the output state next to this strip (engine.cpp:1007) ----
+        const int NX = c.NX, NY = c.NY;
+        const bool west = x0 == 2, east = x0 + MO >= nx + 2, south = y0 == 2, north = y0 + MH >= ny + 2;
+        if (west || east || south || north) {
+            const int cx0 = west ? 0 : x0, cx1 = east ? NX : x0 + MO;
+            const int cy0 = south ? 0 : y0, cy1 = north ? NY : y0 + MH;
+            const int w = cx1 - cx0;
+            for (int k = tid; k < w * (cy1 - cy0); k += MW) {
+                const int gx = cx0 + k % w, gy = cy0 + k / w;
+                if (gx >= 2 && gx < nx + 2 && gy >= 2 && gy < ny + 2) continue;
+                const size_t gi = size_t(gy) * P + gx;
+                for (int q = 0; q < 3; ++q) {
+                    Wout[gi + q * PL] = 0.f;
+                    if (MIXED) Lout[gi + q * PL] = 0.f;
+                }
+            }
+        }
+        if (stats) {
+            double sv[STATS_N];
+            for (int k = 0; k < 6; ++k) sv[k] = acc[k].value();
+            for (int k = 0; k < 4; ++k) sv[6 + k] = fmaxf(mx[k].x, mx[k].y);
+            sv[10] = bad ? 1.0 : 0.0;
+            sv[11] = 0.0;
+            for (int off = 16; off; off >>= 1)
+                for (int k = 0; k < STATS_N - 1; ++k) {
+                    const double o = __shfl_down_sync(0xffffffffu, sv[k], off);
+                    sv[k] = (k >= 6) ? fmax(sv[k], o) : sv[k] + o;
+                }
+            double (*red)[STATS_N] = reinterpret_cast<double (*)[STATS_N]>(ring);
+            const int lane = tid & 31, wid = tid >> 5;
+            __syncthreads();
+            if (lane == 0)
+                for (int k = 0; k < STATS_N - 1; ++k) red[wid][k] = sv[k];
+            __syncthreads();
+            if (tid < STATS_N - 1) {
+                double a = red[0][tid];
+                for (int w = 1; w < MW / 32; ++w) a = (tid >= 6) ? fmax(a, red[w][tid]) : a + red[w][tid];
+                if (tid < 6) { if (a != 0.0) atomicAdd(M.stats + tid, a); }
+                else atomic_max_nonneg(M.stats + tid, a);
+            }
+        }
+    }
     if (__syncthreads_or(tma_late) && tid == 0) atomic_max_nonneg(pa.late_flag, 1.0);
 }
 
@@ -1337,6 +1883,7 @@ struct cel_batch {
     long long cells = 0;
     int cw = 16;                        // column solver band width (columns per CTA)
     int mh = cel::MH_DEFAULT;           // stencil strip height (rows per CTA work item)
+    int rows_per_step = 1;              // stencil rows per thread step: 1 (k_march) or 2 (k_march2)
     int max_nx = 0, max_ny = 0;
 };
 
@@ -1420,10 +1967,13 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     if (pa.stats) B_TRY(cudaMemsetAsync(b->stats_all, 0, nm * STATS_N * sizeof(double), b->stream));
     {
         TimedLaunch t(&b->tm, b->stream, "fused_stencil");
-        if (b->mixed)
-            k_march<true><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
-        else
-            k_march<false><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
+        if (b->rows_per_step == 2) {
+            if (b->mixed) k_march2<true><<<b->grid_stencil, MW, MARCH2_DYN_SMEM, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
+            else k_march2<false><<<b->grid_stencil, MW, MARCH2_DYN_SMEM, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
+        } else {
+            if (b->mixed) k_march<true><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
+            else k_march<false><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
+        }
     }
     // the row (x) and column (y) solves are independent: fork the column solve onto the side
     // stream and join before the boundaries (a fork/join pair inside the captured graph)
@@ -1575,7 +2125,9 @@ void byte_model(int form, int N, double& stencil, double& step) {
 
 // (Re)builds the stencil strips (height mh) and the column bands (width cw) of a batch, sizes the
 // column solver's shared memory and grids, and drops captured graphs (they hold the old lists).
-int configure_work(cel_batch* b, int cw, int mh, std::string& err) {
+int configure_work(cel_batch* b, int cw, int mh, int rps, std::string& err) {
+    if (rps != 1 && rps != 2) { err = "stencil rows per step must be 1 or 2"; return CEL_ERR_ARG; }
+    b->rows_per_step = rps;
     if (cw != 1 && cw != 8 && cw != 16 && cw != 32) { err = "column band width must be 1, 8, 16 or 32"; return CEL_ERR_ARG; }
     if (mh < 8 || mh > 1024) { err = "strip height must be in [8, 1024]"; return CEL_ERR_ARG; }
     const size_t smem_cols = cw == 1 ? 0 : sizeof(float) * size_t(b->max_ny) * cw;
@@ -1624,7 +2176,13 @@ int configure_work(cel_batch* b, int cw, int mh, std::string& err) {
         B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc, NTC, smem_cols));
         b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
     }
-    B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->mixed ? k_march<true> : k_march<false>, MW, 0));
+    if (b->rows_per_step == 2) {
+        auto* k2 = b->mixed ? k_march2<true> : k_march2<false>;
+        B_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, int(MARCH2_DYN_SMEM)));
+        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k2, MW, MARCH2_DYN_SMEM));
+    }
+    else
+        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->mixed ? k_march<true> : k_march<false>, MW, 0));
     b->grid_stencil = std::max(1, std::min(b->nmtiles, b->sms * std::max(occ, 1)));
     return CEL_OK;
 }
@@ -1848,7 +2406,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     }
     {   // column bands of 16 columns (8 for tall domains: shared-memory capacity), strips of 64 rows
         const int cw = (size_t(max_ny) * 16 * sizeof(float) + 8192 <= 227 * 1024) ? 16 : 8;
-        if (configure_work(b.get(), cw, MH_DEFAULT, err)) return nullptr;
+        if (configure_work(b.get(), cw, MH_DEFAULT, 1, err)) return nullptr;
     }
     b->sch.reset(*params[0]);
     cudaMemcpy(b->dt_table, b->dt_host, sizeof(float) * n, cudaMemcpyHostToDevice);
@@ -2040,13 +2598,18 @@ int batch_set_timestep(cel_batch* b, const float* dt, std::string& err) {
 
 int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err) {
     (void)pcr;   // the solves have no cyclic-reduction stage to hand over from (Thomas factors + scans)
-    return configure_work(b, tx > 0 ? tx : b->cw, ty > 0 ? ty : b->mh, err);
+    return configure_work(b, tx > 0 ? tx : b->cw, ty > 0 ? ty : b->mh, b->rows_per_step, err);
 }
 
-int batch_get_tuning(const cel_batch* b, int* tx, int* ty) {
+int batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rps) {
     if (tx) *tx = b->cw;
     if (ty) *ty = b->mh;
+    if (rps) *rps = b->rows_per_step;
     return CEL_OK;
+}
+
+int batch_set_stencil_rows(cel_batch* b, int rps, std::string& err) {
+    return configure_work(b, b->cw, b->mh, rps, err);
 }
 
 // Times `steps` physical steps for every candidate (band width, strip height), in the launch mode
@@ -2054,10 +2617,11 @@ int batch_get_tuning(const cel_batch* b, int* tx, int* ty) {
 // better round.  The ensemble advances by every step taken here.
 int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, std::string& err) {
     if (steps < 1) { err = "autotune needs at least one step per candidate"; return CEL_ERR_ARG; }
-    std::vector<int2> cand;
-    for (int cw : {1, 8, 16, 32})
-        if (cw == 1 || sizeof(float) * size_t(b->max_ny) * cw + 8192 <= 227 * 1024)
-            for (int mh : {32, 64, 128}) cand.push_back(make_int2(cw, mh));
+    std::vector<int3> cand;
+    for (int rps : {1, 2})
+        for (int cw : {1, 8, 16, 32})
+            if (cw == 1 || sizeof(float) * size_t(b->max_ny) * cw + 8192 <= 227 * 1024)
+                for (int mh : {32, 64, 128}) cand.push_back(make_int3(cw, mh, rps));
     std::vector<double> best(cand.size(), 1e300);
     cudaEvent_t e0, e1;
     B_TRY(cudaEventCreate(&e0));
@@ -2065,7 +2629,7 @@ int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, s
     int rc = CEL_OK;
     for (int round = 0; round < 2 && !rc; ++round)
         for (size_t k = 0; k < cand.size() && !rc; ++k) {
-            if ((rc = configure_work(b, cand[k].x, cand[k].y, err))) break;
+            if ((rc = configure_work(b, cand[k].x, cand[k].y, cand[k].z, err))) break;
             if ((rc = batch_step(b, 2, err))) break;   // warm-up (captures the graphs in graph mode)
             cudaEventRecord(e0, b->stream);
             if ((rc = batch_step(b, steps, err))) break;
@@ -2079,7 +2643,7 @@ int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, s
     cudaEventDestroy(e1);
     if (rc) return rc;
     const size_t kb = size_t(std::min_element(best.begin(), best.end()) - best.begin());
-    if ((rc = configure_work(b, cand[kb].x, cand[kb].y, err))) return rc;
+    if ((rc = configure_work(b, cand[kb].x, cand[kb].y, cand[kb].z, err))) return rc;
     if (tx) *tx = cand[kb].x;
     if (ty) *ty = cand[kb].y;
     if (best_ms) *best_ms = best[kb];

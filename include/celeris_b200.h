@@ -200,8 +200,12 @@ int cel_batch_launches_per_step(const cel_batch* b);
  * scans, with no cyclic-reduction stage to hand over from.  Plain engines ignore the call. */
 int cel_set_tuning(cel_engine* h, int tile_x, int tile_y, int pcr_switch);
 int cel_batch_set_tuning(cel_batch* b, int tile_x, int tile_y, int pcr_switch);
-int cel_batch_get_tuning(const cel_batch* b, int* tile_x, int* tile_y);
-/* Times `steps` physical steps for each candidate (band width x strip height) and keeps the
+int cel_batch_get_tuning(const cel_batch* b, int* tile_x, int* tile_y, int* rows_per_step);
+/* Stencil variant: 1 = one row per thread step; 2 = two rows per step as pairs, with the paired
+ * single-precision instructions of sm_100 (f32x2). */
+int cel_batch_set_stencil_rows(cel_batch* b, int rows_per_step);
+/* Times `steps` physical steps for each candidate (band width x strip height x stencil rows per
+ * step) and keeps the
  * fastest; writes the choice and its ms per step.  The members advance by every timed step. */
 int cel_batch_autotune(cel_batch* b, int steps, int* tile_x, int* tile_y, double* ms_per_step);
 /* Per-kernel CUDA-event timing on the launching stream (off by default). */

@@ -183,3 +183,42 @@ def test_tuning_changes_decomposition_not_results(celeris):
     t.use_graph(True)
     t.step(5)
     assert np.isfinite(t.state(0)).all()
+
+
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+@pytest.mark.parametrize("kind", KINDS)
+def test_paired_row_stencil_vs_fp64_oracle(celeris, form, kind):
+    """The two-rows-per-step stencil (paired f32x2 arithmetic) against the FP64 oracle."""
+    p, z, bnx, bny, keep = _case(kind, nx=70, ny=45, N=1)
+    ref = O.Oracle(p, z, bnx, bny, "f64")
+    b = celeris.Batch([(p, z)], form)
+    b.set_stencil_rows(2)
+    assert b.stencil_rows == 2
+    ref.physical_steps(200)
+    b.step(200)
+    a = b.state(0)
+    assert np.isfinite(a).all()
+    assert eta_rms(a, ref.state()) <= 1e-4
+    assert rel_ok(field_errors(a, ref.state()), 2e-3, 1e-6)
+
+
+def test_paired_row_stencil_matches_single_row(celeris):
+    """Both stencils on the same ensemble (odd and even strip heights): the fields agree to FP32
+    rounding and the aux texture (max depth, breaking) is identical in coverage."""
+    members = [_case(k, nx=150 + 10 * i, ny=71 + 30 * i, N=1)[:4] for i, k in enumerate(["mixed", "sponge", "irregular"])]
+    for sh in (32, 33):
+        b1 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+        b2 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+        b1.set_tuning(16, sh)
+        b2.set_tuning(16, sh)
+        b2.set_stencil_rows(2)
+        b1.step(40)
+        b2.step(40)
+        for i in range(len(members)):
+            assert rel_ok(field_errors(b2.state(i), b1.state(i)), 1e-5, 1e-9), (sh, i)
+            a1, a2 = b1.aux(i), b2.aux(i)
+            np.testing.assert_allclose(a2[..., 0], a1[..., 0], rtol=1e-4, atol=1e-6)
+            assert ((a1[..., 3] > 0) == (a2[..., 3] > 0)).mean() > 0.999
+        s1, s2 = b1.stats(), b2.stats()
+        for x, y in zip(s1, s2):
+            assert y["mass_full"] == pytest.approx(x["mass_full"], rel=1e-9)
