@@ -28,6 +28,7 @@ struct HostSetup {
     std::vector<float> BY, BX, BA;          // staggered bottom, NX*NY each
     std::vector<float> corners;             // bathymetry sampled at cell corners, (NX+1)*(NY+1)
     std::vector<float> ic;                  // initial (w, hu, hv) per texel, NX*NY*3
+    std::vector<double> ic64;               // the same in double precision (for the compensated form)
     // Cyclic-reduction coefficient levels, {A, B, C, 0} per texel (engine.cpp:2612-2887)
     int Kx = 0, Ky = 0;
     std::vector<int> lenx, leny;

@@ -104,8 +104,8 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
 
 // Block reduction of the GetStats quantities of one cell per thread into the member's
 // accumulators (FP64 sums, maxima via the ordering of non-negative doubles).
-__device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h, float B, float hu, float hv,
-                             float u, float v, float q, float cc, float odx, float ody, bool bad,
+__device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h, double h64, float B, float hu,
+                             float hv, float u, float v, float q, float cc, float odx, float ody, bool bad,
                              double (*red)[STATS_N]) {
     double s[STATS_N];
     for (int k = 0; k < STATS_N; ++k) s[k] = 0.0;
@@ -116,7 +116,7 @@ __device__ void stats_reduce(double* acc, bool cnt_block, bool cnt_all, float h,
         s[8] = fmaxf((fabsf(u) + cc) * odx, (fabsf(v) + cc) * ody);
         s[9] = u2v2 * q;
     }
-    if (cnt_all) s[5] = h;
+    if (cnt_all) s[5] = h64;
     s[10] = bad ? 1.0 : 0.0;
     for (int off = 16; off; off >>= 1)
         for (int k = 0; k < 11; ++k) {
@@ -416,7 +416,8 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
             if (tid < 2) dr[d2c] = fmaxf(0.f, sl - ba[d2c]);
         };
 
-        Kahan acc[6];
+        Kahan acc[5];
+        double mfull = 0.0;
         float mx[4] = {0.f, 0.f, 0.f, 0.f};
         bool bad = false;
         float nh = 0.f, nu = 0.f, nv = 0.f;       // north face of the previous row (this column)
@@ -591,7 +592,8 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
                     mx[0] = fmaxf(mx[0], blk ? u2v2 : 0.f); mx[1] = fmaxf(mx[1], blk ? h : 0.f);
                     mx[2] = fmaxf(mx[2], blk ? fmaxf((fabsf(u) + cc) * odx, (fabsf(v) + cc) * ody) : 0.f);
                     mx[3] = fmaxf(mx[3], blk ? u2v2 * q : 0.f);
-                    acc[5].add(out_col ? h : 0.f);
+                    // volume in FP64 from the compensated state (w + its low word)
+                    if (out_col) mfull += fmax(0.0, double(wc) - double(BAh) + (MIXED ? double(wlo) : 0.0));
                     bad = bad | (out_col & !(fabsf(wc) <= 3.0e38f && fabsf(huc) <= 3.0e38f && fabsf(hvc) <= 3.0e38f));
                 }
             }
@@ -626,7 +628,8 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
         // ---- strip statistics -> member accumulators (statistics pass only) ----
         if (stats) {
             double sv[STATS_N];
-            for (int k = 0; k < 6; ++k) sv[k] = acc[k].value();
+            for (int k = 0; k < 5; ++k) sv[k] = acc[k].value();
+            sv[5] = mfull;
             for (int k = 0; k < 4; ++k) sv[6 + k] = mx[k];
             sv[10] = bad ? 1.0 : 0.0;
             sv[11] = 0.0;
@@ -888,7 +891,8 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
             if (tid < 2) dr[d2c] = fmaxf(0.f, sl - ba[d2c]);
         };
 
-        Kahan2 acc[6];
+        Kahan2 acc[5];
+        double mfull = 0.0;
         f2 mx[4] = {S2(0.f), S2(0.f), S2(0.f), S2(0.f)};
         bool bad = false;
 
@@ -1142,7 +1146,9 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
                     const f2 cy = mul2(add2(P2(fabsf(v.x), fabsf(v.y)), cc), S2(ody));
                     mx[2] = max2(mx[2], pick(b0, b1, max2(cx, cy)));
                     mx[3] = max2(mx[3], pick(b0, b1, mul2(u2v2, q)));
-                    acc[5].add(pick(a0_, a1_, h));
+                    // volume in FP64 from the compensated state (w + its low word)
+                    if (a0_) mfull += fmax(0.0, double(wc.x) - double(BAh.x) + (MIXED ? double(wlo.x) : 0.0));
+                    if (a1_) mfull += fmax(0.0, double(wc.y) - double(BAh.y) + (MIXED ? double(wlo.y) : 0.0));
                     const bool nb0 = !(fabsf(wc.x) <= 3.0e38f && fabsf(huc.x) <= 3.0e38f && fabsf(hvc.x) <= 3.0e38f);
                     const bool nb1 = !(fabsf(wc.y) <= 3.0e38f && fabsf(huc.y) <= 3.0e38f && fabsf(hvc.y) <= 3.0e38f);
                     bad = bad | (a0_ & nb0) | (a1_ & nb1);
@@ -1172,7 +1178,8 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
         }
         if (stats) {
             double sv[STATS_N];
-            for (int k = 0; k < 6; ++k) sv[k] = acc[k].value();
+            for (int k = 0; k < 5; ++k) sv[k] = acc[k].value();
+            sv[5] = mfull;
             for (int k = 0; k < 4; ++k) sv[6 + k] = fmaxf(mx[k].x, mx[k].y);
             sv[10] = bad ? 1.0 : 0.0;
             sv[11] = 0.0;
@@ -1211,19 +1218,24 @@ __global__ void __launch_bounds__(256) k_stats_only(const MemberDev* __restrict_
             const int gx = tl.y + k % TX, gy = tl.z + k / TX;
             const bool valid = gx < c.nx + 2 && gy < c.ny + 2;
             float h = 0, B = 0, hu = 0, hv = 0, u = 0, v = 0, q = 0, cc = 0;
+            double h64 = 0.0;
             bool bad = false;
             if (valid) {
                 const size_t gi = size_t(gy) * M.P + gx;
                 const float w = M.S[buf][0][gi];
                 hu = M.S[buf][1][gi]; hv = M.S[buf][2][gi]; B = M.BA[gi];
                 h = fmaxf(0.f, w - B);
+                // the volume total in FP64 from the compensated state where there is one (the FP32
+                // difference w - B drops positive parts of eta below half an ulp of the depth)
+                h64 = fmax(0.0, double(w) - double(B) + (M.L[buf][0] ? double(M.L[buf][0][gi]) : 0.0));
                 q = div_by_h(h, c.epsilon);
                 u = q * hu; v = q * hv;
                 cc = sqrtf(c.g * h);
                 bad = !isfinite(w) || !isfinite(hu) || !isfinite(hv);
             }
             const bool in_block = valid && gx < 2 + 4 * (c.nx / 4) && gy < 2 + 4 * (c.ny / 4);
-            stats_reduce(M.stats_now, in_block, valid, h, B, hu, hv, u, v, q, cc, c.one_over_dx, c.one_over_dy, bad, red);
+            stats_reduce(M.stats_now, in_block, valid, h, h64, B, hu, hv, u, v, q, cc, c.one_over_dx, c.one_over_dy, bad,
+                         red);
             __syncthreads();
         }
     }
@@ -1937,19 +1949,27 @@ int dalloc(cel_batch* b, void** ptr, size_t bytes, std::string& err) {
         if (_e != cudaSuccess) { err = std::string(#expr) + ": " + cudaGetErrorString(_e); return CEL_ERR_CUDA; } \
     } while (0)
 
-int upload_state(cel_batch* b, int i, const float* rgba, std::string& err) {
+// Uploads a member's state (RGBA texels); `lo3`, when given, holds the mixed form's low words
+// (3 per texel), else they start at zero.
+int upload_state(cel_batch* b, int i, const float* rgba, std::string& err, const float* lo3 = nullptr) {
     b->step_stats_valid = false;
     Member& m = b->mem[i];
     const MemberDev& d = b->hdev[i];
     const int NX = m.hs.NX, NY = m.hs.NY;
-    std::vector<float> pl[3];
-    for (int q = 0; q < 3; ++q) pl[q].assign(m.plane, 0.f);
+    std::vector<float> pl[3], lp[3];
+    for (int q = 0; q < 3; ++q) { pl[q].assign(m.plane, 0.f); lp[q].assign(lo3 ? m.plane : 0, 0.f); }
     for (int y = 0; y < NY; ++y)
         for (int x = 0; x < NX; ++x)
-            for (int q = 0; q < 3; ++q) pl[q][size_t(y) * m.P + x] = rgba[(size_t(y) * NX + x) * 4 + q];
+            for (int q = 0; q < 3; ++q) {
+                pl[q][size_t(y) * m.P + x] = rgba[(size_t(y) * NX + x) * 4 + q];
+                if (lo3) lp[q][size_t(y) * m.P + x] = lo3[(size_t(y) * NX + x) * 3 + q];
+            }
     for (int q = 0; q < 3; ++q) {
         B_TRY(cudaMemcpyAsync(d.S[b->ix.sin][q], pl[q].data(), m.plane * sizeof(float), cudaMemcpyHostToDevice, b->stream));
-        if (b->mixed) B_TRY(cudaMemsetAsync(d.L[b->ix.sin][q], 0, m.plane * sizeof(float), b->stream));
+        if (b->mixed) {
+            if (lo3) B_TRY(cudaMemcpyAsync(d.L[b->ix.sin][q], lp[q].data(), m.plane * sizeof(float), cudaMemcpyHostToDevice, b->stream));
+            else B_TRY(cudaMemsetAsync(d.L[b->ix.sin][q], 0, m.plane * sizeof(float), b->stream));
+        }
     }
     B_TRY(cudaStreamSynchronize(b->stream));
     return CEL_OK;
@@ -2415,11 +2435,24 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     // initial condition
     for (int i = 0; i < n; ++i) {
         const HostSetup& hs = b->mem[i].hs;
-        std::vector<float> rgba(size_t(hs.NX) * hs.NY * 4, 0.f);
-        for (size_t k = 0; k < size_t(hs.NX) * hs.NY; ++k) {
-            rgba[4 * k] = hs.ic[3 * k]; rgba[4 * k + 1] = hs.ic[3 * k + 1]; rgba[4 * k + 2] = hs.ic[3 * k + 2];
+        const size_t nt = size_t(hs.NX) * hs.NY;
+        std::vector<float> rgba(nt * 4, 0.f), lo;
+        if (b->mixed) {
+            // the compensated form starts from the double-precision initial condition: hi + lo
+            lo.assign(nt * 3, 0.f);
+            for (size_t k = 0; k < nt; ++k)
+                for (int q = 0; q < 3; ++q) {
+                    const double v = hs.ic64[3 * k + q];
+                    const float hi = float(v);
+                    rgba[4 * k + q] = hi;
+                    lo[3 * k + q] = float(v - double(hi));
+                }
+        } else {
+            for (size_t k = 0; k < nt; ++k) {
+                rgba[4 * k] = hs.ic[3 * k]; rgba[4 * k + 1] = hs.ic[3 * k + 1]; rgba[4 * k + 2] = hs.ic[3 * k + 2];
+            }
         }
-        if (upload_state(b.get(), i, rgba.data(), err)) return nullptr;
+        if (upload_state(b.get(), i, rgba.data(), err, lo.empty() ? nullptr : lo.data())) return nullptr;
     }
     return b.release();
 }

@@ -191,6 +191,41 @@ void initial_condition(const cel_params& p, const std::vector<float>* hot, HostS
             }
             s.ic[k] = w; s.ic[k + 1] = hu; s.ic[k + 2] = hv;
         }
+    // The same initial condition evaluated in double precision: the mixed form starts from it as
+    // a (high, low) pair of floats, so its first state is the double-precision one to ~1e-15.
+    const double swl64 = p.still_water_elevation, g64 = p.gravity, PI64 = 3.14159265358979323846;
+    const double dx64 = p.width / double(nx - 1), dy64 = p.length / double(ny - 1);
+    s.ic64.assign(size_t(NX) * NY * 3, 0.0);
+    for (int j = 0; j < NY; ++j)
+        for (int i = 0; i < NX; ++i) {
+            const int ii = std::max(2, std::min(nx + 1, i)), jj = std::max(2, std::min(ny + 1, j));
+            const double B = s.BA[size_t(jj) * NX + ii];
+            const double depth = std::max(0.0, swl64 - B);
+            const size_t k = (size_t(j) * NX + i) * 3;
+            double w, hu, hv;
+            if (hot) { w = (*hot)[k]; hu = (*hot)[k + 1]; hv = (*hot)[k + 2]; }
+            else { w = std::max(swl64, B); hu = 0; hv = 0; }
+            for (int q = 0; q < p.n_solitons; ++q) {
+                const cel_soliton& sw = p.solitons[q];
+                if (sw.H == 0 || depth == 0) continue;
+                const double th = sw.theta, x = dx64 * i, y = dy64 * j;
+                const double dist = std::fabs(std::sin(th) * (x - sw.xc)) + std::fabs(std::cos(th) * (y - sw.yc));
+                double Hq = sw.H;
+                if (dist > sw.length / 2) {
+                    const double smooth = PI64 / std::sqrt(0.75 * sw.H / (depth * depth * depth));
+                    Hq = (dist - sw.length / 2 < smooth) ? sw.H * (0.5 * std::cos(PI64 / smooth * (dist - sw.length / 2)) + 0.5)
+                                                         : 0.0;
+                }
+                const double K = std::sqrt(0.75 * std::fabs(Hq) / (depth * depth * depth));
+                const double C = std::sqrt(g64 * (Hq + depth));
+                const double ch = std::cosh(K * ((x - sw.xc) * std::cos(th) + (y - sw.yc) * std::sin(th)));
+                const double eta = Hq / (ch * ch);
+                w += eta;
+                hu += C * std::cos(th) * eta;
+                hv += C * std::sin(th) * eta;
+            }
+            s.ic64[k] = w; s.ic64[k + 1] = hu; s.ic64[k + 2] = hv;
+        }
 }
 
 int make_setup(const cel_params& p, const float* bathy, int bnx, int bny, HostSetup& s, std::string& err) {
