@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the per-domain plain FP32 comparison")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="0 skips the CPU baseline")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA graphs (profiling)")
+    ap.add_argument("--stencil-rows", type=int, default=0, choices=[0, 1, 2],
+                    help="force the stencil variant (1 or 2 rows per step) after tuning; 0 keeps the choice")
     ap.add_argument("--tune-steps", type=int, default=6, help="steps per autotuner candidate (0 keeps the defaults)")
     return ap.parse_args()
 
@@ -183,6 +185,8 @@ def main():
         # steps are warm-up too and lie outside the timed region
         batch.use_graph(not args.no_graph)
         tuned = batch.autotune(args.tune_steps) if args.tune_steps > 0 else None
+        if args.stencil_rows:
+            batch.set_stencil_rows(args.stencil_rows)
         batch.step(max(3, args.warmup))
     torch.cuda.synchronize()
 

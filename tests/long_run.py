@@ -8,7 +8,10 @@ separately and meet in .npz files:
   python tests/long_run.py compare ref.npz gpu.npz                        # prints one JSON line
 
 Cases: ``c3`` (1024^2 solitary wave on the truncated cone, solid walls), ``c3wm`` (the same
-basin with the sinusoidal wave-maker), ``c1`` (512x64 flume with the sine wave-maker).  Every
+basin with the sinusoidal wave-maker), ``c1`` (512x64 flume with the sine wave-maker), and
+``c4:<i>`` for member i of the 64-member C4 ensemble.  For ``c4:<i>`` the oracle runs member i
+alone, while ``gpu`` runs the whole ensemble as one batch (the production configuration, mixed
+form, graphs, autotuned) and keeps the members listed with ``--members``.  Every
 ``--every`` steps the FP64 total water volume (mass_full) is recorded.
 
 Reported per form: eta RMS over the interior (m), max |eta error| (m), max run-up of each side
@@ -40,7 +43,41 @@ def build_case(name: str, n: int | None):
         return cases.config3(n or 1024, n or 1024, wavemaker=True)
     if name == "c1":
         return cases.config1()
+    if name.startswith("c4:"):
+        return cases.config4()[int(name[3:])]
     raise KeyError(name)
+
+
+def run_gpu_ensemble(args):
+    """The 64-member C4 ensemble as one batch; records the members in --members."""
+    import celeris_b200 as cb
+    members = cases.config4()
+    keep = [int(k) for k in args.members.split(",")]
+    b = cb.Batch([(m[0], m[1]) for m in members], "mixed")
+    b.use_graph(True)
+    tuned = b.autotune(4)
+    # autotuning advanced the members: start over from the initial condition with the tuned setup
+    b2 = cb.Batch([(m[0], m[1]) for m in members], "mixed")
+    b2.set_tuning(tuned["band_width"], tuned["strip_height"])
+    b2.set_stencil_rows(b.stencil_rows)
+    b2.use_graph(True)
+    del b
+    masses = {k: [b2.stats_current()[k]["mass_full"]] for k in keep}
+    done, t0 = 0, time.time()
+    while done < args.steps:
+        k = min(args.every, args.steps - done)
+        b2.step(k)
+        done += k
+        st = b2.stats_current()
+        for i in keep:
+            masses[i].append(st[i]["mass_full"])
+    out = {}
+    for i in keep:
+        out[f"m{i}/eta"] = b2.state(i)[..., 0].astype(np.float32)
+        out[f"m{i}/maxdepth"] = b2.aux(i)[..., 0].astype(np.float32)
+        out[f"m{i}/mass"] = np.array(masses[i])
+    print(f"ensemble: {args.steps} steps in {time.time() - t0:.1f} s, tuning {tuned}", flush=True)
+    np.savez_compressed(args.out, every=args.every, **out)
 
 
 def run_oracle(args):
@@ -63,6 +100,8 @@ def run_oracle(args):
 
 
 def run_gpu(args):
+    if args.case == "c4":
+        return run_gpu_ensemble(args)
     import celeris_b200 as cb
     p, z, bnx, bny = build_case(args.case, args.n)
     out = {}
@@ -115,6 +154,8 @@ def compare(args):
     ru_ref = runup(B[I], initial_dry, ref["maxdepth"][I])
     res["fp64_runup_m"] = ru_ref
     forms = sorted({k.split("/")[0] for k in gpu.files if "/" in k})
+    if args.only:
+        forms = [f for f in forms if f == args.only]
     for f in forms:
         d = gpu[f"{f}/eta"].astype(np.float64)[I] - swl - eta_ref
         m = gpu[f"{f}/mass"]
@@ -144,9 +185,11 @@ def main():
         s.add_argument("--out", required=True)
         if name == "gpu":
             s.add_argument("--forms", default="mixed,fused,plain")
+            s.add_argument("--members", default="0,1,4,5,6", help="c4: ensemble members to record")
     c = sub.add_parser("compare")
     c.add_argument("ref")
     c.add_argument("gpu")
+    c.add_argument("--only", default=None, help="compare one record prefix (e.g. m5 for C4 member 5)")
     a = ap.parse_args()
     {"oracle": run_oracle, "gpu": run_gpu, "compare": compare}[a.cmd](a)
 
