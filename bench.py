@@ -66,6 +66,18 @@ def members_for(cfg: str, rank: int, count: int):
     return [cases.config3(4096, 4096)], "C3 4096^2 single domain, solitary wave on a truncated cone"
 
 
+def job_rate(ms: float, cells: int, steps: int, dist=None, device: str = "cuda"):
+    """Whole-job throughput: every rank's cells over the slowest rank's time (max over ranks)."""
+    import torch
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=device)
+    cells_t = torch.tensor([float(cells)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(cells_t, op=dist.ReduceOp.SUM)
+    ms_max, total = float(ms_t.item()), float(cells_t.item())
+    return total * steps / (ms_max / 1e3) / 1e9, ms_max, total
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -206,14 +218,7 @@ def main():
     clocks = clk.stop()
     ms = e0.elapsed_time(e1)
     barrier()
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    cells_t = torch.tensor([float(cells)], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(cells_t, op=dist.ReduceOp.SUM)
-    ms_max = float(ms_t.item())
-    total_cells = float(cells_t.item())
-    value = total_cells * args.steps / (ms_max / 1e3) / 1e9
+    value, ms_max, total_cells = job_rate(ms, cells, args.steps, dist)
 
     # ---- end to end through the C ABI: pinned dt upload + stats readback every step -------
     n = batch.n
