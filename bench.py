@@ -145,18 +145,26 @@ def reference_arm(args):
     if rank != 0:
         return
     members, workload = members_for(args.config, 0, args.members)
-    rate, cores, sample = cpu_sample(max(1.0, args.cpu_seconds), members)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     kind = "port"
-    # the reference's own shader code compiled for the CPU, when that build is present
-    try:
-        import ref_shader  # noqa: F401
-        if ref_shader.available():
-            p, z, bnx, bny = members[0]
-            r2, c2, s2 = ref_shader.time_sample(members, max(1.0, args.cpu_seconds))
-            rate, cores, sample, kind = r2, c2, s2, "reference"
-    except Exception:
-        pass
+    # the reference's own compute.hlsl compiled for the CPU (oracle/_ref, built from the reference
+    # sources), when that build is present: it runs single-threaded (its texture bindings are
+    # process-wide, as a D3D context's are)
+    if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_shader.so")):
+        import oracle as O
+        sizes = [p.nx * p.ny for p, *_ in members]
+        mean = sum(sizes) / len(sizes)
+        k = min(range(len(sizes)), key=lambda i: abs(sizes[i] - mean))
+        p, z, bnx, bny = members[k]
+        o = O.Oracle(p, z, bnx, bny, "ref")
+        o.physical_steps(1)
+        t = o.time_physical_steps(1)
+        n = max(1, int(max(1.0, args.cpu_seconds) / max(t, 1e-6)))
+        t = o.time_physical_steps(n)
+        rate, cores, kind = p.nx * p.ny * n / t, 1, "reference"
+        sample = f"{n} physical steps of one {p.nx}x{p.ny} member (the reference's compute.hlsl compiled for the CPU)"
+    else:   # the FP32 restatement with OpenMP
+        rate, cores, sample = cpu_sample(max(1.0, args.cpu_seconds), members)
     val = rate / 1e9
     out = {"metric": "Gcell-steps/s", "value": val, "unit": "Gcell-steps/s", "impl": "reference",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
