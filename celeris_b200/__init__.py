@@ -255,3 +255,32 @@ def byte_model(form: str | int, correction_steps: int):
     a, b = C.c_double(), C.c_double()
     check(lib().cel_byte_model(f, correction_steps, C.byref(a), C.byref(b)))
     return a.value, b.value
+
+
+# ---- file output in the reference's text formats (host side) ------------------------------------
+def _texels(params: Params, a: np.ndarray, comps: int) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if a.shape != (params.ny + 4, params.nx + 4, comps):
+        raise ValueError(f"expected a ({params.ny + 4}, {params.nx + 4}, {comps}) array, got {a.shape}")
+    return a
+
+
+def log_dump(params: Params, rgba: np.ndarray, total_time: float, elapsed: float = 0.0):
+    """Appends the time axis, ranges and gauges of ``params.log`` for one state."""
+    a = _texels(params, rgba, 4)
+    check(lib().cel_log_dump(C.byref(params), _fp(a), total_time, elapsed))
+
+
+def write_inundation(params: Params, aux: np.ndarray, path: str | None = None):
+    a = _texels(params, aux, 4)
+    check(lib().cel_write_inundation(C.byref(params), _fp(a), path.encode() if path else None))
+
+
+def write_bathymetry(params: Params, bottom: np.ndarray, path: str | None = None):
+    a = _texels(params, bottom, 3)
+    check(lib().cel_write_bathymetry(C.byref(params), _fp(a), path.encode() if path else None))
+
+
+def write_hotstart(params: Params, rgba: np.ndarray, path: str):
+    a = _texels(params, rgba, 4)
+    check(lib().cel_write_hotstart(C.byref(params), _fp(a), path.encode()))

@@ -11,6 +11,8 @@ import os
 
 CEL_MAX_WAVES = 1000
 CEL_MAX_SOLITONS = 100
+CEL_MAX_LOG_RANGES = 100
+CEL_MAX_GAUGES = 1000
 
 CEL_BC_SOLID, CEL_BC_SPONGE, CEL_BC_SINEWAVE, CEL_BC_IRREGULAR, CEL_BC_UTS = range(5)
 CEL_FORM_PLAIN, CEL_FORM_FUSED, CEL_FORM_MIXED = 0, 1, 2
@@ -40,6 +42,19 @@ class Soliton(C.Structure):
                 ("yc", C.c_double), ("length", C.c_double)]
 
 
+class LogRange(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("x0", C.c_int), ("y0", C.c_int), ("x1", C.c_int), ("y1", C.c_int)]
+
+
+class Log(C.Structure):
+    _fields_ = [
+        ("do_log", C.c_int), ("log_step", C.c_int),
+        ("path", C.c_char * 1024), ("time_axis_name", C.c_char * 256), ("gauges_name", C.c_char * 256),
+        ("n_ranges", C.c_int), ("ranges", LogRange * CEL_MAX_LOG_RANGES),
+        ("n_gauges", C.c_int), ("gauges", (C.c_int * 2) * CEL_MAX_GAUGES),
+    ]
+
+
 class Params(C.Structure):
     _fields_ = [
         ("nx", C.c_int), ("ny", C.c_int),
@@ -60,6 +75,7 @@ class Params(C.Structure):
         ("bathymetry_path", C.c_char * 1024),
         ("hotstart_path", C.c_char * 1024),
         ("project_name", C.c_char * 256),
+        ("log", Log),
     ]
 
 
@@ -95,6 +111,10 @@ def default_params() -> Params:
     for side in (p.west, p.east, p.south, p.north):
         side.type = CEL_BC_SOLID
         side.width = 2
+    p.log.log_step = 100
+    p.log.path = b"NA"
+    p.log.time_axis_name = b"time_axis"
+    p.log.gauges_name = b"gauges"
     return p
 
 
@@ -127,6 +147,11 @@ def _declare(L: C.CDLL) -> None:
         "cel_read_irregular_waves": (i, [C.c_char_p, C.POINTER(Boundary)]),
         "cel_read_uts": (i, [C.c_char_p, C.POINTER(Boundary)]),
         "cel_params_release": (None, [C.POINTER(Params)]),
+        "cel_params_size": (C.c_size_t, []),
+        "cel_log_dump": (i, [C.POINTER(Params), fp, C.c_float, C.c_float]),
+        "cel_write_inundation": (i, [C.POINTER(Params), fp, C.c_char_p]),
+        "cel_write_bathymetry": (i, [C.POINTER(Params), fp, C.c_char_p]),
+        "cel_write_hotstart": (i, [C.POINTER(Params), fp, C.c_char_p]),
         "cel_read_cbf": (i, [C.c_char_p, fp, C.c_size_t, C.POINTER(i), C.POINTER(i)]),
         "cel_create": (i, [C.POINTER(Params), fp, i, i, i, C.POINTER(vp)]),
         "cel_destroy": (i, [vp]),
@@ -190,7 +215,8 @@ def check(status: int) -> None:
 # Exported symbol list of include/celeris_b200.h (checked by the CPU test suite)
 EXPORTED = [
     "cel_last_error", "cel_version", "cel_params_default", "cel_params_from_cml",
-    "cel_read_irregular_waves", "cel_read_uts", "cel_params_release", "cel_read_cbf",
+    "cel_read_irregular_waves", "cel_read_uts", "cel_params_release", "cel_params_size", "cel_read_cbf",
+    "cel_log_dump", "cel_write_inundation", "cel_write_bathymetry", "cel_write_hotstart",
     "cel_create", "cel_destroy", "cel_remesh", "cel_set_stream", "cel_get_dims",
     "cel_set_state", "cel_get_state", "cel_get_bottom", "cel_get_aux",
     "cel_reset_timestep", "cel_timestep", "cel_timesteps", "cel_physical_steps", "cel_get_stats",

@@ -24,6 +24,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("params.cpp", []),
     ("setup.cpp", []),
+    ("logio.cpp", []),
     ("capi.cpp", []),
     ("plain.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("fused.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),

@@ -148,6 +148,48 @@ void cel_params_release(cel_params* p) {
     if (p) cel::params_release(p);
 }
 
+size_t cel_params_size(void) { return sizeof(cel_params); }
+
+int cel_log_dump(const cel_params* p, const float* rgba, float total_time, float elapsed) {
+    if (!p || !rgba) { set_error("null argument"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN
+    std::string err;
+    const int st = cel::log_dump(p->log, rgba, p->nx, p->ny, total_time, elapsed, err);
+    if (st) set_error(err);
+    return st;
+    CEL_GUARD_END
+}
+
+int cel_write_inundation(const cel_params* p, const float* aux_rgba, const char* path) {
+    if (!p || !aux_rgba) { set_error("null argument"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN
+    std::string err;
+    const int st = cel::write_inundation(p->log, aux_rgba, p->nx, p->ny, path, err);
+    if (st) set_error(err);
+    return st;
+    CEL_GUARD_END
+}
+
+int cel_write_bathymetry(const cel_params* p, const float* bottom_b3, const char* path) {
+    if (!p || !bottom_b3) { set_error("null argument"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN
+    std::string err;
+    const int st = cel::write_bathymetry(p->log, bottom_b3, p->nx, p->ny, path, err);
+    if (st) set_error(err);
+    return st;
+    CEL_GUARD_END
+}
+
+int cel_write_hotstart(const cel_params* p, const float* rgba, const char* path) {
+    if (!p || !rgba || !path) { set_error("null argument"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN
+    std::string err;
+    const int st = cel::write_hotstart(rgba, p->nx, p->ny, path, err);
+    if (st) set_error(err);
+    return st;
+    CEL_GUARD_END
+}
+
 int cel_read_cbf(const char* path, float* z, size_t capacity, int* bnx, int* bny) {
     if (!path || !bnx || !bny) { set_error("null argument"); return CEL_ERR_ARG; }
     CEL_GUARD_BEGIN
@@ -221,6 +263,7 @@ int cel_get_aux(cel_engine* h, float* rgba) {
 }
 int cel_reset_timestep(cel_engine* h, float rdt, float el, cel_stats* out) {
     ENG(h);
+    e->log_elapsed = el;
     CEL_GUARD_BEGIN return ret(e, e->reset_timestep(rdt, el, out)); CEL_GUARD_END
 }
 int cel_timestep(cel_engine* h) { ENG(h); CEL_GUARD_BEGIN return ret(e, e->timestep()); CEL_GUARD_END }

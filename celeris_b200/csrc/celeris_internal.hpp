@@ -19,6 +19,13 @@ int read_uts(const std::string& path, cel_boundary* b, std::string& err);
 int read_cbf(const std::string& path, std::vector<float>* z, int& bnx, int& bny, std::string& err);
 int read_hotstart(const std::string& path, int nx, int ny, std::vector<float>& whuhv, std::string& err);
 
+// ---- file output (logio.cpp) ------------------------------------------------------------------
+int log_validate(const cel_log& lg, int nx, int ny, std::string& err);
+int log_dump(const cel_log& lg, const float* rgba, int nx, int ny, float total_time, float elapsed, std::string& err);
+int write_inundation(const cel_log& lg, const float* aux, int nx, int ny, const char* path, std::string& err);
+int write_bathymetry(const cel_log& lg, const float* b3, int nx, int ny, const char* path, std::string& err);
+int write_hotstart(const float* rgba, int nx, int ny, const char* path, std::string& err);
+
 // ---- host setup (setup.cpp): the once-per-remesh host work of the reference ----------------
 struct Float4 { float x, y, z, w; };
 

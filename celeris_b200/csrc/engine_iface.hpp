@@ -54,6 +54,7 @@ public:
     virtual int nx() const = 0;
     virtual int ny() const = 0;
     std::string err;
+    float log_elapsed = 0.f;   // `elapsed` of the latest cel_reset_timestep (the log's elapsed time)
 };
 
 EngineIface* make_plain_engine(const cel_params& p, const float* bathy, int bnx, int bny, std::string& err);

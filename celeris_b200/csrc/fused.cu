@@ -25,6 +25,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -1897,6 +1898,9 @@ struct cel_batch {
     int mh = cel::MH_DEFAULT;           // stencil strip height (rows per CTA work item)
     int rows_per_step = 1;              // stencil rows per thread step: 1 (k_march) or 2 (k_march2)
     int max_nx = 0, max_ny = 0;
+    bool any_log = false;               // some member has <logData> doLog set
+    const float* elapsed_src = nullptr; // engine handles: the elapsed time of their latest resetTimestep
+    std::chrono::steady_clock::time_point created = std::chrono::steady_clock::now();
 };
 
 namespace cel {
@@ -2041,6 +2045,29 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     return CEL_OK;
 }
 
+// <logData> output after a physical step (engine.cpp:1488-1493): each member whose step count is a
+// multiple of its logStep writes the state after the step with the time at the step's start, here
+// the member's FP64 clock minus the step's dt, rounded to float.
+int log_after_step(cel_batch* b, std::string& err) {
+    if (!b->any_log) return CEL_OK;
+    const int count = b->sch.last_count;
+    for (size_t i = 0; i < b->mem.size(); ++i) {
+        const Member& m = b->mem[i];
+        const cel_log& lg = m.p.log;
+        if (!lg.do_log || count % lg.log_step != 0) continue;
+        std::vector<float> host(size_t(m.hs.NX) * m.hs.NY * 4);
+        if (int e = batch_get_state(b, int(i), host.data(), err)) return e;
+        double t_end = 0;
+        B_TRY(cudaMemcpyAsync(&t_end, b->hdev[i].time64, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+        B_TRY(cudaStreamSynchronize(b->stream));
+        const float t0 = float(t_end - double(b->step_dt[i]));
+        const float elapsed = b->elapsed_src ? *b->elapsed_src
+                                             : std::chrono::duration<float>(std::chrono::steady_clock::now() - b->created).count();
+        if (int e = log_dump(lg, host.data(), m.hs.nx, m.hs.ny, t0, elapsed, err)) return e;
+    }
+    return CEL_OK;
+}
+
 // One pass with the host state machine; updates the buffer indices.
 int run_pass(cel_batch* b, bool first_of_step, std::string& err) {
     Scheme& s = b->sch;
@@ -2079,6 +2106,7 @@ int run_pass(cel_batch* b, bool first_of_step, std::string& err) {
         std::swap(ix.scr, ix.spare);
     }
     ix.sin = pa.out;
+    if (book) return log_after_step(b, err);
     return CEL_OK;
 }
 
@@ -2218,6 +2246,11 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         if (params[i]->adaptive) { err = "batches run fixed time steps (adaptive members are not supported)"; return nullptr; }
         if (params[i]->ny > 6900) { err = "fused form supports ny <= 6900 (column band in shared memory)"; return nullptr; }
         if (params[i]->nx > 16000) { err = "fused form supports nx <= 16000 (row in shared memory)"; return nullptr; }
+        if (log_validate(params[i]->log, params[i]->nx, params[i]->ny, err)) {
+            err = "member " + std::to_string(i) + ": " + err;
+            return nullptr;
+        }
+        if (params[i]->log.do_log) b->any_log = true;
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { err = "no CUDA device"; return nullptr; }
@@ -2507,6 +2540,7 @@ int batch_step(cel_batch* b, int nsteps, std::string& err) {
             b->graph_pos = (b->graph_pos + 1) % int(b->graphs.size());
             b->step_stats_valid = true;
             b->step_dt.assign(b->dt_host, b->dt_host + b->mem.size());
+            if (int e = log_after_step(b, err)) return e;
         } else {
             if (int e = run_physical_step(b, err)) return e;
         }
@@ -2711,6 +2745,7 @@ public:
             bz = tmp.data();
         }
         b = batch_create(1, &pp, &bz, &bnx, &bny, form, err);
+        if (b) b->elapsed_src = &log_elapsed;
         return b ? CEL_OK : CEL_ERR_ARG;
     }
     int remesh() override {

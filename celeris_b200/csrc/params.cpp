@@ -226,6 +226,11 @@ void params_default(cel_params* p) {
         b->type = CEL_BC_SOLID;
         b->width = 2;
     }
+    // logging defaults (settings.hpp:389, 423-433)
+    p->log.log_step = 100;
+    copy_str(p->log.path, sizeof(p->log.path), "NA");
+    copy_str(p->log.time_axis_name, sizeof(p->log.time_axis_name), "time_axis");
+    copy_str(p->log.gauges_name, sizeof(p->log.gauges_name), "gauges");
 }
 
 int read_irregular(const std::string& path, cel_boundary* b, std::string& err) {
@@ -268,6 +273,58 @@ int read_uts(const std::string& path, cel_boundary* b, std::string& err) {
     b->uts = static_cast<double*>(std::malloc(rows.size() * sizeof(double)));
     std::memcpy(b->uts, rows.data(), rows.size() * sizeof(double));
     b->n_uts = int(rows.size() / 4);
+    return CEL_OK;
+}
+
+// <logData doLog logStep> with <logPath>, <timeAxis filename>, <range filename> (bottomLeft /
+// topRight x, y) and <gauges filename>x,y,x,y,...</gauges> children (main.cpp:825-887).
+static int read_log_data(const XNode& e, const std::string& cml, cel_log& lg, std::string& err) {
+    bool on = false;
+    if (to_b(e, "doLog", on)) lg.do_log = on ? 1 : 0;
+    to_i(e, "logStep", lg.log_step);
+    for (const XNode& k : e.kids) {
+        std::string fname;
+        if (k.name == "logPath") {
+            // relative paths are taken from the .cml folder; an empty one means that folder
+            const std::string t = trim(k.text);
+            copy_str(lg.path, sizeof(lg.path), t.empty() ? dir_of(cml) : resolve(cml, t));
+        } else if (k.name == "timeAxis") {
+            k.attr("filename", fname);
+            copy_str(lg.time_axis_name, sizeof(lg.time_axis_name), fname);
+        } else if (k.name == "range") {
+            if (lg.n_ranges >= CEL_MAX_LOG_RANGES) { err = "more than 100 log ranges"; return CEL_ERR_IO; }
+            const XNode* bl = k.child("bottomLeft");
+            const XNode* tr = k.child("topRight");
+            if (!bl || !tr) { err = "log range without bottomLeft/topRight"; return CEL_ERR_IO; }
+            cel_log_range& R = lg.ranges[lg.n_ranges++];
+            k.attr("filename", fname);
+            copy_str(R.name, sizeof(R.name), fname);
+            to_i(*bl, "x", R.x0);
+            to_i(*bl, "y", R.y0);
+            to_i(*tr, "x", R.x1);
+            to_i(*tr, "y", R.y1);
+        } else if (k.name == "gauges") {
+            k.attr("filename", fname);
+            copy_str(lg.gauges_name, sizeof(lg.gauges_name), fname);
+            // Pairs are read as `>> x >> sep >> y >> sep` until the stream fails, and the pair of
+            // the failing round is kept too (main.cpp:866-876): "1,2,3,4" gives two gauges and a
+            // trailing comma repeats the last one.  A text without any number gives none.
+            std::istringstream in(k.text);
+            int x = 0, y = 0, rounds = 0;
+            char sep = 0;
+            while (in) {
+                in >> x;
+                const bool got_x = bool(in);
+                in >> sep >> y >> sep;
+                if (!got_x && rounds == 0) break;
+                if (lg.n_gauges >= CEL_MAX_GAUGES) { err = "more than 1000 gauges"; return CEL_ERR_IO; }
+                lg.gauges[lg.n_gauges][0] = x;
+                lg.gauges[lg.n_gauges][1] = y;
+                lg.n_gauges++;
+                ++rounds;
+            }
+        }
+    }
     return CEL_OK;
 }
 
@@ -357,6 +414,8 @@ int params_from_cml(const char* path, cel_params* out, std::string& err) {
                 const int st = ty == CEL_BC_IRREGULAR ? read_irregular(f, b, err) : read_uts(f, b, err);
                 if (st != CEL_OK) return st;
             }
+        } else if (n == "logData") {
+            if (int st = read_log_data(e, cml, out->log, err)) return st;
         } else if (n == "graphics") {
             if (const XNode* ss2 = e.child("surfaceShading"))
                 if (const XNode* di = ss2->child("dissipationIntensity")) {

@@ -543,6 +543,7 @@ public:
         p = prm;
         for (cel_boundary* b : {&p.west, &p.east, &p.south, &p.north})
             if (b->type != CEL_BC_UTS) { b->uts = nullptr; b->n_uts = 0; }
+        if (int st = log_validate(p.log, p.nx, p.ny, err)) return st;
         int st0 = make_setup(p, bathy, bnx, bny, hs, err);
         if (st0) return st0;
         int dev = 0;
@@ -826,11 +827,18 @@ public:
             k_pass1<<<grid2(hs.nx + 2, hs.ny + 2), blk, 0, stream>>>(new_state, BOT, AUX1, H, U, V, AUX2, c);
         }
         CEL_CUDA_TRY(cudaGetLastError());
-        if (sch.after_pass()) {
+        const bool book = sch.after_pass();
+        if (book) {
             const int o = old_i, oo = oldold_i, s = scratch_i;
             old_i = s; oldold_i = o; scratch_i = oo;
         }
         sim_idx = 1 - sim_idx;
+        if (book && p.log.do_log && sch.last_count % p.log.log_step == 0) {
+            // st_DumpToFile of the new state, with the time at the start of the step (engine.cpp:1488-1493)
+            std::vector<float> host(ntex * 4);
+            if (int e = get_state(host.data())) return e;
+            if (int e = log_dump(p.log, host.data(), hs.nx, hs.ny, sch.last_start_time, log_elapsed, err)) return e;
+        }
         return CEL_OK;
     }
 

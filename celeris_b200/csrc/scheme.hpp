@@ -19,6 +19,8 @@ struct Scheme {
     int correction_steps_count = 0;
     float dt = 0, dt_old = 0, dt_old_old = 0;
     float total_time = 0;        // float, as the reference (engine.hpp:302)
+    int last_count = 0;          // timestep_count tested by the reference's log dump (engine.cpp:1491)
+    float last_start_time = 0;   // total_time before the latest step's dt was added
     double total_time_d = 0;     // FP64 copy (the mixed form's wave-maker phase)
     bool initialized = false, target_cfl_set = false;
     float target_cfl = 0;
@@ -33,6 +35,8 @@ struct Scheme {
         dt = dt_old = dt_old_old = 0;
         total_time = 0;
         total_time_d = 0;
+        last_count = 0;
+        last_start_time = 0;
         initialized = false;
         target_cfl_set = false;
         target_cfl = 0;
@@ -74,6 +78,8 @@ struct Scheme {
             }
         }
         if (time_scheme != CEL_SCHEME_CORRECTOR) {
+            last_count = timestep_count;
+            last_start_time = total_time;
             timestep_count++;
             dt_old_old = dt_old;
             dt_old = dt;

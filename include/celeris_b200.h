@@ -73,6 +73,30 @@ typedef struct cel_soliton {
     double H, theta, xc, yc, length; /* theta in radians; length 1e30 = infinite crest */
 } cel_soliton;
 
+/* Run-time logging of the `.cml` <logData> element (main.cpp:825-887; InitSetting fields and
+ * defaults settings.hpp:322, 359-372, 389, 423-433).  Indices are texel indices of the
+ * (nx+4) x (ny+4) layout, ghost cells included, as the reference's staging-texture reads use them. */
+#define CEL_MAX_LOG_RANGES 100  /* InitSetting::MAX_NUM_RANGE (settings.hpp:362) */
+#define CEL_MAX_GAUGES 1000     /* InitSetting::MAX_NUM_GAUGE (settings.hpp:368) */
+
+typedef struct cel_log_range {
+    char name[256];           /* range `filename`: rows go to <path>/<name>.txt */
+    int x0, y0;               /* bottomLeft x, y */
+    int x1, y1;               /* topRight x, y (inclusive) */
+} cel_log_range;
+
+typedef struct cel_log {
+    int do_log;               /* logData doLog (default 0) */
+    int log_step;             /* logData logStep: log after every log_step-th physical step (default 100) */
+    char path[1024];          /* logPath, resolved against the .cml folder (default "NA") */
+    char time_axis_name[256]; /* timeAxis filename (default "time_axis") */
+    char gauges_name[256];    /* gauges filename (default "gauges") */
+    int n_ranges;
+    cel_log_range ranges[CEL_MAX_LOG_RANGES];
+    int n_gauges;
+    int gauges[CEL_MAX_GAUGES][2];  /* {x, y} per gauge */
+} cel_log;
+
 typedef struct cel_params {
     int nx, ny;                       /* gridSize */
     double width, length;             /* fieldDimensions (x, y extent in m) */
@@ -95,6 +119,7 @@ typedef struct cel_params {
     char bathymetry_path[1024];       /* bathymetryFilePath, resolved against the .cml folder */
     char hotstart_path[1024];         /* hotStartFilePath, resolved; "" if none */
     char project_name[256];
+    cel_log log;                      /* logData */
 } cel_params;
 
 /* resetTimestep() outputs (engine.cpp:1685-1746), reduced on the device in FP64. */
@@ -130,6 +155,8 @@ int cel_read_irregular_waves(const char* path, cel_boundary* b);
 /* Reads a UniformTimeSeries file into a boundary (engine.cpp:3863-3874) */
 int cel_read_uts(const char* path, cel_boundary* b);
 void cel_params_release(cel_params* p);
+/* sizeof(cel_params), for bindings that mirror the struct */
+size_t cel_params_size(void);
 
 /* Reads a .cbf bathymetry grid (terrain_heightfield.cpp:136-209).  If z is NULL, only the
  * header size is returned. */
@@ -218,6 +245,36 @@ int cel_kernel_times(void* handle, int is_batch, char (*names)[64], double* tota
  * physical step (the roofline byte model recorded in code). */
 int cel_byte_model(int form, int correction_steps, double* stencil_bytes_per_cell_pass,
                    double* step_bytes_per_cell);
+
+/* ---- logging and file output (host side; no device needed) ------------------------------ */
+/* Engines and batch members whose params have log.do_log set log by themselves, as the reference's
+ * timestep() does (engine.cpp:1488-1493): after physical step s with s % log_step == 0 the state
+ * after that step is written as below, with the simulated time at the start of that step (the
+ * reference writes total_time before adding the step's dt, engine.cpp:1491-1518).  The elapsed
+ * time is the `elapsed` argument of the engine's latest cel_reset_timestep call (0 before one; the
+ * reference writes its "elapsed time" setting, which resetTimestep sets, engine.cpp:1746); batch
+ * members write the wall-clock seconds since the batch was created.  A failed write makes the
+ * stepping call return CEL_ERR_IO after the step has completed.  Creation fails with CEL_ERR_ARG
+ * if a gauge or a non-empty range lies outside the texture, or log_step < 1 with do_log set. */
+
+/* st_DumpToFile (engine.cpp:628-675) for a host state rgba ((nx+4)(ny+4) x {w,hu,hv,a}):
+ * appends total_time to <path>/<time_axis_name>.txt and elapsed to <path>/<time_axis_name>-elapsed.txt,
+ * then "i\tj\tw\thu\thv\ta\n" for each texel of each range (j outer, i inner) to <path>/<name>.txt
+ * and for each gauge to <path>/<gauges_name>.txt; numbers in the default stream format (6
+ * significant digits). */
+int cel_log_dump(const cel_params* p, const float* rgba, float total_time, float elapsed);
+/* dumpInundationToFile (engine.cpp:781-817): the maximum-inundation-depth map from an aux array
+ * (cel_get_aux layout, component 0) with the reference's "[nx]/[ny]" header; rows j = 2..ny+1,
+ * columns i = 2..nx+2 (one ghost column included, as the reference writes it).  path NULL =
+ * <log path>/<Y-M-D H-M-S>-inundation.txt in local time, as the reference names it. */
+int cel_write_inundation(const cel_params* p, const float* aux_rgba, const char* path);
+/* dumpBathymetryToFile (engine.cpp:750-779): the interior cell bottom (BA of a cel_get_bottom
+ * array) as a .cbf text grid.  path NULL = <log path>/<Y-M-D H-M-S>.cbf. */
+int cel_write_bathymetry(const cel_params* p, const float* bottom_b3, const char* path);
+/* A hot-start file for hotStartFilePath (read by engine.cpp:2943-2966): "i j w hu hv a" per texel
+ * over all (nx+4)(ny+4) texels, j outer, with 9 significant digits so that the state reads back
+ * bit for bit (the reference's range dump writes the same columns with 6). */
+int cel_write_hotstart(const cel_params* p, const float* rgba, const char* path);
 
 /* ---- allocation-free statistics (no counterpart in the reference) ----------------------- */
 /* The resetTimestep statistics (mass, energies, momenta, maxima, CFL rate) of a state the caller

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def header_symbols():
     txt = open(os.path.join(ROOT, "include", "celeris_b200.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:const char\*|int|void|long long)\s+(cel_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const char\*|int|void|long long|size_t)\s+(cel_\w+)\s*\(", txt, re.M)))
 
 
 def test_header_symbol_list_matches_binding():
