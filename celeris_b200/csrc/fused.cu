@@ -57,6 +57,7 @@ struct MemberDev {
     const CUtensorMap* tmaps;  // 2D row maps: state [buffer*3 + field], then BA, BX, BY
     float tan_thr;          // tan(dissipation threshold): atan(x) > thr  <=>  x > tan(thr)
     const float* dtp;       // this member's time step (device table, host-updatable)
+    const float* ab;        // adaptive AB3 predictor: {k, A0, A1, A2, K0, K1, K2} (see k_choose_dt)
     float* S[3][3];         // state buffers [buffer][w, hu, hv]
     float* L[3][3];         // compensation words (mixed form)
     const float* BY;
@@ -330,7 +331,7 @@ __device__ __forceinline__ void face_flux(float hm, float um, float vm, float hp
 //   H[s], s = 0..3: HA = float4 {dw/dt, dhu/dt, dhv/dt, F*} (4 planes) and HB = G* (1 plane) |
 //   AUX = float2 {max inundated depth, breaking} (2 planes) | FX (3) | FY (3)
 // ---------------------------------------------------------------------------------------------
-template <bool MIXED>
+template <bool MIXED, bool ADAPT>
 __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
                                                  int ntiles, PassArgs pa) {
     __shared__ __align__(128) float ring[6 * FSTR];
@@ -556,6 +557,13 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
                 float wbase = wc;
                 if (euler) {
                     dw = dt * f0; rhu = dt * f1; rhv = dt * f2;
+                } else if (!corr && ADAPT) {
+                    // variable-step AB3 (compute.hlsl:766-780) with the member's coefficients
+                    const float* q = M.ab;
+                    const float kA = q[0], A0 = q[1], A1 = q[2], A2 = q[3], K0 = q[4], K1 = q[5], K2 = q[6];
+                    dw = kA * (A0 * f0 + A1 * ho.x + A2 * hoo.x);
+                    rhu = kA * (A0 * f1 + A1 * ho.y + A2 * hoo.y) + (K0 * Fs + K1 * ho.w + K2 * hoo.w);
+                    rhv = kA * (A0 * f2 + A1 * ho.z + A2 * hoo.z) + (K0 * Gs + K1 * go + K2 * goo);
                 } else if (!corr) {
                     const float k12 = dt * (1.0f / 12.0f);
                     dw = k12 * (23.0f * f0 - 16.0f * ho.x + 5.0f * hoo.x);
@@ -796,7 +804,7 @@ struct Kahan2 {
     __device__ __forceinline__ double value() const { return (double(s.x) - double(c.x)) + (double(s.y) - double(c.y)); }
 };
 
-template <bool MIXED>
+template <bool MIXED, bool ADAPT>
 __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev* __restrict__ mems,
                                                                const int4* __restrict__ tiles, int ntiles, PassArgs pa) {
     extern __shared__ __align__(128) float ring[];   // 6 * FSTR2 floats (dynamic: the total passes 48 KB)
@@ -1083,6 +1091,16 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
                 f2 wbase = wc;
                 if (euler) {
                     dw = mul2(dt, f0); rhu = mul2(dt, f1); rhv = mul2(dt, f2v);
+                } else if (!corr && ADAPT) {
+                    // variable-step AB3 (compute.hlsl:766-780) with the member's coefficients
+                    const float* q = M.ab;
+                    const f2 kA = S2(q[0]), A0 = S2(q[1]), A1 = S2(q[2]), A2 = S2(q[3]);
+                    const f2 K0 = S2(q[4]), K1 = S2(q[5]), K2 = S2(q[6]);
+                    const f2 o_x = P2(ho0.x, ho1.x), o_y = P2(ho0.y, ho1.y), o_z = P2(ho0.z, ho1.z), o_w = P2(ho0.w, ho1.w);
+                    const f2 q_x = P2(hoo0.x, hoo1.x), q_y = P2(hoo0.y, hoo1.y), q_z = P2(hoo0.z, hoo1.z), q_w = P2(hoo0.w, hoo1.w);
+                    dw = mul2(kA, fma2(A2, q_x, fma2(A1, o_x, mul2(A0, f0))));
+                    rhu = fma2(kA, fma2(A2, q_y, fma2(A1, o_y, mul2(A0, f1))), fma2(K2, q_w, fma2(K1, o_w, mul2(K0, Fs))));
+                    rhv = fma2(kA, fma2(A2, q_z, fma2(A1, o_z, mul2(A0, f2v))), fma2(K2, goo, fma2(K1, go, mul2(K0, Gs))));
                 } else if (!corr) {
                     const f2 k12 = S2(dtm * (1.0f / 12.0f));
                     const f2 o_x = P2(ho0.x, ho1.x), o_y = P2(ho0.y, ho1.y), o_z = P2(ho0.z, ho1.z), o_w = P2(ho0.w, ho1.w);
@@ -1823,12 +1841,112 @@ __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ 
     }
 }
 
-__global__ void k_advance_time(const MemberDev* __restrict__ mems, int n) {
+// Per-member time-step controller of an adaptive batch: resetTimestep's dt logic
+// (engine.cpp:1698-1726) kept on the device, so a physical step needs no host readback and can
+// be replayed from a CUDA graph.  Single precision with IEEE-rounded operations, as the reference's
+// float arithmetic.
+struct DtCtl {
+    float dt, dt_old, dt_old_old;   // this pass, and the two previous steps (engine.hpp:300-301)
+    float target_cfl;               // "target cfl": timestep x the first positive CFL rate
+    int target_set, initialized;
+    float base, min_ratio, alpha;   // timestep, min_timestep_ratio, exponentialMovingAverageAlpha
+    float dt_first;                 // dt of the first pass of the most recent step
+    float ab[7];                    // variable-step AB3 coefficients of the latest adaptive predictor
+};
+
+// std::max(a, b): a unless a < b (NaN in a stays)
+__device__ __forceinline__ float std_max(float a, float b) { return (a < b) ? b : a; }
+
+// AdamsBashforthCoef and the three second-order derivative stencils (compute.hlsl:560-605),
+// folded into one coefficient per history level: the predictor computes
+//   w  += k (A0 f + A1 f_old + A2 f_oldold)
+//   hu  = (A hu_W + B hu + C hu_E) + k (A0 f + ...) + (K0 F* + K1 F*_old + K2 F*_oldold)
+// where K_j = k * sum_m coef_m * D_m,j and D_m,j is the weight of level j in derivative m
+// (backward at t_n, central at t_n-1, forward at t_n-2).  With equal steps this gives
+// k = dt/6, A = (11.5, -8, 2.5) and K = (2, -3, 1): the fixed-step AB3 of the predictor.
+__device__ void ab3_coefficients(float dt, float d1, float d2, float* ab) {
+    const float r = __fdiv_rn(dt, d1);
+    const float s12 = __fadd_rn(d1, d2);
+    const float c0 = __fadd_rn(__fmul_rn(r, __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(2.f, dt), __fmul_rn(6.f, d1)), __fmul_rn(3.f, d2)), s12)), 6.f);
+    const float c1 = -__fmul_rn(r, __fdiv_rn(__fadd_rn(__fadd_rn(__fmul_rn(2.f, dt), __fmul_rn(3.f, d1)), __fmul_rn(3.f, d2)), d2));
+    const float c2 = __fmul_rn(__fdiv_rn(dt, d2), __fdiv_rn(__fadd_rn(__fmul_rn(2.f, dt), __fmul_rn(3.f, d1)), s12));
+    const float p1 = __fmul_rn(d1, s12), p2 = __fmul_rn(d2, s12), p12 = __fmul_rn(d1, d2);
+    // rows: backward, central, forward; columns: levels n, n-1, n-2
+    const float D[3][3] = {
+        {__fdiv_rn(__fadd_rn(__fmul_rn(2.f, d1), d2), p1), -__fdiv_rn(s12, p12), __fdiv_rn(d1, p2)},
+        {__fdiv_rn(d2, p1), __fdiv_rn(__fsub_rn(d1, d2), p12), -__fdiv_rn(d1, p2)},
+        {-__fdiv_rn(d2, p1), __fdiv_rn(s12, p12), -__fdiv_rn(__fadd_rn(d1, __fmul_rn(2.f, d2)), p2)}};
+    const float k = __fdiv_rn(dt, 6.f);
+    ab[0] = k; ab[1] = c0; ab[2] = c1; ab[3] = c2;
+    for (int j = 0; j < 3; ++j)
+        ab[4 + j] = __fmul_rn(k, __fadd_rn(__fadd_rn(__fmul_rn(c0, D[0][j]), __fmul_rn(c1, D[1][j])), __fmul_rn(c2, D[2][j])));
+}
+
+// Max CFL rate max((|u| + c)/dx, (|v| + c)/dy) of each member's current state over the cells of
+// its 4x4 blocks (the GetStats region, compute.hlsl:1319-1378), as non-negative float bits.
+__global__ void __launch_bounds__(256) k_cfl(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
+                                             int ntiles, int buf, unsigned int* __restrict__ out) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int4 tl = tiles[t];
+        const MemberDev& M = mems[tl.x];
+        const SimConsts& c = M.c;
+        float m = 0.f;
+        for (int k = threadIdx.x; k < TX * TY; k += 256) {
+            const int gx = tl.y + k % TX, gy = tl.z + k / TX;
+            if (gx < 2 + 4 * (c.nx / 4) && gy < 2 + 4 * (c.ny / 4)) {
+                const size_t gi = size_t(gy) * M.P + gx;
+                const float h = fmaxf(0.f, M.S[buf][0][gi] - M.BA[gi]);
+                const float q = div_by_h_fast(h, c.epsilon);
+                const float cc = sqrtf(c.g * h);
+                m = fmaxf(m, fmaxf((fabsf(q * M.S[buf][1][gi]) + cc) * c.one_over_dx,
+                                   (fabsf(q * M.S[buf][2][gi]) + cc) * c.one_over_dy));
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out + tl.x, __float_as_uint(m));
+    }
+}
+
+// resetTimestep's dt choice for every member before a pass (engine.cpp:1698-1726): the target
+// CFL is set from the first positive CFL rate seen; adaptive predictors take
+// max(target / cfl, timestep * min ratio), smoothed by the moving average when it grows; every
+// other pass runs with the uniform time step.  cfl may be null (no reduction before this pass).
+__global__ void k_choose_dt(DtCtl* __restrict__ ctl, float* __restrict__ dt_table, const unsigned int* __restrict__ cfl,
+                            int n, int scheme, int first_of_step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    DtCtl& C = ctl[i];
+    float rate = cfl ? __uint_as_float(cfl[i]) : 0.f;
+    if (rate > 0.f && !C.target_set) { C.target_cfl = __fmul_rn(C.base, rate); C.target_set = 1; }
+    if (!C.initialized) {
+        C.dt = C.base;
+        C.dt_old_old = C.dt;
+        C.dt_old = C.dt;
+        C.initialized = 1;
+    }
+    if (scheme == CEL_SCHEME_PREDICTOR_ADAPTIVE) {
+        const float tgt = std_max(__fdiv_rn(C.target_cfl, rate), __fmul_rn(C.base, C.min_ratio));
+        C.dt = tgt > C.dt_old ? __fadd_rn(__fmul_rn(C.alpha, tgt), __fmul_rn(__fsub_rn(1.f, C.alpha), C.dt_old)) : tgt;
+        ab3_coefficients(C.dt, C.dt_old, C.dt_old_old, C.ab);
+    } else {
+        C.dt = C.base;
+    }
+    if (first_of_step) C.dt_first = C.dt;
+    dt_table[i] = C.dt;
+}
+
+// End of a physical step: advance the clocks by the dt of the step's last pass and, in adaptive
+// batches, shift the controller's dt queue (engine.cpp:1507-1518).
+__global__ void k_advance_time(const MemberDev* __restrict__ mems, DtCtl* __restrict__ ctl, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const MemberDev& M = mems[i];
     *M.time64 += double(*M.dtp);
     *M.time32 += *M.dtp;
+    if (ctl) {
+        ctl[i].dt_old_old = ctl[i].dt_old;
+        ctl[i].dt_old = ctl[i].dt;
+    }
 }
 
 // Final Pass1 aux update of the current state (txAuxiliary2 -> reported txAuxiliary1 values are
@@ -1885,6 +2003,10 @@ struct cel_batch {
     bool any_friction = false;
     float* dt_table = nullptr;         // per-member time step on the device
     float* dt_host = nullptr;          // pinned mirror of dt_table
+    bool adaptive = false;              // adaptive time steps: dt chosen per member on the device
+    cel::DtCtl* ctl = nullptr;          // per-member dt controllers (adaptive batches)
+    unsigned int* cfl_now = nullptr;    // per-member max CFL rate of the current state (float bits)
+    bool dt_started = false;            // the controllers have made their first choice
     size_t smem_rows = 0, smem_cols = 0;
     int rowbuf = 0, rows_threads = 256;   // row solver: floats of forward values per warp, threads per CTA
     int grid_stencil = 0, grid_rows = 0, grid_cols = 0;
@@ -1991,12 +2113,15 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     if (pa.stats) B_TRY(cudaMemsetAsync(b->stats_all, 0, nm * STATS_N * sizeof(double), b->stream));
     {
         TimedLaunch t(&b->tm, b->stream, "fused_stencil");
+        const bool ad = pa.scheme == CEL_SCHEME_PREDICTOR_ADAPTIVE;
         if (b->rows_per_step == 2) {
-            if (b->mixed) k_march2<true><<<b->grid_stencil, MW, MARCH2_DYN_SMEM, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
-            else k_march2<false><<<b->grid_stencil, MW, MARCH2_DYN_SMEM, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
+            auto* k = b->mixed ? (ad ? k_march2<true, true> : k_march2<true, false>)
+                               : (ad ? k_march2<false, true> : k_march2<false, false>);
+            k<<<b->grid_stencil, MW, MARCH2_DYN_SMEM, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
         } else {
-            if (b->mixed) k_march<true><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
-            else k_march<false><<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
+            auto* k = b->mixed ? (ad ? k_march<true, true> : k_march<true, false>)
+                               : (ad ? k_march<false, true> : k_march<false, false>);
+            k<<<b->grid_stencil, MW, 0, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
         }
     }
     // the row (x) and column (y) solves are independent: fork the column solve onto the side
@@ -2058,9 +2183,11 @@ int log_after_step(cel_batch* b, std::string& err) {
         std::vector<float> host(size_t(m.hs.NX) * m.hs.NY * 4);
         if (int e = batch_get_state(b, int(i), host.data(), err)) return e;
         double t_end = 0;
+        float last_dt = b->step_dt[i];   // the dt the clock advanced by at the end of the step
         B_TRY(cudaMemcpyAsync(&t_end, b->hdev[i].time64, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+        if (b->adaptive) B_TRY(cudaMemcpyAsync(&last_dt, b->dt_table + i, sizeof(float), cudaMemcpyDeviceToHost, b->stream));
         B_TRY(cudaStreamSynchronize(b->stream));
-        const float t0 = float(t_end - double(b->step_dt[i]));
+        const float t0 = float(t_end - double(last_dt));
         const float elapsed = b->elapsed_src ? *b->elapsed_src
                                              : std::chrono::duration<float>(std::chrono::steady_clock::now() - b->created).count();
         if (int e = log_dump(lg, host.data(), m.hs.nx, m.hs.ny, t0, elapsed, err)) return e;
@@ -2068,12 +2195,34 @@ int log_after_step(cel_batch* b, std::string& err) {
     return CEL_OK;
 }
 
+// Adaptive batches: the CFL rate of every member's current state (before the first pass and
+// before each adaptive predictor), then each member's dt for this pass.
+int choose_dt_device(cel_batch* b, bool first_of_step, std::string& err) {
+    const int n = int(b->mem.size());
+    const int scheme = b->sch.time_scheme;
+    const bool need_cfl = !b->dt_started || scheme == CEL_SCHEME_PREDICTOR_ADAPTIVE;
+    if (need_cfl) {
+        B_TRY(cudaMemsetAsync(b->cfl_now, 0, n * sizeof(unsigned int), b->stream));
+        TimedLaunch t(&b->tm, b->stream, "cfl");
+        k_cfl<<<std::min(b->ntiles, b->sms * 8), 256, 0, b->stream>>>(b->ddev, b->tiles, b->ntiles, b->ix.sin, b->cfl_now);
+    }
+    k_choose_dt<<<(n + 127) / 128, 128, 0, b->stream>>>(b->ctl, b->dt_table, need_cfl ? b->cfl_now : nullptr, n, scheme,
+                                                        first_of_step ? 1 : 0);
+    B_TRY(cudaGetLastError());
+    b->dt_started = true;
+    return CEL_OK;
+}
+
 // One pass with the host state machine; updates the buffer indices.
 int run_pass(cel_batch* b, bool first_of_step, std::string& err) {
     Scheme& s = b->sch;
     Idx& ix = b->ix;
-    if (!s.initialized) s.choose_dt(0.f);
-    else s.choose_dt(0.f);
+    if (b->adaptive) {
+        if (int e = choose_dt_device(b, first_of_step, err)) return e;
+        s.initialized = true;
+    } else {
+        s.choose_dt(0.f);
+    }
     PassArgs pa{};
     pa.scheme = s.time_scheme;
     pa.in = ix.sin;
@@ -2099,7 +2248,7 @@ int run_pass(cel_batch* b, bool first_of_step, std::string& err) {
     if (book) {
         const int o = ix.og, oo = ix.oog, sc = ix.scr;
         ix.og = sc; ix.oog = o; ix.scr = oo;
-        k_advance_time<<<(int(b->mem.size()) + 127) / 128, 128, 0, b->stream>>>(b->ddev, int(b->mem.size()));
+        k_advance_time<<<(int(b->mem.size()) + 127) / 128, 128, 0, b->stream>>>(b->ddev, b->ctl, int(b->mem.size()));
         B_TRY(cudaGetLastError());
     } else if (was_pred) {
         ix.pred = ix.scr;
@@ -2134,10 +2283,13 @@ int build_graphs(cel_batch* b, std::string& err) {
         starts.push_back(b->ix);
         cudaGraph_t g = nullptr;
         B_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-        const bool tm_on = b->tm.enabled;
+        // no timers and no log writes (host readbacks) inside a capture; replays log after each step
+        const bool tm_on = b->tm.enabled, log_on = b->any_log;
         b->tm.enabled = false;
+        b->any_log = false;
         int st = run_physical_step(b, err);
         b->tm.enabled = tm_on;
+        b->any_log = log_on;
         cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
         if (st) { if (g) cudaGraphDestroy(g); return st; }
         if (ce != cudaSuccess) { err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce); return CEL_ERR_CUDA; }
@@ -2224,13 +2376,25 @@ int configure_work(cel_batch* b, int cw, int mh, int rps, std::string& err) {
         B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc, NTC, smem_cols));
         b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
     }
+    // both variants of the stencil (fixed and adaptive predictor) run on the same grid
     if (b->rows_per_step == 2) {
-        auto* k2 = b->mixed ? k_march2<true> : k_march2<false>;
-        B_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, int(MARCH2_DYN_SMEM)));
-        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k2, MW, MARCH2_DYN_SMEM));
+        occ = 1 << 20;
+        for (auto* k2 : {b->mixed ? k_march2<true, false> : k_march2<false, false>,
+                         b->mixed ? k_march2<true, true> : k_march2<false, true>}) {
+            int o = 0;
+            B_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, int(MARCH2_DYN_SMEM)));
+            B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k2, MW, MARCH2_DYN_SMEM));
+            occ = std::min(occ, o);
+        }
+    } else {
+        occ = 1 << 20;
+        for (auto* k1 : {b->mixed ? k_march<true, false> : k_march<false, false>,
+                         b->mixed ? k_march<true, true> : k_march<false, true>}) {
+            int o = 0;
+            B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k1, MW, 0));
+            occ = std::min(occ, o);
+        }
     }
-    else
-        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->mixed ? k_march<true> : k_march<false>, MW, 0));
     b->grid_stencil = std::max(1, std::min(b->nmtiles, b->sms * std::max(occ, 1)));
     return CEL_OK;
 }
@@ -2243,7 +2407,10 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     const int N0 = params[0]->correction_steps;
     for (int i = 0; i < n; ++i) {
         if (params[i]->correction_steps != N0) { err = "batch members must share correctionStepsNum"; return nullptr; }
-        if (params[i]->adaptive) { err = "batches run fixed time steps (adaptive members are not supported)"; return nullptr; }
+        if ((params[i]->adaptive != 0) != (params[0]->adaptive != 0)) {
+            err = "batch members must share the adaptive time-step setting";
+            return nullptr;
+        }
         if (params[i]->ny > 6900) { err = "fused form supports ny <= 6900 (column band in shared memory)"; return nullptr; }
         if (params[i]->nx > 16000) { err = "fused form supports nx <= 16000 (row in shared memory)"; return nullptr; }
         if (log_validate(params[i]->log, params[i]->nx, params[i]->ny, err)) {
@@ -2278,6 +2445,21 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         b->dt_table = static_cast<float*>(p);
         if (cudaMallocHost(&p, size_t(n) * sizeof(float)) != cudaSuccess) { err = "cudaMallocHost failed"; return nullptr; }
         b->dt_host = static_cast<float*>(p);
+        b->adaptive = params[0]->adaptive != 0;
+        if (b->adaptive) {
+            if (dalloc(b.get(), &p, size_t(n) * sizeof(DtCtl), err)) return nullptr;
+            b->ctl = static_cast<DtCtl*>(p);
+            if (dalloc(b.get(), &p, size_t(n) * sizeof(unsigned int), err)) return nullptr;
+            b->cfl_now = static_cast<unsigned int*>(p);
+            std::vector<DtCtl> c0(n);
+            for (int i = 0; i < n; ++i) {
+                std::memset(&c0[i], 0, sizeof(DtCtl));
+                c0[i].base = float(params[i]->timestep);
+                c0[i].min_ratio = float(params[i]->min_timestep_ratio);
+                c0[i].alpha = float(params[i]->ema_alpha);
+            }
+            cudaMemcpy(b->ctl, c0.data(), n * sizeof(DtCtl), cudaMemcpyHostToDevice);
+        }
     }
     std::vector<int4> tiles;
     std::vector<int2> rows, bitems[4];
@@ -2302,6 +2484,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         d.P = m.P;
         b->dt_host[i] = float(m.p.timestep);
         d.dtp = b->dt_table + i;
+        d.ab = b->ctl ? b->ctl[i].ab : nullptr;
         // planes: state 9 (+9 lo), bottom 3, rhs 2, history 12 + 8, aux 2, factors 6
         const int nplanes = 9 + (b->mixed ? 9 : 0) + 3 + 2 + 12 + 8 + 2 + 6;
         void* base = nullptr;
@@ -2526,7 +2709,7 @@ int batch_step(cel_batch* b, int nsteps, std::string& err) {
             Scheme& s = b->sch;
             Idx& ix = b->ix;
             do {
-                s.choose_dt(0.f);
+                if (!b->adaptive) s.choose_dt(0.f);
                 const int in = ix.sin;
                 int out;
                 if (s.time_scheme == CEL_SCHEME_CORRECTOR) out = 3 - in - ix.cur;
@@ -2564,6 +2747,8 @@ int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
     std::vector<double> t64(n);
     for (size_t i = 0; i < n; ++i)
         B_TRY(cudaMemcpyAsync(&t64[i], b->hdev[i].time64, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    std::vector<DtCtl> ctl(b->adaptive ? n : 0);
+    if (b->adaptive) B_TRY(cudaMemcpyAsync(ctl.data(), b->ctl, n * sizeof(DtCtl), cudaMemcpyDeviceToHost, b->stream));
     B_TRY(cudaStreamSynchronize(b->stream));
     for (size_t i = 0; i < n; ++i) {
         const double* s = &v[i * STATS_N];
@@ -2587,9 +2772,11 @@ int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
         o.health = s[10] != 0 ? CEL_ERR_NUMERIC : 0;
         // a bounded TMA wait that gave up (should never happen) is a CUDA error of the batch
         if (late != 0) o.health = CEL_ERR_CUDA;
-        o.timestep = double(b->dt_host[i]);
+        // adaptive members: the dt of the step's first pass; the clock advanced by the last pass's dt
+        o.timestep = b->adaptive ? double(ctl[i].dt_first) : double(b->dt_host[i]);
         o.cfl_number = o.cfl_rate * o.timestep;
-        o.total_time = at_step ? t64[i] - double(b->step_dt[i]) : t64[i];
+        const double last_dt = b->adaptive ? double(ctl[i].dt) : double(b->step_dt[i]);
+        o.total_time = at_step ? t64[i] - last_dt : t64[i];
         o.time_scheme = b->sch.time_scheme;
     }
     return CEL_OK;
@@ -2653,6 +2840,7 @@ int batch_use_graph(cel_batch* b, bool enable, std::string& err) {
 long long batch_cells(const cel_batch* b) { return b->cells; }
 
 int batch_set_timestep(cel_batch* b, const float* dt, std::string& err) {
+    if (b->adaptive) { err = "an adaptive batch chooses its time steps on the device"; return CEL_ERR_STATE; }
     // the uniform time step of each member (the reference's "uniform time step" setting,
     // uploaded with the constant buffers before every pass, engine.cpp:1728-1750)
     for (size_t i = 0; i < b->mem.size(); ++i) {
@@ -2723,7 +2911,9 @@ int batch_launches_per_step(const cel_batch* b) {
     int per_pass = 3;  // stencil, row solve, column solve
     for (int s = 0; s < 4; ++s)
         if (b->nbitems[s] > 0) per_pass += b->two_phase[s] ? 2 : 1;
-    return (1 + b->sch.N) * per_pass + 1;  // + the clock advance
+    // adaptive batches add the dt choice before every pass and the CFL reduction before the predictor
+    if (b->adaptive) per_pass += 1;
+    return (1 + b->sch.N) * per_pass + 1 + (b->adaptive ? 1 : 0);  // + the clock advance
 }
 
 // ---- single-domain fused engine (a batch of one) behind the engine interface ---------------
@@ -2762,7 +2952,7 @@ public:
     }
     int get_aux(float* rgba) override { return batch_get_aux(b, 0, rgba, err); }
     int reset_timestep(float, float, cel_stats* out) override {
-        b->sch.choose_dt(0.f);
+        if (!b->adaptive) b->sch.choose_dt(0.f);
         if (!out) return CEL_OK;
         return batch_stats(b, out, true, err);
     }

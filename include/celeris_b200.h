@@ -195,7 +195,11 @@ int cel_synchronize(cel_engine* h);
 
 /* ---- batched ensembles: many domains advanced by one launch per phase ------------------- */
 /* params[i] and bathy[i] (bnx[i] x bny[i]) describe member i; form is CEL_FORM_FUSED or
- * CEL_FORM_MIXED. */
+ * CEL_FORM_MIXED.  Members share correctionStepsNum and the adaptive setting.  Adaptive batches
+ * choose each member's dt on the device before every pass, as resetTimestep does
+ * (engine.cpp:1698-1726: target CFL from the first positive CFL rate, moving-average growth,
+ * uniform dt for Euler and corrector passes) and run the variable-step AB3 predictor
+ * (compute.hlsl:766-780); a step needs no host readback and replays from a CUDA graph. */
 int cel_batch_create(int n, const cel_params* const* params, const float* const* bathy,
                      const int* bnx, const int* bny, int form, cel_batch** out);
 int cel_batch_destroy(cel_batch* b);
@@ -214,7 +218,8 @@ int cel_batch_get_aux(cel_batch* b, int i, float* rgba);
 int cel_batch_use_graph(cel_batch* b, int enable);        /* capture one physical step in a CUDA graph */
 long long cel_batch_cells(const cel_batch* b);            /* sum of interior nx*ny */
 /* Per-member uniform time step (n floats), uploaded asynchronously on the batch stream; the
- * reference uploads dt with its constant buffers before every pass (engine.cpp:1728-1750). */
+ * reference uploads dt with its constant buffers before every pass (engine.cpp:1728-1750).
+ * CEL_ERR_STATE for adaptive batches, which choose their steps on the device. */
 int cel_batch_set_timestep(cel_batch* b, const float* dt);
 /* Kernel launches one physical step issues (all members together). */
 int cel_batch_launches_per_step(const cel_batch* b);

@@ -222,3 +222,53 @@ def test_paired_row_stencil_matches_single_row(celeris):
         s1, s2 = b1.stats(), b2.stats()
         for x, y in zip(s1, s2):
             assert y["mass_full"] == pytest.approx(x["mass_full"], rel=1e-9)
+
+
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+@pytest.mark.parametrize("kind, N", [("mixed", 1), ("sponge", 0), ("solid", 1)])
+def test_adaptive_batch_vs_fp64_oracle(celeris, form, kind, N):
+    """Adaptive time steps chosen on the device (engine.cpp:1698-1726, compute.hlsl:766-780)."""
+    p, z, bnx, bny, keep = _case(kind, nx=70, ny=45, N=N)
+    p.adaptive = 1
+    ref = O.Oracle(p, z, bnx, bny, "f64")
+    eng = celeris.Engine(p, z, form)
+    ref.physical_steps(150)
+    eng.physical_steps(150)
+    a, b = eng.state(), ref.state()
+    assert np.isfinite(a).all()
+    rms = eta_rms(a, b)
+    assert rms <= 1e-4, rms
+    # the clock is the sum of the chosen steps: the dt sequences agree
+    t_ref = ref.reset_timestep()["total_time"]
+    t_gpu = eng.stats()["total_time"]
+    assert abs(t_gpu - t_ref) <= 1e-5 * t_ref, (t_gpu, t_ref)
+
+
+def test_adaptive_batch_equals_single_engines_and_graph_replay(celeris):
+    members = [_case(k, nx=40 + 8 * i, ny=24 + 4 * i, N=1)[:4] for i, k in enumerate(["solid", "mixed", "sponge"])]
+    for m in members:
+        m[0].adaptive = 1
+    direct = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    direct.step(40)
+    graph = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    graph.use_graph(True)
+    graph.step(40)
+    sd, sg = direct.stats_current(), graph.stats_current()
+    for i, (p, z, bnx, bny) in enumerate(members):
+        e = celeris.Engine(p, z, "mixed")
+        e.physical_steps(40)
+        np.testing.assert_array_equal(direct.state(i), e.state())
+        np.testing.assert_array_equal(graph.state(i), e.state())
+        assert sd[i]["total_time"] == sg[i]["total_time"] == e.stats()["total_time"]
+        assert sd[i]["timestep"] > 0
+
+
+def test_adaptive_batch_refuses_host_time_steps(celeris):
+    p, z, bnx, bny, keep = _case("solid", N=1)
+    p.adaptive = 1
+    b = celeris.Batch([(p, z)], "mixed")
+    with pytest.raises(celeris.CelError, match="adaptive"):
+        b.set_timestep(np.array([1e-3], dtype=np.float32))
+    q, z2, _, _, _ = _case("solid", N=1)
+    with pytest.raises(celeris.CelError, match="adaptive"):
+        celeris.Batch([(p, z), (q, z2)], "mixed")
