@@ -10,7 +10,8 @@ import numpy as np
 from celeris_b200 import cases
 
 STEPS = 20
-NAMES = ["solid", "mixed", "sponge", "irregular", "uts", "solid_wide", "irregular_sea_level", "adaptive_manning"]
+NAMES = ["solid", "mixed", "sponge", "irregular", "uts", "solid_wide", "irregular_sea_level", "adaptive_manning",
+         "nlsw", "adaptive_ab3"]
 
 
 def golden_case(name: str):
@@ -24,6 +25,17 @@ def golden_case(name: str):
     elif name == "irregular_sea_level":
         p, z, bnx, bny = cases.small_case(40, 24, "irregular", correction_steps=1)
         p.west.sea_level, p.south.sea_level = 0.05, 0.02
+    elif name == "nlsw":
+        # model type NLSW: identity tridiagonal systems, dispersion terms kept (engine.cpp:2625, 4127);
+        # those terms are then explicit, so the grid is 4 m (depth / dx ~ 1) with the Courant number kept
+        p, z, bnx, bny = cases.small_case(40, 24, "mixed", correction_steps=1)
+        p.boussinesq = 0
+        p.width, p.length, p.timestep = 4 * p.width, 4 * p.length, 4 * p.timestep
+    elif name == "adaptive_ab3":
+        # adaptive predictor every step (no corrector): the variable-step AB3 of compute.hlsl:766-780
+        p, z, bnx, bny = cases.small_case(44, 26, "mixed", correction_steps=0)
+        p.adaptive = 1
+        p.timestep *= 0.5
     elif name == "adaptive_manning":
         p, z, bnx, bny = cases.small_case(37, 29, "sponge", correction_steps=2)
         p.adaptive = 1

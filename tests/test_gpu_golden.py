@@ -46,14 +46,24 @@ def test_plain_form_bottom_matches_reference_sampling(celeris):
 
 @pytest.mark.parametrize("form", ["fused", "mixed"])
 def test_batched_forms_within_tolerance_of_reference(celeris, form):
-    names = [n for n in NAMES if n != "adaptive_manning"]   # batches run fixed time steps
-    built = [golden_case(n) for n in names]
-    batch = celeris.Batch([(c[0], c[1]) for c in built], form)
-    batch.use_graph(True)
-    batch.step(STEPS)
-    for i, n in enumerate(names):
-        ref = GOLD[f"{n}/state"].astype(np.float64)
-        got = batch.state(i).astype(np.float64)
-        d = got[2:-2, 2:-2, 0] - ref[2:-2, 2:-2, 0]
-        rms = float(np.sqrt(np.mean(d * d)))
-        assert rms < 1e-4, (n, rms)
+    # batch members share the correction count and the adaptive setting: one batch per group
+    built = {n: golden_case(n) for n in NAMES}
+    groups = {}
+    for n, c in built.items():
+        groups.setdefault((c[0].correction_steps, c[0].adaptive), []).append(n)
+    for names in groups.values():
+        batch = celeris.Batch([(built[n][0], built[n][1]) for n in names], form)
+        batch.use_graph(True)
+        batch.step(STEPS)
+        stats = batch.stats()   # gathered at the start of the last step, as the reference's resetTimestep
+        for i, n in enumerate(names):
+            ref = GOLD[f"{n}/state"].astype(np.float64)
+            got = batch.state(i).astype(np.float64)
+            d = got[2:-2, 2:-2, 0] - ref[2:-2, 2:-2, 0]
+            rms = float(np.sqrt(np.mean(d * d)))
+            assert rms < 1e-4, (n, rms)
+            # the clock at the start of the last step (the sum of the steps taken before it, adaptive
+            # ones included) matches the reference's
+            keys = list(GOLD["stat_keys"])
+            t_ref = GOLD[f"{n}/stats"][keys.index("total_time")]
+            assert abs(stats[i]["total_time"] - t_ref) <= 2e-6 * t_ref, (n, stats[i]["total_time"], t_ref)
