@@ -139,6 +139,53 @@ def cpu_sample(seconds: float, members):
     return rate, O.threads("f32"), f"{n} physical steps of one {p.nx}x{p.ny} member (FP32 transcription, OpenMP)"
 
 
+def member_k(cfg: str, k: int):
+    """Member k of a workload alone (without building the others)."""
+    from celeris_b200 import cases
+    if cfg == "c4":
+        return cases.config4(1, 1, first_member=k)[0]
+    if cfg == "c5":
+        return cases.config5(1, 1, first_member=k)[0]
+    return members_for(cfg, 0, 1)[0][0]
+
+
+def _ref_worker(cfg, k, seconds, barrier, out):
+    """One process of the reference arm: the reference-shader build stepping member k."""
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
+    import oracle as O
+    p, z, bnx, bny = member_k(cfg, k)
+    o = O.Oracle(p, z, bnx, bny, "ref")
+    o.physical_steps(1)
+    barrier.wait(timeout=600)
+    steps, t = 0, 0.0
+    while t < seconds:
+        t += o.time_physical_steps(1)
+        steps += 1
+    out.put((k, p.nx * p.ny, steps, t))
+
+
+def reference_pool(cfg: str, count: int, seconds: float):
+    """The reference-shader build on every host core at once: one spawned process per core, each
+    stepping a different member (the build's texture bindings are process-wide, as a D3D
+    context's are, so one process runs one domain).  Rate = all cell-steps / the longest time."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    cores = max(1, min(len(os.sched_getaffinity(0)), count))
+    barrier, out = ctx.Barrier(cores), ctx.Queue()
+    procs = [ctx.Process(target=_ref_worker, args=(cfg, k, seconds, barrier, out)) for k in range(cores)]
+    for q in procs:
+        q.start()
+    res = [out.get(timeout=1800) for _ in procs]
+    for q in procs:
+        q.join(timeout=60)
+    work = sum(cells * steps for _, cells, steps, _ in res)
+    t = max(t for *_, t in res)
+    steps = sum(r[2] for r in res)
+    sample = (f"{steps} physical steps over members 0..{cores - 1} ({cores} processes at once, one member each; "
+              f"the reference's compute.hlsl compiled for the CPU)")
+    return work / t, cores, sample
+
+
 def reference_arm(args):
     """CPU implementation of the path on the host cores, same metric and config."""
     rank = int(os.environ.get("RANK", "0"))
@@ -148,21 +195,10 @@ def reference_arm(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     kind = "port"
     # the reference's own compute.hlsl compiled for the CPU (oracle/_ref, built from the reference
-    # sources), when that build is present: it runs single-threaded (its texture bindings are
-    # process-wide, as a D3D context's are)
+    # sources), when that build is present, on all host cores
     if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_shader.so")):
-        import oracle as O
-        sizes = [p.nx * p.ny for p, *_ in members]
-        mean = sum(sizes) / len(sizes)
-        k = min(range(len(sizes)), key=lambda i: abs(sizes[i] - mean))
-        p, z, bnx, bny = members[k]
-        o = O.Oracle(p, z, bnx, bny, "ref")
-        o.physical_steps(1)
-        t = o.time_physical_steps(1)
-        n = max(1, int(max(1.0, args.cpu_seconds) / max(t, 1e-6)))
-        t = o.time_physical_steps(n)
-        rate, cores, kind = p.nx * p.ny * n / t, 1, "reference"
-        sample = f"{n} physical steps of one {p.nx}x{p.ny} member (the reference's compute.hlsl compiled for the CPU)"
+        rate, cores, sample = reference_pool(args.config, len(members), max(1.0, args.cpu_seconds))
+        kind = "reference"
     else:   # the FP32 restatement with OpenMP
         rate, cores, sample = cpu_sample(max(1.0, args.cpu_seconds), members)
     val = rate / 1e9
