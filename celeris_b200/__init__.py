@@ -284,3 +284,13 @@ def write_bathymetry(params: Params, bottom: np.ndarray, path: str | None = None
 def write_hotstart(params: Params, rgba: np.ndarray, path: str):
     a = _texels(params, rgba, 4)
     check(lib().cel_write_hotstart(C.byref(params), _fp(a), path.encode()))
+
+
+def spectrum_waves(hs: float, tp: float, mean_theta_deg: float, depth: float, seed: int = 0,
+                   gravity: float = 9.81, path: str | None = None) -> abi.Boundary:
+    """Irregular-wave components of a directional spectrum (the reference's generateSpectrumWaves),
+    as a boundary's wave table; set ``type``, ``width`` and ``sea_level`` on the result."""
+    s = abi.Spectrum(hs, tp, mean_theta_deg, depth)
+    b = abi.Boundary()
+    check(lib().cel_spectrum_waves(C.byref(s), gravity, seed, C.byref(b), path.encode() if path else None))
+    return b

@@ -79,6 +79,11 @@ class Params(C.Structure):
     ]
 
 
+class Spectrum(C.Structure):
+    _fields_ = [("significant_waveheight", C.c_double), ("peak_period", C.c_double),
+                ("mean_theta", C.c_double), ("depth_at_source", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [(n, C.c_double) for n in (
         "mass", "x_momentum", "y_momentum", "kinetic_energy", "potential_energy", "total_energy",
@@ -148,6 +153,7 @@ def _declare(L: C.CDLL) -> None:
         "cel_read_uts": (i, [C.c_char_p, C.POINTER(Boundary)]),
         "cel_params_release": (None, [C.POINTER(Params)]),
         "cel_params_size": (C.c_size_t, []),
+        "cel_spectrum_waves": (i, [C.POINTER(Spectrum), C.c_double, C.c_ulonglong, C.POINTER(Boundary), C.c_char_p]),
         "cel_log_dump": (i, [C.POINTER(Params), fp, C.c_float, C.c_float]),
         "cel_write_inundation": (i, [C.POINTER(Params), fp, C.c_char_p]),
         "cel_write_bathymetry": (i, [C.POINTER(Params), fp, C.c_char_p]),
@@ -216,7 +222,7 @@ def check(status: int) -> None:
 EXPORTED = [
     "cel_last_error", "cel_version", "cel_params_default", "cel_params_from_cml",
     "cel_read_irregular_waves", "cel_read_uts", "cel_params_release", "cel_params_size", "cel_read_cbf",
-    "cel_log_dump", "cel_write_inundation", "cel_write_bathymetry", "cel_write_hotstart",
+    "cel_log_dump", "cel_write_inundation", "cel_write_bathymetry", "cel_write_hotstart", "cel_spectrum_waves",
     "cel_create", "cel_destroy", "cel_remesh", "cel_set_stream", "cel_get_dims",
     "cel_set_state", "cel_get_state", "cel_get_bottom", "cel_get_aux",
     "cel_reset_timestep", "cel_timestep", "cel_timesteps", "cel_physical_steps", "cel_get_stats",

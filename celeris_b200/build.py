@@ -25,6 +25,7 @@ UNITS = [
     ("params.cpp", []),
     ("setup.cpp", []),
     ("logio.cpp", []),
+    ("spectrum.cpp", []),
     ("capi.cpp", []),
     ("plain.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("fused.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),

@@ -150,6 +150,16 @@ void cel_params_release(cel_params* p) {
 
 size_t cel_params_size(void) { return sizeof(cel_params); }
 
+int cel_spectrum_waves(const cel_spectrum* s, double gravity, unsigned long long seed, cel_boundary* b, const char* path) {
+    if (!s || !b) { set_error("null argument"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN
+    std::string err;
+    const int st = cel::spectrum_waves(*s, gravity, seed, b, path, err);
+    if (st) set_error(err);
+    return st;
+    CEL_GUARD_END
+}
+
 int cel_log_dump(const cel_params* p, const float* rgba, float total_time, float elapsed) {
     if (!p || !rgba) { set_error("null argument"); return CEL_ERR_ARG; }
     CEL_GUARD_BEGIN

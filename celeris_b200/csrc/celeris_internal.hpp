@@ -19,6 +19,10 @@ int read_uts(const std::string& path, cel_boundary* b, std::string& err);
 int read_cbf(const std::string& path, std::vector<float>* z, int& bnx, int& bny, std::string& err);
 int read_hotstart(const std::string& path, int nx, int ny, std::vector<float>& whuhv, std::string& err);
 
+// ---- irregular-wave spectrum (spectrum.cpp) --------------------------------------------------
+int spectrum_waves(const cel_spectrum& in, double gravity, unsigned long long seed, cel_boundary* b, const char* path,
+                   std::string& err);
+
 // ---- file output (logio.cpp) ------------------------------------------------------------------
 int log_validate(const cel_log& lg, int nx, int ny, std::string& err);
 int log_dump(const cel_log& lg, const float* rgba, int nx, int ny, float total_time, float elapsed, std::string& err);

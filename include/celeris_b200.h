@@ -152,6 +152,22 @@ int cel_params_default(cel_params* p);
 int cel_params_from_cml(const char* path, cel_params* out);
 /* Reads an IrregularWaves component file into a boundary (engine.cpp:3520-3551) */
 int cel_read_irregular_waves(const char* path, cel_boundary* b);
+/* Spectrum wave-maker settings (IrregularWaveSpectrumSetting, settings.hpp:121-129; set from
+ * the GUI's "significant waveheight", "peak period", "mean direction", "depth at source") */
+typedef struct cel_spectrum {
+    double significant_waveheight;  /* Hs (m), capped at half the source depth */
+    double peak_period;             /* Tp (s) */
+    double mean_theta;              /* mean direction (degrees) */
+    double depth_at_source;         /* h (m) */
+} cel_spectrum;
+/* generateSpectrumWaves (engine.cpp:3559-3776): JONSWAP-shaped spectrum (gamma 3.3) on
+ * f_peak +- 5 x 0.005 Hz, cos^2s spreading over mean +- 20 degrees in 5-degree steps, truncated
+ * at 5 % of the peak; one component {amplitude, period, theta (rad), phase} per (f, theta) cell
+ * into b->waves / b->n_waves.  Phases come from `seed` (the reference seeds rand() with the
+ * clock), quantised as (r % 10000) / 10000 x 2 pi.  path != NULL also writes the reference's
+ * component file, which cel_read_irregular_waves reads back. */
+int cel_spectrum_waves(const cel_spectrum* s, double gravity, unsigned long long seed, cel_boundary* b,
+                       const char* path);
 /* Reads a UniformTimeSeries file into a boundary (engine.cpp:3863-3874) */
 int cel_read_uts(const char* path, cel_boundary* b);
 void cel_params_release(cel_params* p);

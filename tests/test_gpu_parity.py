@@ -278,3 +278,27 @@ def test_adaptive_batch_refuses_host_time_steps(celeris):
     q, z2, _, _, _ = _case("solid", N=1)
     with pytest.raises(celeris.CelError, match="adaptive"):
         celeris.Batch([(p, z), (q, z2)], "mixed")
+
+
+@pytest.mark.parametrize("form", ["plain", "mixed"])
+def test_spectrum_wavemaker(celeris, form):
+    """A west wave-maker driven by the spectrum generator's 90 components (a larger pairwise sum
+    tree than the hand-made component lists)."""
+    p, z, bnx, bny, keep = _case("irregular", nx=60, ny=40, N=1)
+    b = celeris.spectrum_waves(0.3, 6.0, 10.0, 5.0, seed=11)
+    assert b.n_waves > 64
+    p.west.n_waves = b.n_waves
+    for k in range(b.n_waves):
+        for q in range(4):
+            p.west.waves[k][q] = b.waves[k][q]
+    eng = celeris.Engine(p, z, form)
+    eng.physical_steps(120)
+    a = eng.state()
+    if form == "plain":
+        ref = O.Oracle(p, z, bnx, bny, "f32")
+        ref.physical_steps(120)
+        np.testing.assert_array_equal(a[2:-2, 2:-2, :3].astype(np.float64), ref.state()[2:-2, 2:-2, :3])
+    else:
+        ref = O.Oracle(p, z, bnx, bny, "f64")
+        ref.physical_steps(120)
+        assert eta_rms(a, ref.state()) <= 1e-4
