@@ -22,6 +22,7 @@ the step.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -271,10 +272,14 @@ def main():
     barrier()
     t0 = time.perf_counter()
     e0.record(stream)
+    # straight through the C ABI (the library's public interface), results into a caller-owned array
+    lib = cb.lib()
+    dt_ptr = C.cast(C.c_void_p(dt_pinned.data_ptr()), C.POINTER(C.c_float))
+    stats_out = (cb.Stats * n)()
     for _ in range(e2e_steps):
-        batch.set_timestep(dt_pinned.data_ptr())
-        batch.step(1)
-        batch.stats()
+        cb.check(lib.cel_batch_set_timestep(batch.h, dt_ptr))
+        cb.check(lib.cel_batch_step(batch.h, 1))
+        cb.check(lib.cel_batch_stats(batch.h, stats_out))
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)

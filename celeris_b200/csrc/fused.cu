@@ -1998,6 +1998,11 @@ struct cel_batch {
     double* stats_all = nullptr;       // members * STATS_N, gathered by the first pass of each step
     double* stats_now_all = nullptr;   // members * STATS_N, on-demand statistics of the current state
     double* late_flag = nullptr;       // a bounded TMA wait gave up (sticky)
+    // readback block: late_flag | clock64 (n) | stats_all (n x STATS_N) | stats_now_all, so that
+    // the statistics of a step, the clocks and the flag come back in one copy
+    double* clock64 = nullptr;         // per-member FP64 clocks
+    float* clock32 = nullptr;          // per-member FP32 clocks
+    double* rb_host = nullptr;         // pinned host copy of the readback block
     bool step_stats_valid = false;     // stats_all describes the start of the most recent step
     std::vector<float> step_dt;        // the time step each member took in its most recent step
     bool any_friction = false;
@@ -2435,12 +2440,16 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     std::vector<float4> waves;
     {
         void* p = nullptr;
-        if (dalloc(b.get(), &p, size_t(n) * STATS_N * sizeof(double), err)) return nullptr;
-        b->stats_all = static_cast<double*>(p);
-        if (dalloc(b.get(), &p, size_t(n) * STATS_N * sizeof(double), err)) return nullptr;
-        b->stats_now_all = static_cast<double*>(p);
-        if (dalloc(b.get(), &p, sizeof(double), err)) return nullptr;
-        b->late_flag = static_cast<double*>(p);
+        const size_t nd = 1 + size_t(n) + 2 * size_t(n) * STATS_N;
+        if (dalloc(b.get(), &p, nd * sizeof(double) + size_t(n) * sizeof(float), err)) return nullptr;
+        double* blk = static_cast<double*>(p);
+        b->late_flag = blk;
+        b->clock64 = blk + 1;
+        b->stats_all = blk + 1 + n;
+        b->stats_now_all = blk + 1 + n + size_t(n) * STATS_N;
+        b->clock32 = reinterpret_cast<float*>(blk + nd);
+        if (cudaMallocHost(&p, nd * sizeof(double)) != cudaSuccess) { err = "cudaMallocHost failed"; return nullptr; }
+        b->rb_host = static_cast<double*>(p);
         if (dalloc(b.get(), &p, size_t(n) * sizeof(float), err)) return nullptr;
         b->dt_table = static_cast<float*>(p);
         if (cudaMallocHost(&p, size_t(n) * sizeof(float)) != cudaSuccess) { err = "cudaMallocHost failed"; return nullptr; }
@@ -2530,12 +2539,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         }
         d.stats = b->stats_all + size_t(i) * STATS_N;
         d.stats_now = b->stats_now_all + size_t(i) * STATS_N;
-        {
-            void* tp = nullptr;
-            if (dalloc(b.get(), &tp, 64, err)) return nullptr;
-            d.time64 = static_cast<double*>(tp);
-            d.time32 = reinterpret_cast<float*>(static_cast<char*>(tp) + 16);
-        }
+        d.time64 = b->clock64 + i;
+        d.time32 = b->clock32 + i;
         // upload planes (pitched)
         auto put = [&](float* dst, const std::vector<float>& src) -> int {
             std::vector<float> pl(m.plane, 0.f);
@@ -2680,6 +2685,7 @@ void batch_destroy(cel_batch* b) {
     if (b->side) cudaStreamSynchronize(b->side);
     for (void* a : b->allocs) cudaFree(a);
     if (b->dt_host) cudaFreeHost(b->dt_host);
+    if (b->rb_host) cudaFreeHost(b->rb_host);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
     if (b->side) cudaStreamDestroy(b->side);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
@@ -2739,17 +2745,22 @@ int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
         k_stats_only<<<std::min(b->ntiles, b->sms * 8), 256, 0, b->stream>>>(b->ddev, b->tiles, b->ntiles, b->ix.sin);
         B_TRY(cudaGetLastError());
     }
-    std::vector<double> v(n * STATS_N);
-    double late = 0.0;
-    B_TRY(cudaMemcpyAsync(v.data(), at_step ? b->stats_all : b->stats_now_all, v.size() * sizeof(double),
-                          cudaMemcpyDeviceToHost, b->stream));
-    B_TRY(cudaMemcpyAsync(&late, b->late_flag, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
-    std::vector<double> t64(n);
-    for (size_t i = 0; i < n; ++i)
-        B_TRY(cudaMemcpyAsync(&t64[i], b->hdev[i].time64, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    // flag, clocks and the step's statistics are contiguous: one copy into pinned memory
+    double* h = b->rb_host;
+    const size_t head = 1 + n;
+    if (at_step) {
+        B_TRY(cudaMemcpyAsync(h, b->late_flag, (head + n * STATS_N) * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    } else {
+        B_TRY(cudaMemcpyAsync(h, b->late_flag, head * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+        B_TRY(cudaMemcpyAsync(h + head, b->stats_now_all, n * STATS_N * sizeof(double), cudaMemcpyDeviceToHost,
+                              b->stream));
+    }
     std::vector<DtCtl> ctl(b->adaptive ? n : 0);
     if (b->adaptive) B_TRY(cudaMemcpyAsync(ctl.data(), b->ctl, n * sizeof(DtCtl), cudaMemcpyDeviceToHost, b->stream));
     B_TRY(cudaStreamSynchronize(b->stream));
+    const double late = h[0];
+    const double* t64 = h + 1;
+    const double* v = h + head;
     for (size_t i = 0; i < n; ++i) {
         const double* s = &v[i * STATS_N];
         const Member& m = b->mem[i];
