@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA graphs (profiling)")
     ap.add_argument("--stencil-rows", type=int, default=0, choices=[0, 1, 2],
                     help="force the stencil variant (1 or 2 rows per step) after tuning; 0 keeps the choice")
+    ap.add_argument("--stencil-width", type=int, default=0, choices=[0, 96, 128],
+                    help="force the stencil strip threads (with two rows per step) after tuning; 0 keeps the choice")
     ap.add_argument("--tune-steps", type=int, default=6, help="steps per autotuner candidate (0 keeps the defaults)")
     return ap.parse_args()
 
@@ -238,12 +240,15 @@ def main():
     cells = batch.cells
     N = members[0][0].correction_steps
     with torch.cuda.stream(stream):
-        # the autotuner times each (band width, strip height) candidate for a few steps; those
+        # the autotuner times each (band width, strip height, stencil rows, stencil width) candidate
+        # for a few steps; those
         # steps are warm-up too and lie outside the timed region
         batch.use_graph(not args.no_graph)
         tuned = batch.autotune(args.tune_steps) if args.tune_steps > 0 else None
         if args.stencil_rows:
             batch.set_stencil_rows(args.stencil_rows)
+        if args.stencil_width:
+            batch.set_stencil_width(args.stencil_width)
         batch.step(max(3, args.warmup))
     torch.cuda.synchronize()
 
@@ -361,6 +366,7 @@ def main():
                        "parallelism": f"ensemble sharded by domain over {world} GPU(s)",
                        "tuning": {"column_band_width": batch.tuning[0], "strip_height": batch.tuning[1],
                                   "stencil_rows_per_step": batch.stencil_rows,
+                                  "stencil_threads_per_strip": batch.stencil_width,
                                   "autotuned": tuned is not None,
                                   "pcr_switch": "none (Thomas factors + scans; no cyclic-reduction stage)"}},
             "e2e": {"value": e2e_value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": h2d,

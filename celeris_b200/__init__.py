@@ -237,6 +237,14 @@ class Batch:
         """1: one row per stencil step; 2: two rows as paired f32x2 arithmetic."""
         check(lib().cel_batch_set_stencil_rows(self.h, rows_per_step))
 
+    @property
+    def stencil_width(self) -> int:
+        return int(lib().cel_batch_stencil_width(self.h))
+
+    def set_stencil_width(self, threads: int):
+        """Threads per stencil CTA (128 or 96; 96 with two rows per step)."""
+        check(lib().cel_batch_set_stencil_width(self.h, threads))
+
     def autotune(self, steps: int = 5) -> dict:
         """Times each candidate for `steps` steps and keeps the fastest (the members advance)."""
         tx, ty, ms = C.c_int(), C.c_int(), C.c_double()

@@ -27,6 +27,8 @@ int batch_set_timestep(cel_batch* b, const float* dt, std::string& err);
 int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err);
 int batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rps);
 int batch_set_stencil_rows(cel_batch* b, int rps, std::string& err);
+int batch_set_stencil_width(cel_batch* b, int threads, std::string& err);
+int batch_stencil_width(const cel_batch* b);
 int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, std::string& err);
 KernelTimer* batch_timer(cel_batch* b);
 int batch_launches_per_step(const cel_batch* b);

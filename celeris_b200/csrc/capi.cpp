@@ -396,6 +396,11 @@ int cel_batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rows_per_ste
     if (!b) { set_error("null batch"); return CEL_ERR_ARG; }
     return cel::batch_get_tuning(b, tx, ty, rows_per_step);
 }
+int cel_batch_set_stencil_width(cel_batch* b, int threads) {
+    BAT(b);
+    CEL_GUARD_BEGIN BRET(cel::batch_set_stencil_width(b, threads, err)); CEL_GUARD_END
+}
+int cel_batch_stencil_width(const cel_batch* b) { return b ? cel::batch_stencil_width(b) : 0; }
 int cel_batch_set_stencil_rows(cel_batch* b, int rows_per_step) {
     BAT(b);
     CEL_GUARD_BEGIN BRET(cel::batch_set_stencil_rows(b, rows_per_step, err)); CEL_GUARD_END

@@ -677,6 +677,9 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
 // t+2 and t+3 and uses those of rows t and t+1 from step j-1.  Ring: RING2 = 9 rows, the window
 // t-2 .. t+4 plus the two rows requested one step ahead.
 // ---------------------------------------------------------------------------------------------
+// CTAs per SM the paired-row stencil is built for: 3 of 128 threads or 4 of 96 (12 warps either
+// way, within the register file at up to 168 registers per thread)
+constexpr int march2_min_ctas(int w) { return w == 128 ? MARCH2_MIN_CTAS : 4; }
 constexpr int RING2 = 9;
 constexpr int FSTR2 = RING2 * RSTR;
 constexpr size_t MARCH2_DYN_SMEM = sizeof(float) * 6 * FSTR2;   // the 9-row TMA ring
@@ -804,14 +807,14 @@ struct Kahan2 {
     __device__ __forceinline__ double value() const { return (double(s.x) - double(c.x)) + (double(s.y) - double(c.y)); }
 };
 
-template <bool MIXED, bool ADAPT>
-__global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev* __restrict__ mems,
+template <bool MIXED, bool ADAPT, int TW>
+__global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const MemberDev* __restrict__ mems,
                                                                const int4* __restrict__ tiles, int ntiles, PassArgs pa) {
     extern __shared__ __align__(128) float ring[];   // 6 * FSTR2 floats (dynamic: the total passes 48 KB)
     __shared__ float dring[RING2 * RSTR];   // still-water depth of each ring row (same stride as the ring)
     __shared__ __align__(8) unsigned long long bars[RING2];
-    __shared__ float fW[2][2][3][MW];       // [step parity][row of the pair][hW, uW, vW][thread]
-    __shared__ float xb[2][3][MW];          // [row of the pair][component][thread]
+    __shared__ float fW[2][2][3][TW];       // [step parity][row of the pair][hW, uW, vW][thread]
+    __shared__ float xb[2][3][TW];          // [row of the pair][component][thread]
     constexpr int OFF = MIXED ? 18 : 9;
     constexpr int iR0 = OFF + 3, iH0 = OFF + 5, iAUX = OFF + 25;
     const int tid = threadIdx.x;
@@ -848,7 +851,7 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
         const int yend = min(y0 + MH, ny + 2);
         const int nsteps = (yend - y0 + 1) / 2;             // output row pairs of this strip
         const int last_row = y0 + 2 * (nsteps - 1) + 4;     // last row any step reads
-        const bool out_col = tid >= 1 && tid <= MO && xc < nx + 2;
+        const bool out_col = tid >= 1 && tid <= (TW - 2) && xc < nx + 2;
         const int xl = min(xc, c.NX - 1);
         const float dtm = *M.dtp;
         const float decay = t_pow(fabsf(c.whitewater_decay_rate), dtm);
@@ -896,7 +899,7 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
             const float* ba = BAr + off;
             float* dr = dring + off;
             dr[dcol] = fmaxf(0.f, sl - ba[dcol]);
-            const int d2c = min(dcol + MW, RBOX - 1);
+            const int d2c = min(dcol + TW, RBOX - 1);
             if (tid < 2) dr[d2c] = fmaxf(0.f, sl - ba[d2c]);
         };
 
@@ -928,7 +931,7 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
         {   // aux of row y0-1 (the ghost row y = 1 belongs to the first strip)
             const int gy = y0 - 1;
             const int cxa = xc < 2 ? 2 : xc, cya = gy < 2 ? 2 : gy;
-            if (xc >= 1 && xc < nx + 2 && gy >= 1 && cxa >= x0 && cxa < x0 + MO && cya >= y0 && cya < y0 + MH) {
+            if (xc >= 1 && xc < nx + 2 && gy >= 1 && cxa >= x0 && cxa < x0 + (TW - 2) && cya >= y0 && cya < y0 + MH) {
                 float2* a = AUX + (size_t(gy) * P + xc);
                 const float2 old = *a;
                 const float md = (((fq.hN.y + fq.hE.y) + (fq.hS.y + fq.hW.y)) * 0.25f);
@@ -970,7 +973,7 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
             for (int k = 0; k < 2; ++k) {
                 const int gy = t + 2 + k;
                 const int cxa = xc < 2 ? 2 : xc, cya = gy < 2 ? 2 : gy;
-                aux_ok[k] = xc >= 1 && xc < nx + 2 && gy >= 1 && gy < ny + 2 && cxa >= x0 && cxa < x0 + MO &&
+                aux_ok[k] = xc >= 1 && xc < nx + 2 && gy >= 1 && gy < ny + 2 && cxa >= x0 && cxa < x0 + (TW - 2) &&
                             cya >= y0 && cya < y0 + MH;
                 ap[k] = AUX + (size_t(min(gy, NYm1)) * P + xc);
                 aux_old[k] = aux_ok[k] ? *ap[k] : make_float2(0.f, 0.f);
@@ -1010,7 +1013,7 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
             face_flux2(fp.hN, fp.uN, fp.vN, P2(fp.hS1, f.hS.x), P2(fp.uS1, f.uS.x), P2(fp.vS1, f.vS.x), g, hg,
                        false, yf);
             {   // x fluxes of rows t, t+1 at this thread's east face
-                const int tn = min(tid + 1, MW - 1);
+                const int tn = min(tid + 1, TW - 1);
                 f2 xo[3];
                 face_flux2(fp.hE, fp.uE, fp.vE, P2(fW[par][0][0][tn], fW[par][1][0][tn]),
                            P2(fW[par][0][1][tn], fW[par][1][1][tn]), P2(fW[par][0][2][tn], fW[par][1][2][tn]), g,
@@ -1180,12 +1183,12 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
         seq = seq0 + unsigned(last_row - (y0 - 2) + 1);
         // ---- zero the ghost ring of the output state next to this strip (engine.cpp:1007) ----
         const int NX = c.NX, NY = c.NY;
-        const bool west = x0 == 2, east = x0 + MO >= nx + 2, south = y0 == 2, north = y0 + MH >= ny + 2;
+        const bool west = x0 == 2, east = x0 + (TW - 2) >= nx + 2, south = y0 == 2, north = y0 + MH >= ny + 2;
         if (west || east || south || north) {
-            const int cx0 = west ? 0 : x0, cx1 = east ? NX : x0 + MO;
+            const int cx0 = west ? 0 : x0, cx1 = east ? NX : x0 + (TW - 2);
             const int cy0 = south ? 0 : y0, cy1 = north ? NY : y0 + MH;
             const int w = cx1 - cx0;
-            for (int k = tid; k < w * (cy1 - cy0); k += MW) {
+            for (int k = tid; k < w * (cy1 - cy0); k += TW) {
                 const int gx = cx0 + k % w, gy = cy0 + k / w;
                 if (gx >= 2 && gx < nx + 2 && gy >= 2 && gy < ny + 2) continue;
                 const size_t gi = size_t(gy) * P + gx;
@@ -1215,7 +1218,7 @@ __global__ void __launch_bounds__(MW, MARCH2_MIN_CTAS) k_march2(const MemberDev*
             __syncthreads();
             if (tid < STATS_N - 1) {
                 double a = red[0][tid];
-                for (int w = 1; w < MW / 32; ++w) a = (tid >= 6) ? fmax(a, red[w][tid]) : a + red[w][tid];
+                for (int w = 1; w < TW / 32; ++w) a = (tid >= 6) ? fmax(a, red[w][tid]) : a + red[w][tid];
                 if (tid < 6) { if (a != 0.0) atomicAdd(M.stats + tid, a); }
                 else atomic_max_nonneg(M.stats + tid, a);
             }
@@ -2024,6 +2027,7 @@ struct cel_batch {
     int cw = 16;                        // column solver band width (columns per CTA)
     int mh = cel::MH_DEFAULT;           // stencil strip height (rows per CTA work item)
     int rows_per_step = 1;              // stencil rows per thread step: 1 (k_march) or 2 (k_march2)
+    int mw = 128;                       // stencil CTA width in threads (k_march2: 128 or 96)
     int max_nx = 0, max_ny = 0;
     bool any_log = false;               // some member has <logData> doLog set
     const float* elapsed_src = nullptr; // engine handles: the elapsed time of their latest resetTimestep
@@ -2113,6 +2117,15 @@ ColsKernel cols_kernel(bool mixed, int cw) {
     return mixed ? k_cols<true, 8> : k_cols<false, 8>;
 }
 
+using March2Kernel = void (*)(const MemberDev*, const int4*, int, PassArgs);
+March2Kernel march2_kernel(bool mixed, bool adapt, int w) {
+    if (w == 96)
+        return mixed ? (adapt ? k_march2<true, true, 96> : k_march2<true, false, 96>)
+                     : (adapt ? k_march2<false, true, 96> : k_march2<false, false, 96>);
+    return mixed ? (adapt ? k_march2<true, true, 128> : k_march2<true, false, 128>)
+                 : (adapt ? k_march2<false, true, 128> : k_march2<false, false, 128>);
+}
+
 int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
     const size_t nm = b->mem.size();
     if (pa.stats) B_TRY(cudaMemsetAsync(b->stats_all, 0, nm * STATS_N * sizeof(double), b->stream));
@@ -2120,9 +2133,8 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
         TimedLaunch t(&b->tm, b->stream, "fused_stencil");
         const bool ad = pa.scheme == CEL_SCHEME_PREDICTOR_ADAPTIVE;
         if (b->rows_per_step == 2) {
-            auto* k = b->mixed ? (ad ? k_march2<true, true> : k_march2<true, false>)
-                               : (ad ? k_march2<false, true> : k_march2<false, false>);
-            k<<<b->grid_stencil, MW, MARCH2_DYN_SMEM, b->stream>>>(b->ddev, b->mtiles, b->nmtiles, pa);
+            march2_kernel(b->mixed, ad, b->mw)<<<b->grid_stencil, b->mw, MARCH2_DYN_SMEM, b->stream>>>(
+                b->ddev, b->mtiles, b->nmtiles, pa);
         } else {
             auto* k = b->mixed ? (ad ? k_march<true, true> : k_march<true, false>)
                                : (ad ? k_march<false, true> : k_march<false, false>);
@@ -2330,9 +2342,12 @@ void byte_model(int form, int N, double& stencil, double& step) {
 
 // (Re)builds the stencil strips (height mh) and the column bands (width cw) of a batch, sizes the
 // column solver's shared memory and grids, and drops captured graphs (they hold the old lists).
-int configure_work(cel_batch* b, int cw, int mh, int rps, std::string& err) {
+int configure_work(cel_batch* b, int cw, int mh, int rps, int mw, std::string& err) {
     if (rps != 1 && rps != 2) { err = "stencil rows per step must be 1 or 2"; return CEL_ERR_ARG; }
+    if (mw != 128 && mw != 96) { err = "stencil width must be 128 or 96 threads"; return CEL_ERR_ARG; }
+    if (rps == 1) mw = MW;   // the one-row stencil has one width
     b->rows_per_step = rps;
+    const int mo = mw - 2;   // output columns per strip
     if (cw != 1 && cw != 8 && cw != 16 && cw != 32) { err = "column band width must be 1, 8, 16 or 32"; return CEL_ERR_ARG; }
     if (mh < 8 || mh > 1024) { err = "strip height must be in [8, 1024]"; return CEL_ERR_ARG; }
     const size_t smem_cols = cw == 1 ? 0 : sizeof(float) * size_t(b->max_ny) * cw;
@@ -2342,7 +2357,7 @@ int configure_work(cel_batch* b, int cw, int mh, int rps, std::string& err) {
     for (int i = 0; i < int(b->mem.size()); ++i) {
         const HostSetup& hs = b->mem[i].hs;
         for (int y0 = 2; y0 < hs.ny + 2; y0 += mh)
-            for (int x0 = 2; x0 < hs.nx + 2; x0 += MO) mt.push_back(make_int4(i, x0, y0, mh));
+            for (int x0 = 2; x0 < hs.nx + 2; x0 += mo) mt.push_back(make_int4(i, x0, y0, mh));
         if (cw == 1) {
             // one entry per column; columns 0, 1 and past nx+1 are padding (-1) so that each warp
             // covers 32 columns starting on a 128-byte boundary
@@ -2371,6 +2386,7 @@ int configure_work(cel_batch* b, int cw, int mh, int rps, std::string& err) {
     b->nbands = int(bd.size());
     b->cw = cw;
     b->mh = mh;
+    b->mw = mw;
     b->smem_cols = smem_cols;
     int occ = 1;
     if (cw == 1) {
@@ -2384,11 +2400,10 @@ int configure_work(cel_batch* b, int cw, int mh, int rps, std::string& err) {
     // both variants of the stencil (fixed and adaptive predictor) run on the same grid
     if (b->rows_per_step == 2) {
         occ = 1 << 20;
-        for (auto* k2 : {b->mixed ? k_march2<true, false> : k_march2<false, false>,
-                         b->mixed ? k_march2<true, true> : k_march2<false, true>}) {
+        for (auto* k2 : {march2_kernel(b->mixed, false, mw), march2_kernel(b->mixed, true, mw)}) {
             int o = 0;
             B_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, int(MARCH2_DYN_SMEM)));
-            B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k2, MW, MARCH2_DYN_SMEM));
+            B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k2, mw, MARCH2_DYN_SMEM));
             occ = std::min(occ, o);
         }
     } else {
@@ -2647,7 +2662,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     }
     {   // column bands of 16 columns (8 for tall domains: shared-memory capacity), strips of 64 rows
         const int cw = (size_t(max_ny) * 16 * sizeof(float) + 8192 <= 227 * 1024) ? 16 : 8;
-        if (configure_work(b.get(), cw, MH_DEFAULT, 1, err)) return nullptr;
+        if (configure_work(b.get(), cw, MH_DEFAULT, 1, MW, err)) return nullptr;
     }
     b->sch.reset(*params[0]);
     cudaMemcpy(b->dt_table, b->dt_host, sizeof(float) * n, cudaMemcpyHostToDevice);
@@ -2864,7 +2879,7 @@ int batch_set_timestep(cel_batch* b, const float* dt, std::string& err) {
 
 int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err) {
     (void)pcr;   // the solves have no cyclic-reduction stage to hand over from (Thomas factors + scans)
-    return configure_work(b, tx > 0 ? tx : b->cw, ty > 0 ? ty : b->mh, b->rows_per_step, err);
+    return configure_work(b, tx > 0 ? tx : b->cw, ty > 0 ? ty : b->mh, b->rows_per_step, b->mw, err);
 }
 
 int batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rps) {
@@ -2875,19 +2890,29 @@ int batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rps) {
 }
 
 int batch_set_stencil_rows(cel_batch* b, int rps, std::string& err) {
-    return configure_work(b, b->cw, b->mh, rps, err);
+    return configure_work(b, b->cw, b->mh, rps, rps == 2 ? b->mw : MW, err);
 }
+
+int batch_set_stencil_width(cel_batch* b, int threads, std::string& err) {
+    if (b->rows_per_step != 2 && threads != MW) {
+        err = "the one-row stencil runs 128-thread strips; select two rows per step first";
+        return CEL_ERR_ARG;
+    }
+    return configure_work(b, b->cw, b->mh, b->rows_per_step, threads, err);
+}
+
+int batch_stencil_width(const cel_batch* b) { return b->mw; }
 
 // Times `steps` physical steps for every candidate (band width, strip height), in the launch mode
 // the batch is set to (graph replay or direct), two rounds in turn, and keeps the fastest by its
 // better round.  The ensemble advances by every step taken here.
 int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, std::string& err) {
     if (steps < 1) { err = "autotune needs at least one step per candidate"; return CEL_ERR_ARG; }
-    std::vector<int3> cand;
-    for (int rps : {1, 2})
+    std::vector<int4> cand;   // band width, strip height, stencil rows per step, stencil width
+    for (int2 v : {make_int2(1, 128), make_int2(2, 128), make_int2(2, 96)})
         for (int cw : {1, 8, 16, 32})
             if (cw == 1 || sizeof(float) * size_t(b->max_ny) * cw + 8192 <= 227 * 1024)
-                for (int mh : {32, 64, 128}) cand.push_back(make_int3(cw, mh, rps));
+                for (int mh : {32, 64, 128}) cand.push_back(make_int4(cw, mh, v.x, v.y));
     std::vector<double> best(cand.size(), 1e300);
     cudaEvent_t e0, e1;
     B_TRY(cudaEventCreate(&e0));
@@ -2895,7 +2920,7 @@ int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, s
     int rc = CEL_OK;
     for (int round = 0; round < 2 && !rc; ++round)
         for (size_t k = 0; k < cand.size() && !rc; ++k) {
-            if ((rc = configure_work(b, cand[k].x, cand[k].y, cand[k].z, err))) break;
+            if ((rc = configure_work(b, cand[k].x, cand[k].y, cand[k].z, cand[k].w, err))) break;
             if ((rc = batch_step(b, 2, err))) break;   // warm-up (captures the graphs in graph mode)
             cudaEventRecord(e0, b->stream);
             if ((rc = batch_step(b, steps, err))) break;
@@ -2909,7 +2934,7 @@ int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, s
     cudaEventDestroy(e1);
     if (rc) return rc;
     const size_t kb = size_t(std::min_element(best.begin(), best.end()) - best.begin());
-    if ((rc = configure_work(b, cand[kb].x, cand[kb].y, cand[kb].z, err))) return rc;
+    if ((rc = configure_work(b, cand[kb].x, cand[kb].y, cand[kb].z, cand[kb].w, err))) return rc;
     if (tx) *tx = cand[kb].x;
     if (ty) *ty = cand[kb].y;
     if (best_ms) *best_ms = best[kb];

@@ -252,9 +252,13 @@ int cel_batch_get_tuning(const cel_batch* b, int* tile_x, int* tile_y, int* rows
 /* Stencil variant: 1 = one row per thread step; 2 = two rows per step as pairs, with the paired
  * single-precision instructions of sm_100 (f32x2). */
 int cel_batch_set_stencil_rows(cel_batch* b, int rows_per_step);
+/* Threads per stencil CTA, i.e. strip width + 2 halo columns: 128 or 96 (96 with two rows per step
+ * only).  Narrower strips waste fewer lanes on members whose width is not a multiple of 126. */
+int cel_batch_set_stencil_width(cel_batch* b, int threads);
+int cel_batch_stencil_width(const cel_batch* b);
 /* Times `steps` physical steps for each candidate (band width x strip height x stencil rows per
- * step) and keeps the
- * fastest; writes the choice and its ms per step.  The members advance by every timed step. */
+ * step x stencil width) and keeps the fastest; writes the choice and its ms per step.  The
+ * members advance by every timed step. */
 int cel_batch_autotune(cel_batch* b, int steps, int* tile_x, int* tile_y, double* ms_per_step);
 /* Per-kernel CUDA-event timing on the launching stream (off by default). */
 int cel_batch_kernel_timing(cel_batch* b, int enable);

@@ -302,3 +302,28 @@ def test_spectrum_wavemaker(celeris, form):
         ref = O.Oracle(p, z, bnx, bny, "f64")
         ref.physical_steps(120)
         assert eta_rms(a, ref.state()) <= 1e-4
+
+
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+def test_stencil_width_changes_decomposition_not_results(celeris, form):
+    """96-thread strips (94 columns) against 128-thread strips (126 columns): every cell is computed
+    by the same arithmetic, so the states and aux are identical; the statistics only regroup their
+    sums (different partial sums per strip)."""
+    members = [_case(k, nx=nx, ny=ny, N=1)[:4]
+               for k, nx, ny in (("mixed", 130, 41), ("sponge", 256, 33), ("irregular", 95, 64), ("uts", 190, 20))]
+    b1 = celeris.Batch([(m[0], m[1]) for m in members], form)
+    b2 = celeris.Batch([(m[0], m[1]) for m in members], form)
+    for b in (b1, b2):
+        b.set_stencil_rows(2)
+    b2.set_stencil_width(96)
+    assert (b1.stencil_width, b2.stencil_width) == (128, 96)
+    b1.step(30)
+    b2.step(30)
+    for i in range(len(members)):
+        np.testing.assert_array_equal(b2.state(i), b1.state(i))
+        np.testing.assert_array_equal(b2.aux(i), b1.aux(i))
+    for x, y in zip(b1.stats(), b2.stats()):
+        assert y["mass_full"] == pytest.approx(x["mass_full"], rel=1e-12)
+        assert y["max_depth"] == x["max_depth"]
+    with pytest.raises(celeris.CelError):
+        b1.set_stencil_width(64)
