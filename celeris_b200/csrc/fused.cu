@@ -43,7 +43,12 @@ namespace cel {
 namespace {
 
 constexpr int TX = 32, TY = 16;
-constexpr int NTC = 512;                     // column solver threads: CWT columns x (512/CWT) chunks
+constexpr int NTC = 512;
+// column solver CTAs per SM the build targets: 2 (64 registers, no spills); 1 lets the compiler take
+// about 100 registers and run one CTA per SM, 3 spills (measured on C4: 8.9 / 10.3 / 9.2 Gcell-steps/s)
+#ifndef CEL_COLS_MIN_CTAS
+#define CEL_COLS_MIN_CTAS 2
+#endif                     // column solver threads: CWT columns x (512/CWT) chunks
 constexpr int STATS_N = 12;
 
 // stats accumulator layout
@@ -1453,7 +1458,7 @@ __global__ void __launch_bounds__(256) k_rows(const MemberDev* __restrict__ mems
 }
 
 template <bool MIXED, int CW>
-__global__ void __launch_bounds__(NTC) k_cols(const MemberDev* __restrict__ mems, const int2* __restrict__ bands,
+__global__ void __launch_bounds__(NTC, CEL_COLS_MIN_CTAS) k_cols(const MemberDev* __restrict__ mems, const int2* __restrict__ bands,
                                               int nbands, PassArgs pa) {
     // Column (y) solves: a CTA takes a band of CW adjacent columns, thread (c, k) runs chunk k of
     // column c; a half warp reads CW consecutive floats of one row.  Every loop over a chunk's rows
