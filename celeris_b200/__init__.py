@@ -118,6 +118,11 @@ class Engine:
     def add_solitary_wave(self, H: float, theta_deg: float, xc: float, yc: float):
         check(lib().cel_add_solitary_wave(self.h, H, theta_deg, xc, yc))
 
+    def set_bathymetry(self, z: np.ndarray):
+        """newTerrainSettings with a new bathymetry grid (the .cbf layout, rows = y)."""
+        z = np.ascontiguousarray(z, dtype=np.float32)
+        check(lib().cel_set_bathymetry(self.h, _fp(z), z.shape[1], z.shape[0]))
+
     def synchronize(self):
         check(lib().cel_synchronize(self.h))
 
@@ -215,6 +220,10 @@ class Batch:
         out = np.zeros(self.shapes[i] + (4,), dtype=np.float32)
         check(lib().cel_batch_get_aux(self.h, i, _fp(out)))
         return out
+
+    def set_bathymetry(self, i: int, z: np.ndarray):
+        z = np.ascontiguousarray(z, dtype=np.float32)
+        check(lib().cel_batch_set_bathymetry(self.h, i, _fp(z), z.shape[1], z.shape[0]))
 
     def set_tuning(self, band_width: int = 0, strip_height: int = 0):
         """Column-solver band width (8/16/32) and stencil strip height (0 keeps the current value)."""

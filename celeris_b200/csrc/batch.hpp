@@ -21,6 +21,7 @@ int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err);
 int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err);
 int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err);
 int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err);
+int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, std::string& err);
 int batch_use_graph(cel_batch* b, bool enable, std::string& err);
 long long batch_cells(const cel_batch* b);
 int batch_set_timestep(cel_batch* b, const float* dt, std::string& err);

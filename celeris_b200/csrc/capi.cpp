@@ -319,6 +319,11 @@ int cel_get_water_height(cel_engine* h, float x, float y, float* out) {
     return CEL_OK;
     CEL_GUARD_END
 }
+int cel_set_bathymetry(cel_engine* h, const float* bathy, int bnx, int bny) {
+    ENG(h);
+    if (!bathy || bnx < 2 || bny < 2) { set_error("bathymetry grid needs at least 2 x 2 values"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN return ret(e, e->set_bathymetry(bathy, bnx, bny)); CEL_GUARD_END
+}
 int cel_synchronize(cel_engine* h) { ENG(h); CEL_GUARD_BEGIN return ret(e, e->synchronize()); CEL_GUARD_END }
 int cel_set_tuning(cel_engine* h, int tx, int ty, int pcr) {
     ENG(h);
@@ -374,6 +379,10 @@ int cel_batch_set_state(cel_batch* b, int i, const float* rgba) {
     BAT(b);
     if (!rgba) { set_error("null buffer"); return CEL_ERR_ARG; }
     CEL_GUARD_BEGIN BRET(cel::batch_set_state(b, i, rgba, err)); CEL_GUARD_END
+}
+int cel_batch_set_bathymetry(cel_batch* b, int i, const float* bathy, int bnx, int bny) {
+    BAT(b);
+    CEL_GUARD_BEGIN BRET(cel::batch_set_bathymetry(b, i, bathy, bnx, bny, err)); CEL_GUARD_END
 }
 int cel_batch_get_aux(cel_batch* b, int i, float* rgba) {
     BAT(b);

@@ -47,6 +47,8 @@ public:
     virtual int physical_steps(int n) = 0;
     virtual int get_stats(cel_stats* out) = 0;
     virtual int add_solitary_wave(double H, double theta_deg, double xc, double yc) = 0;
+    // newTerrainSettings (engine.cpp:820-823, 3313-3379) with a new bathymetry grid
+    virtual int set_bathymetry(const float* z, int bnx, int bny) = 0;
     virtual int set_stream(cudaStream_t s) = 0;
     virtual int synchronize() = 0;
     virtual int set_tuning(int tx, int ty, int pcr) = 0;

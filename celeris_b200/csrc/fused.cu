@@ -2843,6 +2843,45 @@ int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err) {
     return upload_state(b, i, rgba, err);
 }
 
+// newTerrainSettings for member i (engine.cpp:3313-3379): every texel keeps its water depth
+// (w - BA_old + BA_new; in double on the compensated state of the mixed form), the bottom planes
+// are resampled from the new grid, the aux planes are cleared; the Thomas factors stay those of
+// the old bottom, as the reference keeps its coefficient textures until a remesh.
+int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, std::string& err) {
+    if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
+    if (!z || bnx < 2 || bny < 2) { err = "bathymetry grid needs at least 2 x 2 values"; return CEL_ERR_ARG; }
+    Member& m = b->mem[i];
+    MemberDev& d = b->hdev[i];
+    const int NX = m.hs.NX, NY = m.hs.NY, sin = b->ix.sin;
+    B_TRY(cudaStreamSynchronize(b->stream));
+    std::vector<float> hi(m.plane), lo(b->mixed ? m.plane : 0);
+    B_TRY(cudaMemcpy(hi.data(), d.S[sin][0], m.plane * sizeof(float), cudaMemcpyDeviceToHost));
+    if (b->mixed) B_TRY(cudaMemcpy(lo.data(), d.L[sin][0], m.plane * sizeof(float), cudaMemcpyDeviceToHost));
+    const std::vector<float> ba_old = m.hs.BA;
+    prepare_bottom(z, bnx, bny, m.hs.nx, m.hs.ny, float(m.p.width), float(m.p.length), m.hs);
+    std::vector<float> by(m.plane, 0.f), bx(m.plane, 0.f), ba(m.plane, 0.f);
+    for (int y = 0; y < NY; ++y)
+        for (int x = 0; x < NX; ++x) {
+            const size_t k = size_t(y) * NX + x, e = size_t(y) * m.P + x;
+            by[e] = m.hs.BY[k]; bx[e] = m.hs.BX[k]; ba[e] = m.hs.BA[k];
+            if (b->mixed) {
+                const double w = (double(hi[e]) + double(lo[e])) - double(ba_old[k]) + double(m.hs.BA[k]);
+                hi[e] = float(w);
+                lo[e] = float(w - double(hi[e]));
+            } else {
+                hi[e] = (hi[e] - ba_old[k]) + m.hs.BA[k];
+            }
+        }
+    B_TRY(cudaMemcpy(const_cast<float*>(d.BY), by.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
+    B_TRY(cudaMemcpy(const_cast<float*>(d.BX), bx.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
+    B_TRY(cudaMemcpy(const_cast<float*>(d.BA), ba.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
+    B_TRY(cudaMemcpy(d.S[sin][0], hi.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
+    if (b->mixed) B_TRY(cudaMemcpy(d.L[sin][0], lo.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
+    B_TRY(cudaMemset(d.AUX[0], 0, 2 * m.plane * sizeof(float)));
+    b->step_stats_valid = false;   // the gathered totals describe the state before the change
+    return CEL_OK;
+}
+
 int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     Member& m = b->mem[i];
@@ -3008,6 +3047,13 @@ public:
     int add_solitary_wave(double, double, double, double) override {
         err = "cel_add_solitary_wave is available on CEL_FORM_PLAIN engines";
         return CEL_ERR_STATE;
+    }
+    int set_bathymetry(const float* z, int gx, int gy) override {
+        if (int st = batch_set_bathymetry(b, 0, z, gx, gy, err)) return st;
+        bathy.assign(z, z + size_t(gx) * gy);   // a remesh starts over from the new grid
+        bnx = gx;
+        bny = gy;
+        return CEL_OK;
     }
     int set_stream(cudaStream_t s) override { return batch_set_stream(b, s, err); }
     int synchronize() override {

@@ -518,6 +518,8 @@ public:
     int sim_idx = 0, old_i = 0, oldold_i = 1, scratch_i = 2;
     int uts_iter[4] = {1, 1, 1, 1};
     bool bootstrap_needed = true;
+    std::vector<float> terrain;   // bathymetry grid given by set_bathymetry (used by remesh)
+    int terrain_nx = 0, terrain_ny = 0;
     // stats bookkeeping for the latest device-side GetStats
     int last_stats_scheme = 0;
     float last_stats_dt = 0, last_stats_time = 0;
@@ -608,6 +610,20 @@ public:
     }
 
     int remesh() override {
+        if (!terrain.empty()) {   // the bathymetry changed since creation: rebuild from the new grid
+            HostSetup fresh;
+            if (int st0 = make_setup(p, terrain.data(), terrain_nx, terrain_ny, fresh, err)) return st0;
+            hs = fresh;
+            for (int k = 0; k < hs.Kx; ++k)
+                CEL_CUDA_TRY(cudaMemcpy(ABCx[k], hs.ABCx[k].data(), size_t(hs.lenx[k] + 4) * hs.NY * sizeof(float4),
+                                        cudaMemcpyHostToDevice));
+            for (int k = 0; k < hs.Ky; ++k)
+                CEL_CUDA_TRY(cudaMemcpy(ABCy[k], hs.ABCy[k].data(), size_t(hs.NX) * (hs.leny[k] + 4) * sizeof(float4),
+                                        cudaMemcpyHostToDevice));
+            std::vector<float4> b(ntex);
+            for (size_t i = 0; i < ntex; ++i) b[i] = make_float4(hs.BY[i], hs.BX[i], hs.BA[i], 0.f);
+            CEL_CUDA_TRY(cudaMemcpy(BOT, b.data(), ntex * sizeof(float4), cudaMemcpyHostToDevice));
+        }
         std::vector<float4> s(ntex);
         for (size_t i = 0; i < ntex; ++i) s[i] = make_float4(hs.ic[3 * i], hs.ic[3 * i + 1], hs.ic[3 * i + 2], 0.f);
         CEL_CUDA_TRY(cudaMemcpyAsync(st[0], s.data(), ntex * sizeof(float4), cudaMemcpyHostToDevice, stream));
@@ -882,6 +898,30 @@ public:
         CEL_CUDA_TRY(cudaStreamSynchronize(stream));
         return CEL_OK;
     }
+    // newTerrainSettings -> fillTerrainTexture (engine.cpp:3313-3379): keep every texel's water depth
+    // (w - BA_old + BA_new, in float as there), resample the bottom, clear both aux textures and
+    // re-bootstrap.  The tridiagonal coefficients stay those of the old bottom until cel_remesh,
+    // which rebuilds everything from the new grid (remesh re-creates the coefficient textures).
+    int set_bathymetry(const float* z, int bnx, int bny) override {
+        std::vector<float> host(ntex * 4);
+        if (int e = get_state(host.data())) return e;
+        for (size_t k = 0; k < ntex; ++k) host[4 * k] -= hs.BA[k];
+        prepare_bottom(z, bnx, bny, hs.nx, hs.ny, float(p.width), float(p.length), hs);
+        for (size_t k = 0; k < ntex; ++k) host[4 * k] += hs.BA[k];
+        std::vector<float4> b(ntex);
+        for (size_t i = 0; i < ntex; ++i) b[i] = make_float4(hs.BY[i], hs.BX[i], hs.BA[i], 0.f);
+        CEL_CUDA_TRY(cudaMemcpyAsync(BOT, b.data(), ntex * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        CEL_CUDA_TRY(cudaMemcpyAsync(st[sim_idx], host.data(), ntex * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        CEL_CUDA_TRY(cudaMemsetAsync(AUX1, 0, ntex * sizeof(float4), stream));
+        CEL_CUDA_TRY(cudaMemsetAsync(AUX2, 0, ntex * sizeof(float4), stream));
+        CEL_CUDA_TRY(cudaStreamSynchronize(stream));
+        terrain.assign(z, z + size_t(bnx) * bny);
+        terrain_nx = bnx;
+        terrain_ny = bny;
+        bootstrap_needed = true;
+        return CEL_OK;
+    }
+
     int add_solitary_wave(double Hh, double theta_deg, double xc, double yc) override {
         // the state texture is updated in place from a copy; faces are not rebuilt
         // (engine.cpp:2154-2219 leaves bootstrap_needed unchanged)

@@ -208,6 +208,12 @@ int cel_get_stats(cel_engine* h, cel_stats* out);
 int cel_add_solitary_wave(cel_engine* h, double H, double theta_deg, double xc, double yc);
 int cel_get_water_height(cel_engine* h, float x, float y, float* out);
 int cel_synchronize(cel_engine* h);
+/* newTerrainSettings (engine.hpp:63, engine.cpp:820-823 -> fillTerrainTexture 3313-3379): a new
+ * bathymetry grid (bnx x bny, the .cbf layout) replaces the bottom.  Every texel keeps its water
+ * depth (w - BA_old + BA_new), both aux textures are cleared and the next pass re-bootstraps.  As
+ * in the reference, the tridiagonal coefficients keep the old bottom until cel_remesh, which
+ * rebuilds everything (coefficients, initial condition) from the new grid. */
+int cel_set_bathymetry(cel_engine* h, const float* bathy, int bnx, int bny);
 
 /* ---- batched ensembles: many domains advanced by one launch per phase ------------------- */
 /* params[i] and bathy[i] (bnx[i] x bny[i]) describe member i; form is CEL_FORM_FUSED or
@@ -231,6 +237,8 @@ int cel_batch_stats_current(cel_batch* b, cel_stats* out);
 int cel_batch_get_state(cel_batch* b, int i, float* rgba);
 int cel_batch_set_state(cel_batch* b, int i, const float* rgba);
 int cel_batch_get_aux(cel_batch* b, int i, float* rgba);
+/* cel_set_bathymetry for member i (the member's Thomas factors keep the old bottom). */
+int cel_batch_set_bathymetry(cel_batch* b, int i, const float* bathy, int bnx, int bny);
 int cel_batch_use_graph(cel_batch* b, int enable);        /* capture one physical step in a CUDA graph */
 long long cel_batch_cells(const cel_batch* b);            /* sum of interior nx*ny */
 /* Per-member uniform time step (n floats), uploaded asynchronously on the batch stream; the

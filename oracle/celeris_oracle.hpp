@@ -968,6 +968,21 @@ public:
         return s;
     }
 
+    // newTerrainSettings -> fillTerrainTexture (engine.cpp:820-823, 3313-3379): the water depth of
+    // every texel is kept (w - BA_old, then + BA_new), the bottom is sampled from the new grid,
+    // both aux textures are reset (copied from a tridiagonal scratch level the engine never writes,
+    // i.e. cleared), and the next pass re-bootstraps.  The tridiagonal coefficients are not rebuilt.
+    void new_terrain(const std::vector<float>& zgrid, int bnx, int bny) {
+        std::vector<T4>& st = state[sim_idx];
+        for (size_t k = 0; k < st.size(); ++k) st[k].r -= BA[k];
+        std::vector<float> by, bx, ba;
+        prepare_bottom(zgrid, bnx, bny, nx, ny, float(p.width), float(p.length), by, bx, ba);
+        BY.assign(by.begin(), by.end()); BX.assign(bx.begin(), bx.end()); BA.assign(ba.begin(), ba.end());
+        for (auto* t : {&aux1, &aux2}) t->assign(t->size(), T4());
+        for (size_t k = 0; k < st.size(); ++k) st[k].r += BA[k];
+        bootstrap_needed = true;
+    }
+
     // AddSolitaryWave (compute.hlsl:949-976, engine.cpp:2154-2219); theta in degrees
     virtual void add_solitary_wave(double Hh, double theta_deg, double xc, double yc) {
         std::vector<T4>& st = state[sim_idx];

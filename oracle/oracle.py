@@ -55,6 +55,7 @@ def _lib(real: str) -> C.CDLL:
         L.orc_total_time.restype = C.c_double
         L.orc_passes.argtypes = [vp]
         L.orc_add_solitary_wave.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_new_terrain.argtypes = [vp, C.POINTER(C.c_float), i, i]
         L.orc_cr_solve.argtypes = [i, dp, dp, dp, dp, dp]
         L.orc_time_physical_steps.argtypes = [vp, i]
         L.orc_time_physical_steps.restype = C.c_double
@@ -148,6 +149,11 @@ class Oracle:
 
     def add_solitary_wave(self, H, theta_deg, xc, yc):
         self.L.orc_add_solitary_wave(self.h, H, theta_deg, xc, yc)
+
+    def new_terrain(self, z: np.ndarray):
+        """newTerrainSettings with a new bathymetry grid (same layout as the creation grid)."""
+        z = np.ascontiguousarray(z, dtype=np.float32)
+        self.L.orc_new_terrain(self.h, z.ctypes.data_as(C.POINTER(C.c_float)), z.shape[1], z.shape[0])
 
     def time_physical_steps(self, n: int) -> float:
         return self.L.orc_time_physical_steps(self.h, n)

@@ -170,6 +170,10 @@ int orc_time_scheme(void* h) { return static_cast<Eng*>(h)->time_scheme; }
 double orc_total_time(void* h) { return double(static_cast<Eng*>(h)->total_time); }
 int orc_passes(void* h) { return static_cast<Eng*>(h)->passes; }
 
+void orc_new_terrain(void* h, const float* bathy, int bnx, int bny) {
+    static_cast<Eng*>(h)->new_terrain(std::vector<float>(bathy, bathy + size_t(bnx) * bny), bnx, bny);
+}
+
 void orc_add_solitary_wave(void* h, double H, double theta_deg, double xc, double yc) {
     static_cast<Eng*>(h)->add_solitary_wave(H, theta_deg, xc, yc);
 }

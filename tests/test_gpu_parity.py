@@ -327,3 +327,92 @@ def test_stencil_width_changes_decomposition_not_results(celeris, form):
         assert y["max_depth"] == x["max_depth"]
     with pytest.raises(celeris.CelError):
         b1.set_stencil_width(64)
+
+
+_WIDE = {}
+
+
+def _widest_reference():
+    """FP64 oracle state of the widest case after 40 steps (computed once for both forms)."""
+    if "state" not in _WIDE:
+        p, z, bnx, bny, keep = _case("sponge", nx=16000, ny=12, N=1)
+        ref = O.Oracle(p, z, bnx, bny, "f64")
+        ref.physical_steps(40)
+        _WIDE["state"] = ref.state()
+    return _WIDE["state"]
+
+
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+def test_widest_domain(celeris, form):
+    """The widest row the fused forms accept (nx = 16000: the row solver keeps a whole row in
+    shared memory), against the FP64 oracle; one column past the limit is refused."""
+    p, z, bnx, bny, keep = _case("sponge", nx=16000, ny=12, N=1)
+    eng = celeris.Engine(p, z, form)
+    eng.physical_steps(40)
+    a = eng.state()
+    assert np.isfinite(a).all()
+    assert eta_rms(a, _widest_reference()) <= 1e-4
+    q, z2, _, _, _ = _case("sponge", nx=16001, ny=12, N=1)
+    with pytest.raises(celeris.CelError, match="nx"):
+        celeris.Engine(q, z2, form)
+
+
+def _terrain_change(z):
+    """A new bathymetry: the old one with a shoal added and the beach lowered."""
+    ny, nx = z.shape
+    X, Y = np.meshgrid(np.arange(nx), np.arange(ny))
+    return (z + 1.2 * np.exp(-((X - 0.55 * nx) ** 2 + (Y - 0.4 * ny) ** 2) / (2 * (0.1 * nx) ** 2))
+            - 0.3 * (X > 0.8 * nx)).astype(np.float32)
+
+
+@pytest.mark.parametrize("kind", ["mixed", "sponge"])
+def test_new_terrain_plain_matches_fp32_transcription(celeris, kind):
+    """newTerrainSettings mid-run (engine.cpp:3313-3379): depth kept, aux cleared, coefficients kept;
+    then a remesh rebuilds everything from the new grid."""
+    p, z, bnx, bny, keep = _case(kind, nx=48, ny=30, N=1)
+    ref = O.Oracle(p, z, bnx, bny, "f32")
+    eng = celeris.Engine(p, z, "plain")
+    ref.physical_steps(30)
+    eng.physical_steps(30)
+    z2 = _terrain_change(z)
+    ref.new_terrain(z2)
+    eng.set_bathymetry(z2)
+    np.testing.assert_array_equal(eng.bottom().astype(np.float64), ref.bottom())
+    np.testing.assert_array_equal(eng.state()[..., :3].astype(np.float64), ref.state()[..., :3])
+    assert not eng.aux()[..., 0].any()
+    ref.physical_steps(40)
+    eng.physical_steps(40)
+    np.testing.assert_array_equal(eng.state()[2:-2, 2:-2, :3].astype(np.float64), ref.state()[2:-2, 2:-2, :3])
+    # remesh: a fresh engine on the new grid
+    eng.remesh()
+    fresh = O.Oracle(p, z2, bnx, bny, "f32")
+    np.testing.assert_array_equal(eng.state()[..., :3].astype(np.float64), fresh.state()[..., :3])
+    eng.physical_steps(10)
+    fresh.physical_steps(10)
+    np.testing.assert_array_equal(eng.state()[2:-2, 2:-2, :3].astype(np.float64), fresh.state()[2:-2, 2:-2, :3])
+
+
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+def test_new_terrain_fused_forms(celeris, form):
+    p, z, bnx, bny, keep = _case("mixed", nx=70, ny=45, N=1)
+    ref = O.Oracle(p, z, bnx, bny, "f64")
+    eng = celeris.Engine(p, z, form)
+    ref.physical_steps(40)
+    eng.physical_steps(40)
+    z2 = _terrain_change(z)
+    ref.new_terrain(z2)
+    eng.set_bathymetry(z2)
+    np.testing.assert_array_equal(eng.bottom().astype(np.float64), ref.bottom())
+    ref.physical_steps(60)
+    eng.physical_steps(60)
+    assert eta_rms(eng.state(), ref.state()) <= 1e-4
+    # the same change on one member of a batch leaves the other members untouched
+    q, zq, _, _, _ = _case("sponge", nx=40, ny=24, N=1)
+    b = celeris.Batch([(p, z), (q, zq)], form)
+    solo = celeris.Batch([(q, zq)], form)
+    b.step(5)
+    solo.step(5)
+    b.set_bathymetry(0, z2)
+    b.step(5)
+    solo.step(5)
+    np.testing.assert_array_equal(b.state(1), solo.state(0))

@@ -80,3 +80,21 @@ def test_cbf_reader_reads_reference_layout(tmp_path, celeris):
 def test_live_reference_build_matches_fixture(name):
     o, _, _ = _run(name, "ref")
     np.testing.assert_array_equal(o.state().astype(np.float32), GOLD[f"{name}/state"])
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SHADER), reason="oracle/_ref not built in this tree")
+def test_terrain_change_matches_reference_shader():
+    """After a mid-run newTerrainSettings the FP32 oracle and the reference's shader build step on
+    identically (coefficients of the old bottom, new bottom textures, re-bootstrap)."""
+    p, z, bnx, bny, keep = golden_case("mixed")
+    ny, nx = z.shape
+    X, Y = np.meshgrid(np.arange(nx), np.arange(ny))
+    z2 = (z + 1.0 * np.exp(-((X - 0.5 * nx) ** 2 + (Y - 0.5 * ny) ** 2) / (2 * (0.15 * nx) ** 2))).astype(np.float32)
+    out = []
+    for real in ("f32", "ref"):
+        o = Oracle(p, z, bnx, bny, real=real)
+        o.physical_steps(10)
+        o.new_terrain(z2)
+        o.physical_steps(10)
+        out.append(o.state().astype(np.float32))
+    np.testing.assert_array_equal(out[0], out[1])
