@@ -972,7 +972,7 @@ public:
     // every texel is kept (w - BA_old, then + BA_new), the bottom is sampled from the new grid,
     // both aux textures are reset (copied from a tridiagonal scratch level the engine never writes,
     // i.e. cleared), and the next pass re-bootstraps.  The tridiagonal coefficients are not rebuilt.
-    void new_terrain(const std::vector<float>& zgrid, int bnx, int bny) {
+    virtual void new_terrain(const std::vector<float>& zgrid, int bnx, int bny) {
         std::vector<T4>& st = state[sim_idx];
         for (size_t k = 0; k < st.size(); ++k) st[k].r -= BA[k];
         std::vector<float> by, bx, ba;

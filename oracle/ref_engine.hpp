@@ -95,6 +95,12 @@ public:
     }
 
     // ---- Pass1: region [1, nx+3) x [1, ny+3) (engine.cpp:2532) -------------------------
+    // the bound bottom texture is rebuilt from the new BY/BX/BA (UpdateSubresource, engine.cpp:3349-3354)
+    void new_terrain(const std::vector<float>& zgrid, int bnx, int bny) override {
+        oracle::Engine<float>::new_terrain(zgrid, bnx, bny);
+        bottom3.clear();
+    }
+
     void pass1(const std::vector<T4>& st) override {
         set_sim_consts();
         unbind_all();
