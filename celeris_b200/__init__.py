@@ -118,6 +118,12 @@ class Engine:
     def add_solitary_wave(self, H: float, theta_deg: float, xc: float, yc: float):
         check(lib().cel_add_solitary_wave(self.h, H, theta_deg, xc, yc))
 
+    def water_height(self, x: float, y: float) -> float:
+        """getWaterHeight at world point (x, y): terrain height + the 4x4 block's mean depth."""
+        out = C.c_float()
+        check(lib().cel_get_water_height(self.h, x, y, C.byref(out)))
+        return np.float32(out.value)
+
     def set_bathymetry(self, z: np.ndarray):
         """newTerrainSettings with a new bathymetry grid (the .cbf layout, rows = y)."""
         z = np.ascontiguousarray(z, dtype=np.float32)

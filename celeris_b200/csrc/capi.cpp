@@ -297,27 +297,10 @@ int cel_add_solitary_wave(cel_engine* h, double H, double th, double xc, double 
     CEL_GUARD_BEGIN return ret(e, e->add_solitary_wave(H, th, xc, yc)); CEL_GUARD_END
 }
 int cel_get_water_height(cel_engine* h, float x, float y, float* out) {
-    // getWaterHeight: bilinear sample of w at a physical point (x in [-W/2, W/2], y in [0, L])
+    // getWaterHeight (engine.cpp:4994-5012) at a world point (x in [-W/2, W/2], y in [0, L])
     ENG(h);
     if (!out) { set_error("null buffer"); return CEL_ERR_ARG; }
-    CEL_GUARD_BEGIN
-    const int nx = e->nx(), ny = e->ny(), NX = nx + 4;
-    std::vector<float> st(size_t(NX) * (ny + 4) * 4);
-    if (int s = e->get_state(st.data())) return ret(e, s);
-    (void)x; (void)y;
-    // The engine keeps no W, L copy at this level; callers pass texel coordinates.
-    float fx = x, fy = y;
-    fx = fx < 0 ? 0 : (fx > nx + 3 ? float(nx + 3) : fx);
-    fy = fy < 0 ? 0 : (fy > ny + 3 ? float(ny + 3) : fy);
-    const int x0 = int(fx), y0 = int(fy);
-    const int x1 = x0 + 1 < NX ? x0 + 1 : x0, y1 = y0 + 1 < ny + 4 ? y0 + 1 : y0;
-    const float tx = fx - x0, ty = fy - y0;
-    auto w = [&](int xx, int yy) { return st[(size_t(yy) * NX + xx) * 4]; };
-    const float a = w(x0, y0) + tx * (w(x1, y0) - w(x0, y0));
-    const float b = w(x0, y1) + tx * (w(x1, y1) - w(x0, y1));
-    *out = a + ty * (b - a);
-    return CEL_OK;
-    CEL_GUARD_END
+    CEL_GUARD_BEGIN return ret(e, e->water_height(x, y, out)); CEL_GUARD_END
 }
 int cel_set_bathymetry(cel_engine* h, const float* bathy, int bnx, int bny) {
     ENG(h);

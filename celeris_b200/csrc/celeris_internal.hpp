@@ -47,6 +47,12 @@ struct HostSetup {
 };
 
 int count_of_matrices(int n);
+// GetTerrainHeight (terrain_heightfield.cpp:313-351): bilinear in float of the cell-centre bottom
+// BA (the terrain heightfield's B) at world point (x, y), x in [-W/2, W/2], y in [0, L], clamped.
+float terrain_height(const HostSetup& s, float W, float L, float x, float y);
+// getWaterHeight's 4x4 block (engine.cpp:5001-5006): the GetStats block of world point (x, y),
+// clamped to the block array (the reference reads past it at x = W/2 or y = L).
+void water_height_block(int nx, int ny, float W, float L, float x, float y, int& ix, int& iy);
 // terrain_heightfield.cpp:213-297 (bilinear sampling, corner averaging), in float
 void prepare_bottom(const float* z, int bnx, int bny, int nx, int ny, float W, float L, HostSetup& s);
 // engine.cpp:2612-2887

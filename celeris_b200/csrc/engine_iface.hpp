@@ -49,6 +49,9 @@ public:
     virtual int add_solitary_wave(double H, double theta_deg, double xc, double yc) = 0;
     // newTerrainSettings (engine.cpp:820-823, 3313-3379) with a new bathymetry grid
     virtual int set_bathymetry(const float* z, int bnx, int bny) = 0;
+    // getWaterHeight (engine.cpp:4994-5012): terrain height at (x, y) plus the mean depth of the
+    // GetStats 4x4 block holding the point
+    virtual int water_height(float x, float y, float* out) = 0;
     virtual int set_stream(cudaStream_t s) = 0;
     virtual int synchronize() = 0;
     virtual int set_tuning(int tx, int ty, int pcr) = 0;

@@ -3048,6 +3048,24 @@ public:
         err = "cel_add_solitary_wave is available on CEL_FORM_PLAIN engines";
         return CEL_ERR_STATE;
     }
+    // the block's depth sum is taken from the current state, in GetStats' order (compute.hlsl:1331-1345)
+    int water_height(float x, float y, float* out) override {
+        const HostSetup& hs = b->mem[0].hs;
+        const float W = float(p.width), L = float(p.length);
+        if (hs.nx < 4 || hs.ny < 4) { err = "getWaterHeight needs at least one 4x4 block"; return CEL_ERR_STATE; }
+        std::vector<float> st(size_t(hs.NX) * hs.NY * 4);
+        if (int e = batch_get_state(b, 0, st.data(), err)) return e;
+        int ix = 0, iy = 0;
+        water_height_block(hs.nx, hs.ny, W, L, x, y, ix, iy);
+        float sum_h = 0.f;
+        for (int j = 2; j < 6; ++j)
+            for (int i = 2; i < 6; ++i) {
+                const size_t k = size_t(iy * 4 + j) * hs.NX + ix * 4 + i;
+                sum_h += std::max(0.f, st[4 * k] - hs.BA[k]);
+            }
+        *out = terrain_height(hs, W, L, x, y) + sum_h / 16.0f;
+        return CEL_OK;
+    }
     int set_bathymetry(const float* z, int gx, int gy) override {
         if (int st = batch_set_bathymetry(b, 0, z, gx, gy, err)) return st;
         bathy.assign(z, z + size_t(gx) * gy);   // a remesh starts over from the new grid

@@ -922,6 +922,22 @@ public:
         return CEL_OK;
     }
 
+    // the block sum of h comes from the latest GetStats (the state of the latest resetTimestep),
+    // as the reference reads its GetStats staging texture
+    int water_height(float x, float y, float* out) override {
+        const float W = float(p.width), L = float(p.length);
+        if (hs.nx < 4 || hs.ny < 4) { err = "getWaterHeight needs at least one 4x4 block"; return CEL_ERR_STATE; }
+        if (!sch.initialized) { if (int e = reset_timestep(0.f, 0.f, nullptr)) return e; }
+        int ix = 0, iy = 0;
+        water_height_block(hs.nx, hs.ny, W, L, x, y, ix, iy);
+        float sum_h = 0.f;
+        CEL_CUDA_TRY(cudaMemcpyAsync(&sum_h, blocks + (size_t(iy) * (hs.nx / 4) + ix) * 9, sizeof(float),
+                                     cudaMemcpyDeviceToHost, stream));
+        CEL_CUDA_TRY(cudaStreamSynchronize(stream));
+        *out = terrain_height(hs, W, L, x, y) + sum_h / 16.0f;
+        return CEL_OK;
+    }
+
     int add_solitary_wave(double Hh, double theta_deg, double xc, double yc) override {
         // the state texture is updated in place from a copy; faces are not rebuilt
         // (engine.cpp:2154-2219 leaves bootstrap_needed unchanged)

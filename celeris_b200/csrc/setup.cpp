@@ -40,6 +40,30 @@ float sample(const float* z, int bnx, int bny, float W, float L, float x, float 
 
 }  // namespace
 
+float terrain_height(const HostSetup& s, float W, float L, float x, float y) {
+    const int width = s.nx, height = s.ny;
+    x = (x + W / 2) / W * float(width - 1);
+    y = y / L * float(height - 1);
+    x = x < 0 ? 0.f : (x > float(width - 1) ? float(width - 1) : x);
+    y = y < 0 ? 0.f : (y > float(height - 1) ? float(height - 1) : y);
+    x += 2;
+    y += 2;
+    const int xd = int(std::floor(x)), xu = int(std::ceil(x)), yd = int(std::floor(y)), yu = int(std::ceil(y));
+    const float xf = x - float(xd), yf = y - float(yd);
+    const int pitch = width + 4;
+    auto B = [&](int xx, int yy) { return s.BA[size_t(yy) * pitch + xx]; };
+    auto lerp = [](float t, float dn, float up) { return dn + t * (up - dn); };
+    return lerp(yf, lerp(xf, B(xd, yd), B(xu, yd)), lerp(xf, B(xd, yu), B(xu, yu)));
+}
+
+void water_height_block(int nx, int ny, float W, float L, float x, float y, int& ix, int& iy) {
+    const float tx = (x + W / 2) / W, ty = y / L;
+    ix = int(tx * float(nx / 4));
+    iy = int(ty * float(ny / 4));
+    ix = ix < 0 ? 0 : (ix > nx / 4 - 1 ? nx / 4 - 1 : ix);
+    iy = iy < 0 ? 0 : (iy > ny / 4 - 1 ? ny / 4 - 1 : iy);
+}
+
 void prepare_bottom(const float* z, int bnx, int bny, int nx, int ny, float W, float L, HostSetup& s) {
     const int NX = nx + 4, NY = ny + 4;
     s.corners.assign(size_t(NX + 1) * (NY + 1), 0.f);

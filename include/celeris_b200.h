@@ -206,6 +206,12 @@ int cel_physical_steps(cel_engine* h, int n);
 /* latest device-side stats (copies to host; synchronizes the stream) */
 int cel_get_stats(cel_engine* h, cel_stats* out);
 int cel_add_solitary_wave(cel_engine* h, double H, double theta_deg, double xc, double yc);
+/* getWaterHeight (engine.cpp:4994-5012): the water surface at world point (x, y), x in
+ * [-W/2, W/2], y in [0, L], as the terrain height there (GetTerrainHeight, a float bilinear of BA)
+ * plus the mean depth of the GetStats 4x4 block holding the point.  The plain form takes the block
+ * from its latest GetStats (the state of the latest resetTimestep), as the reference reads its
+ * staging texture; the fused forms sum the block of the current state.  Points on the far edges
+ * use the last block (the reference reads past its block array there). */
 int cel_get_water_height(cel_engine* h, float x, float y, float* out);
 int cel_synchronize(cel_engine* h);
 /* newTerrainSettings (engine.hpp:63, engine.cpp:820-823 -> fillTerrainTexture 3313-3379): a new

@@ -416,3 +416,44 @@ def test_new_terrain_fused_forms(celeris, form):
     b.step(5)
     solo.step(5)
     np.testing.assert_array_equal(b.state(1), solo.state(0))
+
+
+def _water_height_expected(state, bottom, p, x, y):
+    """getWaterHeight (engine.cpp:4994-5012) restated in float32: GetTerrainHeight's bilinear of BA
+    (terrain_heightfield.cpp:313-351) plus the 4x4 block's sum of h (GetStats order) / 16."""
+    f = np.float32
+    nx, ny, W, L = p.nx, p.ny, f(p.width), f(p.length)
+    BA = bottom[..., 2].astype(np.float32)
+    tx = f(f(f(x) + W / f(2)) / W * f(nx - 1))
+    ty = f(f(y) / L * f(ny - 1))
+    tx, ty = f(min(max(tx, f(0)), f(nx - 1)) + f(2)), f(min(max(ty, f(0)), f(ny - 1)) + f(2))
+    xd, xu, yd, yu = int(np.floor(tx)), int(np.ceil(tx)), int(np.floor(ty)), int(np.ceil(ty))
+    xf, yf = f(tx - f(xd)), f(ty - f(yd))
+    lerp = lambda t, a, b: f(a + f(t * f(b - a)))
+    terrain = lerp(yf, lerp(xf, BA[yd, xd], BA[yd, xu]), lerp(xf, BA[yu, xd], BA[yu, xu]))
+    ix = int(f(f(f(x) + W / f(2)) / W) * f(nx // 4))
+    iy = int(f(f(y) / L) * f(ny // 4))
+    ix, iy = min(max(ix, 0), nx // 4 - 1), min(max(iy, 0), ny // 4 - 1)
+    s = f(0)
+    for j in range(2, 6):
+        for i in range(2, 6):
+            yy, xx = iy * 4 + j, ix * 4 + i
+            s = f(s + max(f(0), f(state[yy, xx, 0] - BA[yy, xx])))
+    return f(terrain + f(s / f(16)))
+
+
+@pytest.mark.parametrize("form", ["plain", "mixed"])
+def test_water_height_follows_get_water_height(celeris, form):
+    p, z, bnx, bny, keep = _case("mixed", nx=48, ny=32, N=1)
+    eng = celeris.Engine(p, z, form)
+    eng.physical_steps(20)
+    eng.reset_timestep()
+    st, bot = eng.state(), eng.bottom()
+    W, L = p.width, p.length
+    for x, y in [(0.0, 0.5 * L), (-0.3 * W, 0.21 * L), (0.41 * W, 0.77 * L), (-W / 2, 0.0), (W / 2, L)]:
+        want = _water_height_expected(st, bot, p, x, y)
+        got = eng.water_height(x, y)
+        if form == "plain":
+            assert got == want, (x, y, got, want)
+        else:
+            assert got == pytest.approx(float(want), rel=1e-6, abs=1e-6), (x, y)
