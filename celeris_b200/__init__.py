@@ -227,6 +227,9 @@ class Batch:
         check(lib().cel_batch_get_aux(self.h, i, _fp(out)))
         return out
 
+    def add_solitary_wave(self, i: int, H: float, theta_deg: float, xc: float, yc: float):
+        check(lib().cel_batch_add_solitary_wave(self.h, i, H, theta_deg, xc, yc))
+
     def set_bathymetry(self, i: int, z: np.ndarray):
         z = np.ascontiguousarray(z, dtype=np.float32)
         check(lib().cel_batch_set_bathymetry(self.h, i, _fp(z), z.shape[1], z.shape[0]))

@@ -178,6 +178,7 @@ def _declare(L: C.CDLL) -> None:
         "cel_synchronize": (i, [vp]),
         "cel_set_bathymetry": (i, [vp, fp, i, i]),
         "cel_batch_set_bathymetry": (i, [vp, i, fp, i, i]),
+        "cel_batch_add_solitary_wave": (i, [vp, i, C.c_double, C.c_double, C.c_double, C.c_double]),
         "cel_batch_create": (i, [i, C.POINTER(C.POINTER(Params)), C.POINTER(fp), C.POINTER(i),
                                  C.POINTER(i), i, C.POINTER(vp)]),
         "cel_batch_destroy": (i, [vp]),
@@ -231,7 +232,7 @@ EXPORTED = [
     "cel_set_state", "cel_get_state", "cel_get_bottom", "cel_get_aux",
     "cel_reset_timestep", "cel_timestep", "cel_timesteps", "cel_physical_steps", "cel_get_stats",
     "cel_add_solitary_wave", "cel_get_water_height", "cel_synchronize", "cel_set_bathymetry",
-    "cel_batch_set_bathymetry",
+    "cel_batch_set_bathymetry", "cel_batch_add_solitary_wave",
     "cel_batch_create", "cel_batch_destroy", "cel_batch_set_stream", "cel_batch_step",
     "cel_batch_stats", "cel_batch_stats_current", "cel_batch_get_state", "cel_batch_set_state", "cel_batch_get_aux",
     "cel_batch_use_graph", "cel_batch_cells", "cel_batch_set_timestep", "cel_batch_launches_per_step", "cel_set_tuning", "cel_batch_set_tuning",

@@ -22,6 +22,7 @@ int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err);
 int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err);
 int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err);
 int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, std::string& err);
+int batch_add_solitary_wave(cel_batch* b, int i, double H, double theta_deg, double xc, double yc, std::string& err);
 int batch_use_graph(cel_batch* b, bool enable, std::string& err);
 long long batch_cells(const cel_batch* b);
 int batch_set_timestep(cel_batch* b, const float* dt, std::string& err);

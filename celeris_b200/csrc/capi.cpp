@@ -363,6 +363,10 @@ int cel_batch_set_state(cel_batch* b, int i, const float* rgba) {
     if (!rgba) { set_error("null buffer"); return CEL_ERR_ARG; }
     CEL_GUARD_BEGIN BRET(cel::batch_set_state(b, i, rgba, err)); CEL_GUARD_END
 }
+int cel_batch_add_solitary_wave(cel_batch* b, int i, double H, double th, double xc, double yc) {
+    BAT(b);
+    CEL_GUARD_BEGIN BRET(cel::batch_add_solitary_wave(b, i, H, th, xc, yc, err)); CEL_GUARD_END
+}
 int cel_batch_set_bathymetry(cel_batch* b, int i, const float* bathy, int bnx, int bny) {
     BAT(b);
     CEL_GUARD_BEGIN BRET(cel::batch_set_bathymetry(b, i, bathy, bnx, bny, err)); CEL_GUARD_END

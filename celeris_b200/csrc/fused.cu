@@ -1849,6 +1849,40 @@ __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ 
     }
 }
 
+// AddSolitaryWave (compute.hlsl:949-976) on member i's state buffer `buf`: every texel of
+// [1, nx+3) x [1, ny+3) adds the sech^2 wave of its own water depth (the draw region of
+// engine.cpp:2154-2219).  Each texel reads only itself, so the update runs in place; the
+// transcendentals run in double.
+template <bool MIXED>
+__global__ void k_add_solitary(const MemberDev* __restrict__ mems, int i, int buf, float H, float th, float xc, float yc) {
+    const MemberDev& M = mems[i];
+    const SimConsts& c = M.c;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (x >= c.nx + 3 || y >= c.ny + 3) return;
+    const size_t gi = size_t(y) * M.P + x;
+    float* W = M.S[buf][0];
+    float* HU = M.S[buf][1];
+    float* HV = M.S[buf][2];
+    const double w = double(W[gi]) + (MIXED ? double(M.L[buf][0][gi]) : 0.0);
+    const double depth = fmax(w - double(M.BA[gi]), 0.0);
+    const double K = sqrt(0.75 * fabs(double(H)) / (depth * depth * depth));
+    const double C = sqrt(double(c.g) * (double(H) + depth));
+    const double ch = cosh(K * ((double(x) * c.dx - xc) * cos(double(th)) + (double(y) * c.dy - yc) * sin(double(th))));
+    const double e = double(H) / (ch * ch);
+    const float de = float(e), du = float(C * cos(double(th)) * e), dv = float(C * sin(double(th)) * e);
+    if (MIXED) {
+        float hi = W[gi], lo = M.L[buf][0][gi];
+        two_sum_add(hi, lo, de); W[gi] = hi; M.L[buf][0][gi] = lo;
+        hi = HU[gi]; lo = M.L[buf][1][gi];
+        two_sum_add(hi, lo, du); HU[gi] = hi; M.L[buf][1][gi] = lo;
+        hi = HV[gi]; lo = M.L[buf][2][gi];
+        two_sum_add(hi, lo, dv); HV[gi] = hi; M.L[buf][2][gi] = lo;
+    } else {
+        W[gi] += de; HU[gi] += du; HV[gi] += dv;
+    }
+}
+
 // Per-member time-step controller of an adaptive batch: resetTimestep's dt logic
 // (engine.cpp:1698-1726) kept on the device, so a physical step needs no host readback and can
 // be replayed from a CUDA graph.  Single precision with IEEE-rounded operations, as the reference's
@@ -2882,6 +2916,22 @@ int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, 
     return CEL_OK;
 }
 
+// addSolitaryWave (engine.cpp:2154-2219) on member i; theta in degrees
+int batch_add_solitary_wave(cel_batch* b, int i, double H, double theta_deg, double xc, double yc, std::string& err) {
+    if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
+    const HostSetup& hs = b->mem[i].hs;
+    const float th = float(theta_deg) * 3.14159274101257324f / 180.0f;
+    const dim3 blk(32, 8), grd((hs.nx + 2 + 31) / 32, (hs.ny + 2 + 7) / 8);
+    if (b->mixed)
+        k_add_solitary<true><<<grd, blk, 0, b->stream>>>(b->ddev, i, b->ix.sin, float(H), th, float(xc), float(yc));
+    else
+        k_add_solitary<false><<<grd, blk, 0, b->stream>>>(b->ddev, i, b->ix.sin, float(H), th, float(xc), float(yc));
+    B_TRY(cudaGetLastError());
+    B_TRY(cudaStreamSynchronize(b->stream));
+    b->step_stats_valid = false;
+    return CEL_OK;
+}
+
 int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     Member& m = b->mem[i];
@@ -3044,9 +3094,8 @@ public:
     }
     int physical_steps(int n) override { return batch_step(b, n, err); }
     int get_stats(cel_stats* out) override { return batch_stats(b, out, true, err); }
-    int add_solitary_wave(double, double, double, double) override {
-        err = "cel_add_solitary_wave is available on CEL_FORM_PLAIN engines";
-        return CEL_ERR_STATE;
+    int add_solitary_wave(double Hh, double theta_deg, double xc, double yc) override {
+        return batch_add_solitary_wave(b, 0, Hh, theta_deg, xc, yc, err);
     }
     // the block's depth sum is taken from the current state, in GetStats' order (compute.hlsl:1331-1345)
     int water_height(float x, float y, float* out) override {

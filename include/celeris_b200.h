@@ -205,6 +205,9 @@ int cel_timesteps(cel_engine* h, int n);
 int cel_physical_steps(cel_engine* h, int n);
 /* latest device-side stats (copies to host; synchronizes the stream) */
 int cel_get_stats(cel_engine* h, cel_stats* out);
+/* addSolitaryWave (engine.cpp:2154-2219, AddSolitaryWave pass compute.hlsl:949-976): adds a sech^2
+ * wave of height H, direction theta_deg and centre (xc, yc) (texel-index coordinates x dx, y dy)
+ * to the current state, each texel with its own water depth. */
 int cel_add_solitary_wave(cel_engine* h, double H, double theta_deg, double xc, double yc);
 /* getWaterHeight (engine.cpp:4994-5012): the water surface at world point (x, y), x in
  * [-W/2, W/2], y in [0, L], as the terrain height there (GetTerrainHeight, a float bilinear of BA)
@@ -243,6 +246,8 @@ int cel_batch_stats_current(cel_batch* b, cel_stats* out);
 int cel_batch_get_state(cel_batch* b, int i, float* rgba);
 int cel_batch_set_state(cel_batch* b, int i, const float* rgba);
 int cel_batch_get_aux(cel_batch* b, int i, float* rgba);
+/* cel_add_solitary_wave for member i */
+int cel_batch_add_solitary_wave(cel_batch* b, int i, double H, double theta_deg, double xc, double yc);
 /* cel_set_bathymetry for member i (the member's Thomas factors keep the old bottom). */
 int cel_batch_set_bathymetry(cel_batch* b, int i, const float* bathy, int bnx, int bny);
 int cel_batch_use_graph(cel_batch* b, int enable);        /* capture one physical step in a CUDA graph */

@@ -457,3 +457,29 @@ def test_water_height_follows_get_water_height(celeris, form):
             assert got == want, (x, y, got, want)
         else:
             assert got == pytest.approx(float(want), rel=1e-6, abs=1e-6), (x, y)
+
+
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+def test_add_solitary_wave_fused_forms(celeris, form):
+    """addSolitaryWave mid-run (engine.cpp:2154-2219) in the fused forms against the FP64 oracle,
+    and on one batch member without touching the others."""
+    p, z, bnx, bny, keep = _case("solid", nx=70, ny=45, N=1)
+    ref = O.Oracle(p, z, bnx, bny, "f64")
+    eng = celeris.Engine(p, z, form)
+    ref.physical_steps(20)
+    eng.physical_steps(20)
+    ref.add_solitary_wave(0.3, 25.0, 30.0, 20.0)
+    eng.add_solitary_wave(0.3, 25.0, 30.0, 20.0)
+    assert eta_rms(eng.state(), ref.state()) <= 1e-6
+    ref.physical_steps(40)
+    eng.physical_steps(40)
+    assert eta_rms(eng.state(), ref.state()) <= 1e-4
+    q, zq, _, _, _ = _case("sponge", nx=40, ny=24, N=1)
+    b = celeris.Batch([(p, z), (q, zq)], form)
+    solo = celeris.Batch([(q, zq)], form)
+    b.step(3)
+    solo.step(3)
+    b.add_solitary_wave(0, 0.3, 25.0, 30.0, 20.0)
+    b.step(3)
+    solo.step(3)
+    np.testing.assert_array_equal(b.state(1), solo.state(0))
