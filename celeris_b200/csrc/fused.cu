@@ -2381,6 +2381,21 @@ void byte_model(int form, int N, double& stencil, double& step) {
 
 // (Re)builds the stencil strips (height mh) and the column bands (width cw) of a batch, sizes the
 // column solver's shared memory and grids, and drops captured graphs (they hold the old lists).
+// Lets `kernel` take as much dynamic shared memory as the device allows beside its static shared
+// memory.  The limit is an attribute of the function for the whole process, so setting it to one
+// batch's need would refuse the larger launches of another live batch; the launches themselves
+// still request only what their batch needs (occupancy follows the request, not the limit).
+cudaError_t allow_max_dynamic_smem(const void* kernel) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - int(fa.sharedSizeBytes));
+    return e;
+}
+
 int configure_work(cel_batch* b, int cw, int mh, int rps, int mw, std::string& err) {
     if (rps != 1 && rps != 2) { err = "stencil rows per step must be 1 or 2"; return CEL_ERR_ARG; }
     if (mw != 128 && mw != 96) { err = "stencil width must be 128 or 96 threads"; return CEL_ERR_ARG; }
@@ -2432,7 +2447,7 @@ int configure_work(cel_batch* b, int cw, int mh, int rps, int mw, std::string& e
         b->grid_cols = (b->nbands + 127) / 128;
     } else {
         ColsKernel kc = cols_kernel(b->mixed, cw);
-        B_TRY(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_cols)));
+        B_TRY(allow_max_dynamic_smem(reinterpret_cast<const void*>(kc)));
         B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc, NTC, smem_cols));
         b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
     }
@@ -2441,7 +2456,7 @@ int configure_work(cel_batch* b, int cw, int mh, int rps, int mw, std::string& e
         occ = 1 << 20;
         for (auto* k2 : {march2_kernel(b->mixed, false, mw), march2_kernel(b->mixed, true, mw)}) {
             int o = 0;
-            B_TRY(cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, int(MARCH2_DYN_SMEM)));
+            B_TRY(allow_max_dynamic_smem(reinterpret_cast<const void*>(k2)));
             B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k2, mw, MARCH2_DYN_SMEM));
             occ = std::min(occ, o);
         }
@@ -2691,8 +2706,8 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         b->rows_threads = 32 * warps;
         b->smem_rows = per_warp * warps;
     }
-    cudaFuncSetAttribute(k_rows<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
-    cudaFuncSetAttribute(k_rows<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_rows));
+    for (const void* kr : {reinterpret_cast<const void*>(k_rows<false>), reinterpret_cast<const void*>(k_rows<true>)})
+        if (allow_max_dynamic_smem(kr) != cudaSuccess) { err = "cannot raise the row solver's shared-memory limit"; return nullptr; }
     {
         int occ = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rows<true>, b->rows_threads, b->smem_rows);

@@ -56,6 +56,7 @@ def _lib(real: str) -> C.CDLL:
         L.orc_passes.argtypes = [vp]
         L.orc_add_solitary_wave.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_new_terrain.argtypes = [vp, C.POINTER(C.c_float), i, i]
+        L.orc_rebootstrap.argtypes = [vp]
         L.orc_cr_solve.argtypes = [i, dp, dp, dp, dp, dp]
         L.orc_time_physical_steps.argtypes = [vp, i]
         L.orc_time_physical_steps.restype = C.c_double
@@ -149,6 +150,10 @@ class Oracle:
 
     def add_solitary_wave(self, H, theta_deg, xc, yc):
         self.L.orc_add_solitary_wave(self.h, H, theta_deg, xc, yc)
+
+    def rebootstrap(self):
+        """Recompute the Pass1 faces from the current state at the next pass."""
+        self.L.orc_rebootstrap(self.h)
 
     def new_terrain(self, z: np.ndarray):
         """newTerrainSettings with a new bathymetry grid (same layout as the creation grid)."""

@@ -170,6 +170,10 @@ int orc_time_scheme(void* h) { return static_cast<Eng*>(h)->time_scheme; }
 double orc_total_time(void* h) { return double(static_cast<Eng*>(h)->total_time); }
 int orc_passes(void* h) { return static_cast<Eng*>(h)->passes; }
 
+// The next pass recomputes the Pass1 faces from the current state (what the fused forms, which keep
+// no Pass1 textures, do after any change of state).
+void orc_rebootstrap(void* h) { static_cast<Eng*>(h)->bootstrap_needed = true; }
+
 void orc_new_terrain(void* h, const float* bathy, int bnx, int bny) {
     static_cast<Eng*>(h)->new_terrain(std::vector<float>(bathy, bathy + size_t(bnx) * bny), bnx, bny);
 }
