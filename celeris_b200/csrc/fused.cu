@@ -2166,6 +2166,9 @@ March2Kernel march2_kernel(bool mixed, bool adapt, int w) {
 }
 
 int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
+    // the launch checks below read the runtime's last-error state: drop what calls outside this pass
+    // left there (they reported it, or ignored it, where they happened)
+    (void)cudaGetLastError();
     const size_t nm = b->mem.size();
     if (pa.stats) B_TRY(cudaMemsetAsync(b->stats_all, 0, nm * STATS_N * sizeof(double), b->stream));
     {
@@ -2760,6 +2763,7 @@ void batch_destroy(cel_batch* b) {
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
     delete b;
+    (void)cudaGetLastError();   // teardown has no caller to report to; leave no stale error behind
 }
 
 int batch_set_stream(cel_batch* b, cudaStream_t s, std::string& err) {

@@ -529,6 +529,7 @@ public:
         for (cel_boundary* b : {&p.west, &p.east, &p.south, &p.north})
             if (b->uts) std::free(b->uts);
         if (own_stream && stream) cudaStreamDestroy(stream);
+        (void)cudaGetLastError();   // teardown has no caller to report to; leave no stale error behind
     }
 
     template <typename T>
@@ -691,6 +692,7 @@ public:
     }
 
     int run_stats_kernels() {
+        (void)cudaGetLastError();
         const float4* s = st[sim_idx];
         const int nbx = hs.nx / 4, nby = hs.ny / 4;
         if (nbx > 0 && nby > 0) {
@@ -768,6 +770,7 @@ public:
 
     // timestep() (engine.cpp:849-1522): one pass
     int timestep() override {
+        (void)cudaGetLastError();   // the launch checks below must see only this pass's launches
         if (!sch.initialized) { if (int e = reset_timestep(0.f, 0.f, nullptr)) return e; }
         const dim3 blk(BX2, BY2);
         float4* old_state = st[sim_idx];
