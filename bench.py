@@ -53,6 +53,8 @@ def parse():
                     help="force the stencil variant (1 or 2 rows per step) after tuning; 0 keeps the choice")
     ap.add_argument("--stencil-width", type=int, default=0, choices=[0, 96, 128],
                     help="force the stencil strip threads (with two rows per step) after tuning; 0 keeps the choice")
+    ap.add_argument("--band-width", type=int, default=0, help="force the column band width after tuning (0 keeps it)")
+    ap.add_argument("--strip-height", type=int, default=0, help="force the stencil strip height after tuning (0 keeps it)")
     ap.add_argument("--tune-steps", type=int, default=6, help="steps per autotuner candidate (0 keeps the defaults)")
     return ap.parse_args()
 
@@ -249,6 +251,8 @@ def main():
             batch.set_stencil_rows(args.stencil_rows)
         if args.stencil_width:
             batch.set_stencil_width(args.stencil_width)
+        if args.band_width or args.strip_height:
+            batch.set_tuning(args.band_width, args.strip_height)
         batch.step(max(3, args.warmup))
     torch.cuda.synchronize()
 
