@@ -117,3 +117,19 @@ def test_byte_model(celeris):
     assert s == 112 and t == (112 + 48) + (136 + 48)
     s2, t2 = celeris.byte_model("mixed", 1)
     assert t2 > t
+
+
+def test_new_entry_points_refuse_null_handles(celeris):
+    """Argument checks come before any device work, so they hold on a machine without a GPU."""
+    L = celeris.lib()
+    z = (C.c_float * 16)()
+    f = C.c_float()
+    assert L.cel_set_bathymetry(None, z, 4, 4) == 1
+    assert L.cel_batch_set_bathymetry(None, 0, z, 4, 4) == 1
+    assert L.cel_batch_add_solitary_wave(None, 0, 0.1, 0.0, 1.0, 1.0) == 1
+    assert L.cel_get_water_height(None, 0.0, 0.0, C.byref(f)) == 1
+    assert L.cel_batch_set_stencil_width(None, 96) == 1
+    assert L.cel_batch_stencil_width(None) == 0
+    assert L.cel_spectrum_waves(None, 9.81, 0, None, None) == 1
+    assert L.cel_log_dump(None, None, 0.0, 0.0) == 1
+    assert L.cel_write_hotstart(None, None, None) == 1
