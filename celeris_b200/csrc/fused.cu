@@ -2857,9 +2857,10 @@ int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
         // a bounded TMA wait that gave up (should never happen) is a CUDA error of the batch
         if (late != 0) o.health = CEL_ERR_CUDA;
         // adaptive members: the dt of the step's first pass; the clock advanced by the last pass's dt
-        o.timestep = b->adaptive ? double(ctl[i].dt_first) : double(b->dt_host[i]);
+        // (before an adaptive batch's first pass its controllers have chosen nothing: the uniform step)
+        o.timestep = (b->adaptive && b->dt_started) ? double(ctl[i].dt_first) : double(b->dt_host[i]);
         o.cfl_number = o.cfl_rate * o.timestep;
-        const double last_dt = b->adaptive ? double(ctl[i].dt) : double(b->step_dt[i]);
+        const double last_dt = (b->adaptive && b->dt_started) ? double(ctl[i].dt) : double(b->step_dt.empty() ? 0.f : b->step_dt[i]);
         o.total_time = at_step ? t64[i] - last_dt : t64[i];
         o.time_scheme = b->sch.time_scheme;
     }

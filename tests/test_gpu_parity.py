@@ -510,3 +510,14 @@ def test_live_batches_of_different_sizes_step_in_any_order(celeris):
     ref.step(5)
     for i in range(len(big)):
         np.testing.assert_array_equal(b1.state(i), ref.state(i))
+
+
+def test_adaptive_batch_reports_the_uniform_step_before_its_first_pass(celeris):
+    p, z, bnx, bny, keep = _case("solid", N=1)
+    p.adaptive = 1
+    b = celeris.Batch([(p, z)], "mixed")
+    s = b.stats()[0]
+    assert s["timestep"] == float(np.float32(p.timestep))
+    assert s["total_time"] == 0.0
+    b.step(3)
+    assert b.stats()[0]["timestep"] > 0
