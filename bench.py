@@ -43,7 +43,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c4", choices=["c4", "c2", "c3", "c5"])
+    ap.add_argument("--config", default="c4", choices=["c4", "c2", "c3", "c5", "c1"])
+    ap.add_argument("--correction-steps", type=int, default=-1, help="override correctionStepsNum (-1 keeps 1)")
+    ap.add_argument("--adaptive", action="store_true", help="adaptive time steps chosen on the device")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fused"])
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--no-plain", action="store_true", help="skip the per-domain plain FP32 comparison")
@@ -68,6 +70,8 @@ def members_for(cfg: str, rank: int, count: int):
         return cases.config5(count, 1, first_member=rank * count), f"C5 {count}-domain ensemble (128..512 sides)"
     if cfg == "c2":
         return [cases.config2(member=rank)], "C2 2048^2 single domain, JONSWAP wave-maker, sponges, Manning 0.02"
+    if cfg == "c1":
+        return [cases.config1()], "C1 512x64 flume, dx=0.5 m, sine wave-maker, 1:20 beach"
     return [cases.config3(4096, 4096)], "C3 4096^2 single domain, solitary wave on a truncated cone"
 
 
@@ -236,6 +240,11 @@ def main():
     import celeris_b200 as cb
 
     members, workload = members_for(args.config, rank, args.members)
+    for m in members:
+        if args.correction_steps >= 0:
+            m[0].correction_steps = args.correction_steps
+        if args.adaptive:
+            m[0].adaptive = 1
     batch = cb.Batch([(m[0], m[1]) for m in members], args.form)
     stream = torch.cuda.Stream()
     batch.set_stream(stream.cuda_stream)
@@ -286,7 +295,8 @@ def main():
     dt_ptr = C.cast(C.c_void_p(dt_pinned.data_ptr()), C.POINTER(C.c_float))
     stats_out = (cb.Stats * n)()
     for _ in range(e2e_steps):
-        cb.check(lib.cel_batch_set_timestep(batch.h, dt_ptr))
+        if not args.adaptive:   # an adaptive batch chooses its steps on the device
+            cb.check(lib.cel_batch_set_timestep(batch.h, dt_ptr))
         cb.check(lib.cel_batch_step(batch.h, 1))
         cb.check(lib.cel_batch_stats(batch.h, stats_out))
     e1.record(stream)
@@ -296,7 +306,7 @@ def main():
     if dist is not None:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = total_cells * e2e_steps / (float(e2e_t.item()) / 1e3) / 1e9
-    h2d = n * 4
+    h2d = 0 if args.adaptive else n * 4
     d2h = n * (12 * 8 + 8)
 
     # ---- roofline of the dominant kernel: per-launch CUDA events, direct launches ----------
@@ -365,7 +375,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload, "form": args.form, "members_per_gpu": len(members),
-                       "cells_per_gpu": cells, "correction_steps": N, "cuda_graph": not args.no_graph,
+                       "cells_per_gpu": cells, "correction_steps": N, "adaptive": bool(args.adaptive), "cuda_graph": not args.no_graph,
                        "l2": "working set (%.1f GB) larger than L2 (126 MB); no flush" % (
                            cells * 4 * (42 + (9 if args.form == "mixed" else 0)) / 1e9),
                        "parallelism": f"ensemble sharded by domain over {world} GPU(s)",
