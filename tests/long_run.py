@@ -9,9 +9,10 @@ separately and meet in .npz files:
 
 Cases: ``c3`` (1024^2 solitary wave on the truncated cone, solid walls), ``c3wm`` (the same
 basin with the sinusoidal wave-maker), ``c1`` (512x64 flume with the sine wave-maker), and
-``c4:<i>`` for member i of the 64-member C4 ensemble.  For ``c4:<i>`` the oracle runs member i
-alone, while ``gpu`` runs the whole ensemble as one batch (the production configuration, mixed
-form, graphs, autotuned) and keeps the members listed with ``--members``.  Every
+``c4:<i>`` / ``c5:<i>`` for member i of the 64-member C4 or 1024-member C5 ensemble.  For
+those the oracle runs member i alone, while ``gpu --case c4`` (or ``c5``) runs the whole
+ensemble as one batch (the production configuration, mixed form, graphs, autotuned) and keeps
+the members listed with ``--members``.  Every
 ``--every`` steps the FP64 total water volume (mass_full) is recorded.
 
 Reported per form: eta RMS over the interior (m), max |eta error| (m), max run-up of each side
@@ -45,21 +46,26 @@ def build_case(name: str, n: int | None):
         return cases.config1()
     if name.startswith("c4:"):
         return cases.config4()[int(name[3:])]
+    if name.startswith("c5:"):
+        return cases.config5(1, first_member=int(name[3:]))[0]
     raise KeyError(name)
 
 
 def run_gpu_ensemble(args):
-    """The 64-member C4 ensemble as one batch; records the members in --members."""
+    """The 64-member C4 or 1024-member C5 ensemble as one batch; records the members in --members."""
     import celeris_b200 as cb
-    members = cases.config4()
+    members = cases.config4() if args.case == "c4" else cases.config5()
     keep = [int(k) for k in args.members.split(",")]
-    b = cb.Batch([(m[0], m[1]) for m in members], "mixed")
+    form = args.forms.split(",")[0]   # the ensemble runs one form (fused or mixed)
+    b = cb.Batch([(m[0], m[1]) for m in members], form)
     b.use_graph(True)
     tuned = b.autotune(4)
     # autotuning advanced the members: start over from the initial condition with the tuned setup
-    b2 = cb.Batch([(m[0], m[1]) for m in members], "mixed")
+    b2 = cb.Batch([(m[0], m[1]) for m in members], form)
     b2.set_tuning(tuned["band_width"], tuned["strip_height"])
     b2.set_stencil_rows(b.stencil_rows)
+    if b.stencil_rows == 2:
+        b2.set_stencil_width(b.stencil_width)
     b2.use_graph(True)
     del b
     masses = {k: [b2.stats_current()[k]["mass_full"]] for k in keep}
@@ -100,7 +106,7 @@ def run_oracle(args):
 
 
 def run_gpu(args):
-    if args.case == "c4":
+    if args.case in ("c4", "c5"):
         return run_gpu_ensemble(args)
     import celeris_b200 as cb
     p, z, bnx, bny = build_case(args.case, args.n)
