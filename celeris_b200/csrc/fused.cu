@@ -2437,8 +2437,12 @@ int configure_work(cel_batch* b, int cw, int mh, int rps, int mw, std::string& e
     b->mtiles = static_cast<int4*>(p);
     if (dalloc(b, &p, bd.size() * sizeof(int2), err)) return CEL_ERR_CUDA;
     b->bands = static_cast<int2*>(p);
-    B_TRY(cudaMemcpy(b->mtiles, mt.data(), mt.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    B_TRY(cudaMemcpy(b->bands, bd.data(), bd.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    // the allocations' zeroing ran on the legacy stream: finish it before the batch stream writes
+    B_TRY(cudaDeviceSynchronize());
+    // on the batch stream (non-blocking: it would not wait for legacy-stream copies)
+    B_TRY(cudaMemcpyAsync(b->mtiles, mt.data(), mt.size() * sizeof(int4), cudaMemcpyHostToDevice, b->stream));
+    B_TRY(cudaMemcpyAsync(b->bands, bd.data(), bd.size() * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+    B_TRY(cudaStreamSynchronize(b->stream));
     b->nmtiles = int(mt.size());
     b->nbands = int(bd.size());
     b->cw = cw;
@@ -2747,6 +2751,9 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
         }
         if (upload_state(b.get(), i, rgba.data(), err, lo.empty() ? nullptr : lo.data())) return nullptr;
     }
+    // The set-up copies and memsets above ran on the legacy stream, which the batch's non-blocking
+    // streams do not wait for (and a pageable upload may return before its DMA lands): finish them.
+    if (cudaDeviceSynchronize() != cudaSuccess) { err = "batch setup: device synchronisation failed"; return nullptr; }
     return b.release();
 }
 
@@ -2907,10 +2914,11 @@ int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, 
     Member& m = b->mem[i];
     MemberDev& d = b->hdev[i];
     const int NX = m.hs.NX, NY = m.hs.NY, sin = b->ix.sin;
-    B_TRY(cudaStreamSynchronize(b->stream));
     std::vector<float> hi(m.plane), lo(b->mixed ? m.plane : 0);
-    B_TRY(cudaMemcpy(hi.data(), d.S[sin][0], m.plane * sizeof(float), cudaMemcpyDeviceToHost));
-    if (b->mixed) B_TRY(cudaMemcpy(lo.data(), d.L[sin][0], m.plane * sizeof(float), cudaMemcpyDeviceToHost));
+    B_TRY(cudaMemcpyAsync(hi.data(), d.S[sin][0], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+    if (b->mixed)
+        B_TRY(cudaMemcpyAsync(lo.data(), d.L[sin][0], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+    B_TRY(cudaStreamSynchronize(b->stream));
     const std::vector<float> ba_old = m.hs.BA;
     prepare_bottom(z, bnx, bny, m.hs.nx, m.hs.ny, float(m.p.width), float(m.p.length), m.hs);
     std::vector<float> by(m.plane, 0.f), bx(m.plane, 0.f), ba(m.plane, 0.f);
@@ -2926,12 +2934,15 @@ int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, 
                 hi[e] = (hi[e] - ba_old[k]) + m.hs.BA[k];
             }
         }
-    B_TRY(cudaMemcpy(const_cast<float*>(d.BY), by.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
-    B_TRY(cudaMemcpy(const_cast<float*>(d.BX), bx.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
-    B_TRY(cudaMemcpy(const_cast<float*>(d.BA), ba.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
-    B_TRY(cudaMemcpy(d.S[sin][0], hi.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
-    if (b->mixed) B_TRY(cudaMemcpy(d.L[sin][0], lo.data(), m.plane * sizeof(float), cudaMemcpyHostToDevice));
-    B_TRY(cudaMemset(d.AUX[0], 0, 2 * m.plane * sizeof(float)));
+    // ordered on the batch stream, and complete before the host buffers go out of scope
+    const size_t pb = m.plane * sizeof(float);
+    B_TRY(cudaMemcpyAsync(const_cast<float*>(d.BY), by.data(), pb, cudaMemcpyHostToDevice, b->stream));
+    B_TRY(cudaMemcpyAsync(const_cast<float*>(d.BX), bx.data(), pb, cudaMemcpyHostToDevice, b->stream));
+    B_TRY(cudaMemcpyAsync(const_cast<float*>(d.BA), ba.data(), pb, cudaMemcpyHostToDevice, b->stream));
+    B_TRY(cudaMemcpyAsync(d.S[sin][0], hi.data(), pb, cudaMemcpyHostToDevice, b->stream));
+    if (b->mixed) B_TRY(cudaMemcpyAsync(d.L[sin][0], lo.data(), pb, cudaMemcpyHostToDevice, b->stream));
+    B_TRY(cudaMemsetAsync(d.AUX[0], 0, 2 * pb, b->stream));
+    B_TRY(cudaStreamSynchronize(b->stream));
     b->step_stats_valid = false;   // the gathered totals describe the state before the change
     return CEL_OK;
 }

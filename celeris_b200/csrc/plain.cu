@@ -607,6 +607,9 @@ public:
         const int nb = std::max(1, (hs.nx / 4) * (hs.ny / 4));
         if (int e = dalloc(blocks, size_t(nb) * 9)) return e;
         if (int e = dalloc(dstats, 16)) return e;
+        // the set-up copies and memsets above ran on the legacy stream, which the engine's
+        // non-blocking stream does not wait for: finish them
+        CEL_CUDA_TRY(cudaDeviceSynchronize());
         return remesh();
     }
 
@@ -615,15 +618,17 @@ public:
             HostSetup fresh;
             if (int st0 = make_setup(p, terrain.data(), terrain_nx, terrain_ny, fresh, err)) return st0;
             hs = fresh;
+            // on the engine's stream, finished before the host copies go out of scope
             for (int k = 0; k < hs.Kx; ++k)
-                CEL_CUDA_TRY(cudaMemcpy(ABCx[k], hs.ABCx[k].data(), size_t(hs.lenx[k] + 4) * hs.NY * sizeof(float4),
-                                        cudaMemcpyHostToDevice));
+                CEL_CUDA_TRY(cudaMemcpyAsync(ABCx[k], hs.ABCx[k].data(), size_t(hs.lenx[k] + 4) * hs.NY * sizeof(float4),
+                                             cudaMemcpyHostToDevice, stream));
             for (int k = 0; k < hs.Ky; ++k)
-                CEL_CUDA_TRY(cudaMemcpy(ABCy[k], hs.ABCy[k].data(), size_t(hs.NX) * (hs.leny[k] + 4) * sizeof(float4),
-                                        cudaMemcpyHostToDevice));
+                CEL_CUDA_TRY(cudaMemcpyAsync(ABCy[k], hs.ABCy[k].data(), size_t(hs.NX) * (hs.leny[k] + 4) * sizeof(float4),
+                                             cudaMemcpyHostToDevice, stream));
             std::vector<float4> b(ntex);
             for (size_t i = 0; i < ntex; ++i) b[i] = make_float4(hs.BY[i], hs.BX[i], hs.BA[i], 0.f);
-            CEL_CUDA_TRY(cudaMemcpy(BOT, b.data(), ntex * sizeof(float4), cudaMemcpyHostToDevice));
+            CEL_CUDA_TRY(cudaMemcpyAsync(BOT, b.data(), ntex * sizeof(float4), cudaMemcpyHostToDevice, stream));
+            CEL_CUDA_TRY(cudaStreamSynchronize(stream));
         }
         std::vector<float4> s(ntex);
         for (size_t i = 0; i < ntex; ++i) s[i] = make_float4(hs.ic[3 * i], hs.ic[3 * i + 1], hs.ic[3 * i + 2], 0.f);
