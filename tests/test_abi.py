@@ -133,3 +133,32 @@ def test_new_entry_points_refuse_null_handles(celeris):
     assert L.cel_spectrum_waves(None, 9.81, 0, None, None) == 1
     assert L.cel_log_dump(None, None, 0.0, 0.0) == 1
     assert L.cel_write_hotstart(None, None, None) == 1
+
+
+EXAMPLES = os.environ.get("CELERIS_REFERENCE", "/root/reference") + "/msvc/Examples"
+
+
+@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="the reference's example folder is not present")
+def test_reference_example_inputs_parse(celeris):
+    """Every .cml the reference ships parses, with the files it names (.cbf grids, irregular-wave
+    components, time series) read where they exist."""
+    import glob
+    seen = {}
+    for path in sorted(glob.glob(os.path.join(EXAMPLES, "**", "*.cml"), recursive=True)):
+        p = celeris.params_from_cml(path)
+        assert p.nx >= 2 and p.ny >= 2 and p.width > 0 and p.length > 0, path
+        bp = p.bathymetry_path.decode()
+        if os.path.exists(bp):
+            z = celeris.read_cbf(bp)
+            assert z.size > 0 and np.isfinite(z).all(), bp
+        seen[os.path.basename(path)] = p
+    assert len(seen) >= 5
+    irr = seen.get("conical_island - irregular.cml")
+    if irr is not None:
+        assert irr.west.type == abi.CEL_BC_IRREGULAR and irr.west.n_waves > 0
+    uts = seen.get("conical_island - UniformTimeSeries.cml")
+    if uts is not None:
+        assert uts.west.type == abi.CEL_BC_UTS and uts.west.n_uts > 1
+    ready = seen.get("conical_island_ready.cml")
+    if ready is not None:
+        assert ready.log.do_log == 1 and ready.log.n_gauges == 5 and ready.log.n_ranges == 2
