@@ -98,3 +98,30 @@ def test_terrain_change_matches_reference_shader():
         o.physical_steps(10)
         out.append(o.state().astype(np.float32))
     np.testing.assert_array_equal(out[0], out[1])
+
+
+EXAMPLES = os.environ.get("CELERIS_REFERENCE", "/root/reference") + "/msvc/Examples"
+
+
+@pytest.mark.skipif(not (os.path.exists(REF_SHADER) and os.path.isdir(EXAMPLES)),
+                    reason="oracle/_ref or the reference's example folder is not present")
+def test_fp32_oracle_matches_reference_shader_on_the_reference_examples():
+    """The reference's own example inputs (conical island, irregular and time-series wave-makers,
+    the tutorial case, the flume), 8 physical steps: the FP32 oracle and the reference's shader
+    build agree bit for bit."""
+    import glob
+    import celeris_b200 as cb
+    ran = 0
+    for path in sorted(glob.glob(os.path.join(EXAMPLES, "**", "*.cml"), recursive=True)):
+        p = cb.params_from_cml(path)
+        if not os.path.exists(p.bathymetry_path.decode()):
+            continue
+        z = cb.read_cbf(p.bathymetry_path.decode())
+        states = []
+        for real in ("f32", "ref"):
+            o = Oracle(p, z, z.shape[1], z.shape[0], real=real)
+            o.physical_steps(8)
+            states.append(o.state().astype(np.float32))
+        np.testing.assert_array_equal(states[0], states[1], err_msg=path)
+        ran += 1
+    assert ran >= 4
