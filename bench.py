@@ -75,6 +75,21 @@ def members_for(cfg: str, rank: int, count: int):
     return [cases.config3(4096, 4096)], "C3 4096^2 single domain, solitary wave on a truncated cone"
 
 
+STAT_FIELDS = ("mass_full", "total_time", "max_depth", "cfl_rate", "health")
+
+
+def gather_member_stats(stats: list, dist=None, device: str = "cuda") -> np.ndarray:
+    """Every rank's per-member FP64 totals (one row of STAT_FIELDS per member, ranks in order),
+    gathered once at the end of a run: about 40 B per member, no collective inside a step."""
+    import torch
+    local = torch.tensor([[float(s[k]) for k in STAT_FIELDS] for s in stats], dtype=torch.float64, device=device)
+    if dist is None:
+        return local.cpu().numpy()
+    parts = [torch.empty_like(local) for _ in range(dist.get_world_size())]
+    dist.all_gather(parts, local)
+    return torch.cat(parts).cpu().numpy()
+
+
 def job_rate(ms: float, cells: int, steps: int, dist=None, device: str = "cuda"):
     """Whole-job throughput: every rank's cells over the slowest rank's time (max over ranks)."""
     import torch
@@ -306,6 +321,10 @@ def main():
     if dist is not None:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = total_cells * e2e_steps / (float(e2e_t.item()) / 1e3) / 1e9
+    # the whole ensemble's totals on every rank (members are sharded; each rank holds `count`)
+    ens = gather_member_stats(batch.stats(), dist)
+    ensemble = {"members": int(ens.shape[0]), "mass_full_sum_m3": float(ens[:, 0].sum()),
+                "unhealthy_members": int((ens[:, 4] != 0).sum())}
     h2d = 0 if args.adaptive else n * 4
     d2h = n * (12 * 8 + 8)
 
@@ -396,6 +415,7 @@ def main():
                               "frac": value * 1e9 * step_bytes / world / 1e9 / peak if peak else None},
             "kernel_shares": shares,
             "gpu_launches": batch.launches_per_step * args.steps,
+            "ensemble": ensemble,
             "clocks": clocks,
             "cpu_baseline": cpu,
             "plain_per_domain": plain,

@@ -41,7 +41,11 @@ def _rank(rank: int, world: int, port: int, out):
         dist.all_gather_object(gathered, mine)
         cells = sum(p.nx * p.ny for p, _, _, _ in members)
         rate, ms_max, total = bench.job_rate(10.0 + rank, cells, 100, dist, device="cpu")
-        out.put((rank, mine == expect, gathered, cells, rate, ms_max, total))
+        # per-member totals of this rank's members, gathered at the end of a run
+        fake = [{"mass_full": 100.0 * rank + k, "total_time": 1.5, "max_depth": 2.0, "cfl_rate": 3.0,
+                 "health": 5 if (rank, k) == (1, 2) else 0} for k in range(count)]
+        ens = bench.gather_member_stats(fake, dist, device="cpu")
+        out.put((rank, mine == expect, gathered, cells, rate, ms_max, total, ens))
     finally:
         dist.destroy_process_group()
 
@@ -63,7 +67,12 @@ def test_ensemble_shards_and_job_rate():
     flat = [m for shard in shards for m in shard]
     assert len(set(flat)) == len(flat)                         # disjoint members
     total = sum(r[3] for r in res)
-    for _, _, _, _, rate, ms_max, tot in res:
+    for r in res:                                              # every rank holds the whole ensemble's rows
+        ens = r[7]
+        assert ens.shape == (world * 3, 5)
+        np.testing.assert_array_equal(ens[:, 0], [0, 1, 2, 100, 101, 102])
+        assert int((ens[:, 4] != 0).sum()) == 1
+    for _, _, _, _, rate, ms_max, tot, _ in res:
         assert ms_max == 11.0                                  # the slowest rank's time
         assert tot == total                                    # every rank's cells
         assert abs(rate - total * 100 / (11.0 / 1e3) / 1e9) < 1e-9
