@@ -326,7 +326,7 @@ def main():
     ensemble = {"members": int(ens.shape[0]), "mass_full_sum_m3": float(ens[:, 0].sum()),
                 "unhealthy_members": int((ens[:, 4] != 0).sum())}
     h2d = 0 if args.adaptive else n * 4
-    d2h = n * (12 * 8 + 8)
+    d2h = (1 + n + 12 * n) * 8   # the read-back block: error flag, n FP64 clocks, n x 12 FP64 totals
 
     # ---- roofline of the dominant kernel: per-launch CUDA events, direct launches ----------
     batch.use_graph(False)
