@@ -1926,14 +1926,29 @@ __device__ void ab3_coefficients(float dt, float d1, float d2, float* ab) {
 
 // Max CFL rate max((|u| + c)/dx, (|v| + c)/dy) of each member's current state over the cells of
 // its 4x4 blocks (the GetStats region, compute.hlsl:1319-1378), as non-negative float bits.
+// Each CTA takes a contiguous range of tiles (consecutive tiles mostly belong to one member), keeps
+// the maximum in registers and publishes it with one atomic per warp when the member changes or
+// the range ends: a few thousand atomics instead of one per warp per tile on 64 words.
 __global__ void __launch_bounds__(256) k_cfl(const MemberDev* __restrict__ mems, const int4* __restrict__ tiles,
                                              int ntiles, int buf, unsigned int* __restrict__ out) {
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int per = (ntiles + gridDim.x - 1) / gridDim.x;
+    const int t_begin = blockIdx.x * per, t_end = min(ntiles, t_begin + per);
+    int cur = -1;
+    float m = 0.f;
+    auto flush = [&]() {   // warp-uniform: every lane has the same `cur`
+        float v = m;
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0 && cur >= 0 && v > 0.f) atomicMax(out + cur, __float_as_uint(v));
+        m = 0.f;
+    };
+    for (int t = t_begin; t < t_end; ++t) {
         const int4 tl = tiles[t];
+        if (tl.x != cur) { flush(); cur = tl.x; }
         const MemberDev& M = mems[tl.x];
         const SimConsts& c = M.c;
-        float m = 0.f;
-        for (int k = threadIdx.x; k < TX * TY; k += 256) {
+#pragma unroll
+        for (int r = 0; r < (TX * TY) / 256; ++r) {
+            const int k = r * 256 + threadIdx.x;
             const int gx = tl.y + k % TX, gy = tl.z + k / TX;
             if (gx < 2 + 4 * (c.nx / 4) && gy < 2 + 4 * (c.ny / 4)) {
                 const size_t gi = size_t(gy) * M.P + gx;
@@ -1944,9 +1959,8 @@ __global__ void __launch_bounds__(256) k_cfl(const MemberDev* __restrict__ mems,
                                    (fabsf(q * M.S[buf][2][gi]) + cc) * c.one_over_dy));
             }
         }
-        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(out + tl.x, __float_as_uint(m));
     }
+    flush();
 }
 
 // resetTimestep's dt choice for every member before a pass (engine.cpp:1698-1726): the target
