@@ -1699,7 +1699,9 @@ __global__ void __launch_bounds__(128) k_cols_serial(const MemberDev* __restrict
 
 // ---------------------------------------------------------------------------------------------
 // Boundary strips (compute.hlsl:985-1309), one side per launch over every member.
-// work item: {member, first strip cell}; 256 strip cells per item.
+// work item: {member, first strip cell}; 256 strip cells per item, or BND_CELLS for a sponge strip,
+// whose threads take BND_CPT cells each and issue all their loads before the first store (the
+// narrow strips of the other kinds keep one cell per thread, so they still spread over the SMs).
 // phase 0: compute and write in place; 1: compute into the member's scratch; 2: copy back.
 // ---------------------------------------------------------------------------------------------
 __device__ float3 irregular_tree(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, double t64,
@@ -1756,6 +1758,9 @@ __device__ void uts_lookup(const float* tab, int n, float t, float out[3]) {
     }
 }
 
+constexpr int BND_CPT = 4;
+constexpr int BND_CELLS = 256 * BND_CPT;
+
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ mems, const int2* __restrict__ items,
                                                   int nitems, int side, int phase, int out) {
@@ -1773,78 +1778,119 @@ __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ 
         if (x0 < 0) { sw += x0; x0 = 0; }
         if (y0 < 0) { sh += y0; y0 = 0; }
         sw = min(sw, NX - x0); sh = min(sh, NY - y0);
-        const int cell = wi.y + threadIdx.x;
-        if (cell >= sw * sh) continue;
-        const int x = x0 + cell % sw, y = y0 + cell / sw;
-        const size_t gi = size_t(y) * P + x;
         float* W = M.S[out][0];
         float* HU = M.S[out][1];
         float* HV = M.S[out][2];
-        if (phase == 2) {
-            W[gi] = M.strip[3 * cell]; HU[gi] = M.strip[3 * cell + 1]; HV[gi] = M.strip[3 * cell + 2];
-            if (MIXED) { M.L[out][0][gi] = 0.f; M.L[out][1][gi] = 0.f; M.L[out][2][gi] = 0.f; }
+        if (b.type == CEL_BC_SPONGE && phase == 0) {
+            // Pointwise: the loads of all the thread's cells are issued before the first store.
+            const float sl = b.sea_level;
+            const float L = (side == 1 || side == 3) ? float(b.width) * c.dx : float(b.width) * c.dy;
+            const float dt = *M.dtp;
+            size_t gi[BND_CPT];
+            float dist[BND_CPT], vw[BND_CPT], vu[BND_CPT], vv[BND_CPT], ba[BND_CPT];
+            float l0[BND_CPT], l1[BND_CPT], l2[BND_CPT];
+            bool ok[BND_CPT];
+#pragma unroll
+            for (int k = 0; k < BND_CPT; ++k) {
+                const int cell = wi.y + k * 256 + threadIdx.x;
+                ok[k] = cell < sw * sh;
+                const int x = x0 + cell % sw, y = y0 + cell / sw;
+                gi[k] = size_t(y) * P + x;
+                if (side == 3) dist[k] = float(x) * c.dx;
+                else if (side == 1) dist[k] = float(NX - x) * c.dx;
+                else if (side == 2) dist[k] = float(y) * c.dy;
+                else dist[k] = float(NY - y) * c.dy;
+                vw[k] = vu[k] = vv[k] = ba[k] = l0[k] = l1[k] = l2[k] = 0.f;
+                if (ok[k]) {
+                    vw[k] = W[gi[k]]; vu[k] = HU[gi[k]]; vv[k] = HV[gi[k]]; ba[k] = M.BA[gi[k]];
+                    if (MIXED) { l0[k] = M.L[out][0][gi[k]]; l1[k] = M.L[out][1][gi[k]]; l2[k] = M.L[out][2][gi[k]]; }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < BND_CPT; ++k) {
+                if (!ok[k]) continue;
+                const float dh = fmaxf(CEL_MIN_DEPTH, sl - ba[k]);
+                const float gam = sponge_fn(L, dist[k]) / sponge_fn(L, dist[k] + sqrtf(c.g * dh) * dt);
+                W[gi[k]] = gam * (vw[k] - sl) + sl;
+                HU[gi[k]] = gam * vu[k];
+                HV[gi[k]] = gam * vv[k];
+                if (MIXED) { M.L[out][0][gi[k]] = gam * l0[k]; M.L[out][1][gi[k]] = gam * l1[k]; M.L[out][2][gi[k]] = gam * l2[k]; }
+            }
             continue;
         }
-        float ow = 0.f, ou = 0.f, ov = 0.f;
-        float lw = 0.f, lu = 0.f, lv = 0.f;
-        const float sl = b.sea_level;
-        const double t64 = *M.time64;
-        const float t32 = *M.time32;
-        if (b.type == CEL_BC_SOLID) {
-            int qx, qy;
-            solid_source(side, x, y, c.nx, c.ny, qx, qy);
-            float sw_ = 0.f, su = 0.f, sv = 0.f, lw_ = 0.f, lu_ = 0.f, lv_ = 0.f;
-            if (qx >= 0 && qy >= 0 && qx < NX && qy < NY) {
-                const size_t qi = size_t(qy) * P + qx;
-                sw_ = W[qi]; su = HU[qi]; sv = HV[qi];
-                if (MIXED) { lw_ = M.L[out][0][qi]; lu_ = M.L[out][1][qi]; lv_ = M.L[out][2][qi]; }
+        const int cpt = (b.type == CEL_BC_SPONGE) ? BND_CPT : 1;
+        for (int k = 0; k < cpt; ++k) {
+            const int cell = wi.y + k * 256 + threadIdx.x;
+            if (cell >= sw * sh) break;   // cells ascend with k
+            const int x = x0 + cell % sw, y = y0 + cell / sw;
+            const size_t gi = size_t(y) * P + x;
+            if (phase == 2) {
+                W[gi] = M.strip[3 * cell]; HU[gi] = M.strip[3 * cell + 1]; HV[gi] = M.strip[3 * cell + 2];
+                if (MIXED) { M.L[out][0][gi] = 0.f; M.L[out][1][gi] = 0.f; M.L[out][2][gi] = 0.f; }
+                continue;
             }
-            ow = sw_; lw = lw_;
-            ou = (side == 1 || side == 3) ? -su : su; lu = (side == 1 || side == 3) ? -lu_ : lu_;
-            ov = (side == 0 || side == 2) ? -sv : sv; lv = (side == 0 || side == 2) ? -lv_ : lv_;
-        } else if (b.type == CEL_BC_SPONGE) {
-            const float dh = fmaxf(CEL_MIN_DEPTH, sl - M.BA[gi]);
-            float L, dist;
-            if (side == 3) { L = float(b.width) * c.dx; dist = float(x) * c.dx; }
-            else if (side == 1) { L = float(b.width) * c.dx; dist = float(NX - x) * c.dx; }
-            else if (side == 2) { L = float(b.width) * c.dy; dist = float(y) * c.dy; }
-            else { L = float(b.width) * c.dy; dist = float(NY - y) * c.dy; }
-            const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * (*M.dtp));
-            ow = gam * (W[gi] - sl) + sl;
-            ou = gam * HU[gi];
-            ov = gam * HV[gi];
-            if (MIXED) { lw = gam * M.L[out][0][gi]; lu = gam * M.L[out][1][gi]; lv = gam * M.L[out][2][gi]; }
-        } else if (b.type == CEL_BC_SINEWAVE) {
-            const float dh = fmaxf(0.f, sl - M.BA[gi]);
-            const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
-            const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
-            float e = 0.f, hu = 0.f, hv = 0.f;
-            if (dh > CEL_MIN_DEPTH) {
-                if (MIXED) sine_wave_t64(xx, yy, t64, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
-                else sine_wave(xx, yy, t32, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
-            }
-            ow = e + sl; ou = hu; ov = hv;
-        } else if (b.type == CEL_BC_UTS) {
-            float v[3];
-            uts_lookup(M.uts[side], M.nuts[side], MIXED ? float(t64) : t32, v);
-            ow = v[0] + sl; ou = v[1]; ov = v[2];
-        } else {
-            const bool colwise = (side == 1 || side == 3);
-            const int along = colwise ? y : x;
-            const int lim = colwise ? c.ny : c.nx;
-            if (along >= 2 && along < lim + 2) {
+            float ow = 0.f, ou = 0.f, ov = 0.f;
+            float lw = 0.f, lu = 0.f, lv = 0.f;
+            const float sl = b.sea_level;
+            const double t64 = *M.time64;
+            const float t32 = *M.time32;
+            if (b.type == CEL_BC_SOLID) {
+                int qx, qy;
+                solid_source(side, x, y, c.nx, c.ny, qx, qy);
+                float sw_ = 0.f, su = 0.f, sv = 0.f, lw_ = 0.f, lu_ = 0.f, lv_ = 0.f;
+                if (qx >= 0 && qy >= 0 && qx < NX && qy < NY) {
+                    const size_t qi = size_t(qy) * P + qx;
+                    sw_ = W[qi]; su = HU[qi]; sv = HV[qi];
+                    if (MIXED) { lw_ = M.L[out][0][qi]; lu_ = M.L[out][1][qi]; lv_ = M.L[out][2][qi]; }
+                }
+                ow = sw_; lw = lw_;
+                ou = (side == 1 || side == 3) ? -su : su; lu = (side == 1 || side == 3) ? -lu_ : lu_;
+                ov = (side == 0 || side == 2) ? -sv : sv; lv = (side == 0 || side == 2) ? -lv_ : lv_;
+            } else if (b.type == CEL_BC_SPONGE) {
+                const float dh = fmaxf(CEL_MIN_DEPTH, sl - M.BA[gi]);
+                float L, dist;
+                if (side == 3) { L = float(b.width) * c.dx; dist = float(x) * c.dx; }
+                else if (side == 1) { L = float(b.width) * c.dx; dist = float(NX - x) * c.dx; }
+                else if (side == 2) { L = float(b.width) * c.dy; dist = float(y) * c.dy; }
+                else { L = float(b.width) * c.dy; dist = float(NY - y) * c.dy; }
+                const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * (*M.dtp));
+                ow = gam * (W[gi] - sl) + sl;
+                ou = gam * HU[gi];
+                ov = gam * HV[gi];
+                if (MIXED) { lw = gam * M.L[out][0][gi]; lu = gam * M.L[out][1][gi]; lv = gam * M.L[out][2][gi]; }
+            } else if (b.type == CEL_BC_SINEWAVE) {
                 const float dh = fmaxf(0.f, sl - M.BA[gi]);
                 const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
                 const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
-                const float3 r = irregular_tree(b, M.waves, xx, yy, t32, t64, MIXED, dh, c.g);
-                ow = r.x; ou = r.y; ov = r.z;
+                float e = 0.f, hu = 0.f, hv = 0.f;
+                if (dh > CEL_MIN_DEPTH) {
+                    if (MIXED) sine_wave_t64(xx, yy, t64, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
+                    else sine_wave(xx, yy, t32, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
+                }
+                ow = e + sl; ou = hu; ov = hv;
+            } else if (b.type == CEL_BC_UTS) {
+                float v[3];
+                uts_lookup(M.uts[side], M.nuts[side], MIXED ? float(t64) : t32, v);
+                ow = v[0] + sl; ou = v[1]; ov = v[2];
+            } else {
+                const bool colwise = (side == 1 || side == 3);
+                const int along = colwise ? y : x;
+                const int lim = colwise ? c.ny : c.nx;
+                if (along >= 2 && along < lim + 2) {
+                    const float dh = fmaxf(0.f, sl - M.BA[gi]);
+                    const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
+                    const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
+                    const float3 r = irregular_tree(b, M.waves, xx, yy, t32, t64, MIXED, dh, c.g);
+                    ow = r.x; ou = r.y; ov = r.z;
+                }
             }
-        }
-        if (phase == 1) {
-            M.strip[3 * cell] = ow; M.strip[3 * cell + 1] = ou; M.strip[3 * cell + 2] = ov;
-        } else {
-            W[gi] = ow; HU[gi] = ou; HV[gi] = ov;
-            if (MIXED) { M.L[out][0][gi] = lw; M.L[out][1][gi] = lu; M.L[out][2][gi] = lv; }
+            if (phase == 1) {
+                M.strip[3 * cell] = ow; M.strip[3 * cell + 1] = ou; M.strip[3 * cell + 2] = ov;
+            } else {
+                W[gi] = ow; HU[gi] = ou; HV[gi] = ov;
+                if (MIXED) { M.L[out][0][gi] = lw; M.L[out][1][gi] = lu; M.L[out][2][gi] = lv; }
+            }
+
         }
     }
 }
@@ -2672,7 +2718,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
                 d.nuts[s] = bb.n_uts;
             }
             const int cellsn = (s == 0 || s == 2) ? NX * std::min(bb.width, NY) : std::min(bb.width, NX) * NY;
-            for (int c0 = 0; c0 < cellsn; c0 += 256) bitems[s].push_back(make_int2(i, c0));
+            for (int c0 = 0; c0 < cellsn; c0 += (bb.type == CEL_BC_SPONGE ? BND_CELLS : 256)) bitems[s].push_back(make_int2(i, c0));
             // a solid strip wider than 2 reads ghost cells of its own strip: compute, then write
             if (bb.type == CEL_BC_SOLID && bb.width >= 3) b->two_phase[s] = true;
         }
