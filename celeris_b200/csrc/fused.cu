@@ -43,12 +43,18 @@ namespace cel {
 namespace {
 
 constexpr int TX = 32, TY = 16;
-constexpr int NTC = 512;
+// column solver threads per CTA: CW columns x (NTC/CW) chunks.  1024 threads at one CTA per SM
+// (64 registers) measured slower on C4 than 512 at two: 10.07 with 32-column bands and 9.67 with
+// 16, against 10.34 Gcell-steps/s; a CTA's barriers and carry scans then stall the whole SM.
+#ifndef CEL_COLS_THREADS
+#define CEL_COLS_THREADS 512
+#endif
+constexpr int NTC = CEL_COLS_THREADS;
 // column solver CTAs per SM the build targets: 2 (64 registers, no spills); 1 lets the compiler take
 // about 100 registers and run one CTA per SM, 3 spills (measured on C4: 8.9 / 10.3 / 9.2 Gcell-steps/s)
 #ifndef CEL_COLS_MIN_CTAS
 #define CEL_COLS_MIN_CTAS 2
-#endif                     // column solver threads: CWT columns x (512/CWT) chunks
+#endif
 constexpr int STATS_N = 12;
 
 // stats accumulator layout
