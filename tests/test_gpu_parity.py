@@ -106,6 +106,48 @@ def test_batch_equals_single_engines(celeris):
         np.testing.assert_array_equal(batch.state(i), e.state())
 
 
+TINY = [(2, 2), (3, 5), (7, 2), (2, 9)]
+
+
+@pytest.mark.parametrize("nx, ny", TINY)
+def test_smallest_domains(celeris, nx, ny):
+    """The smallest grids the parameters accept (nx, ny >= 2: a 2-texel ghost frame around as
+    little as 2 x 2 interior cells), with systems of 2 and 3 unknowns and strips wider than the
+    domain: plain against the FP32 transcription bit for bit, the fused forms against the FP64
+    oracle."""
+    for kind in ("solid", "sponge", "mixed"):
+        p, z, bnx, bny, keep = _case(kind, nx=nx, ny=ny, N=1)
+        r32 = O.Oracle(p, z, bnx, bny, "f32")
+        eng = celeris.Engine(p, z, "plain")
+        r32.physical_steps(40)
+        eng.physical_steps(40)
+        a, b = eng.state(), r32.state()
+        errs = field_errors(a, b)
+        assert rel_ok(errs, 1e-5, 1e-9), (kind, errs)
+        assert np.array_equal(a[2:-2, 2:-2, :3].astype(np.float64), b[2:-2, 2:-2, :3]), (kind, errs)
+        r64 = O.Oracle(p, z, bnx, bny, "f64")
+        r64.physical_steps(40)
+        for form in ("fused", "mixed"):
+            e = celeris.Engine(p, z, form)
+            e.physical_steps(40)
+            s = e.state()
+            assert np.isfinite(s).all(), (kind, form)
+            assert eta_rms(s, r64.state()) <= 1e-4, (kind, form)
+
+
+def test_batch_of_smallest_domains_equals_single_engines(celeris):
+    """Tiny members beside a larger one in one batch, replayed from graphs."""
+    members = [_case(k, nx=nx, ny=ny, N=1)[:4] for (nx, ny), k in zip(TINY, ["solid", "sponge", "mixed", "solid"])]
+    members.append(_case("irregular", nx=40, ny=24, N=1)[:4])
+    batch = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
+    batch.use_graph(True)
+    batch.step(30)
+    for i, (p, z, bnx, bny) in enumerate(members):
+        e = celeris.Engine(p, z, "mixed")
+        e.physical_steps(30)
+        np.testing.assert_array_equal(batch.state(i), e.state())
+
+
 def test_batch_graph_replay_matches_direct(celeris):
     members = [_case(k, nx=48, ny=32, N=1)[:4] for k in ["mixed", "sponge", "irregular"]]
     b1 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
