@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--adaptive", action="store_true", help="adaptive time steps chosen on the device")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fused"])
     ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--lanes", type=int, default=0, help="lanes the batch is split into (0 = the library default)")
     ap.add_argument("--no-plain", action="store_true", help="skip the per-domain plain FP32 comparison")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="0 skips the CPU baseline")
     ap.add_argument("--no-graph", action="store_true", help="direct launches instead of CUDA graphs (profiling)")
@@ -260,7 +261,7 @@ def main():
             m[0].correction_steps = args.correction_steps
         if args.adaptive:
             m[0].adaptive = 1
-    batch = cb.Batch([(m[0], m[1]) for m in members], args.form)
+    batch = cb.Batch([(m[0], m[1]) for m in members], args.form, lanes=args.lanes)
     stream = torch.cuda.Stream()
     batch.set_stream(stream.cuda_stream)
     cells = batch.cells
@@ -326,9 +327,13 @@ def main():
     ensemble = {"members": int(ens.shape[0]), "mass_full_sum_m3": float(ens[:, 0].sum()),
                 "unhealthy_members": int((ens[:, 4] != 0).sum())}
     h2d = 0 if args.adaptive else n * 4
-    d2h = (1 + n + 12 * n) * 8   # the read-back block: error flag, n FP64 clocks, n x 12 FP64 totals
+    # the read-back block of each lane: error flag, its members' FP64 clocks and 12 FP64 totals each
+    lanes = batch.lanes
+    d2h = (lanes + n + 12 * n) * 8
 
     # ---- roofline of the dominant kernel: per-launch CUDA events, direct launches ----------
+    # (with timing on, the lanes run one after another, so each launch's span is its own; a
+    # stencil launch covers one lane's cells, cells / lanes on average)
     batch.use_graph(False)
     batch.kernel_timing(True)
     kt_steps = 10
@@ -341,7 +346,8 @@ def main():
     comp = 8.0 if args.form == "mixed" else 0.0
     stencil_bytes_cell = ((112 + comp) + N * (136 + comp)) / (1 + N)  # average over pass kinds
     avg_launch_s = st_ms / max(st_n, 1) / 1e3
-    achieved = stencil_bytes_cell * cells / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
+    cells_launch = cells / lanes
+    achieved = stencil_bytes_cell * cells_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -356,7 +362,7 @@ def main():
     traffic = None
     if args.form in ncu_bytes_cell:
         pb, cbytes = ncu_bytes_cell[args.form]
-        traffic = (pb + N * cbytes) / (1 + N) * cells
+        traffic = (pb + N * cbytes) / (1 + N) * cells_launch
     total_kernel_ms = sum(v[0] for v in kt.values())
     shares = {k: round(v[0] / total_kernel_ms, 4) for k, v in kt.items()} if total_kernel_ms > 0 else {}
     step_bytes = cb.byte_model(args.form, N)[1]
@@ -398,6 +404,7 @@ def main():
                        "l2": "working set (%.1f GB) larger than L2 (126 MB); no flush" % (
                            cells * 4 * (42 + (9 if args.form == "mixed" else 0)) / 1e9),
                        "parallelism": f"ensemble sharded by domain over {world} GPU(s)",
+                       "lanes": lanes,
                        "tuning": {"column_band_width": batch.tuning[0], "strip_height": batch.tuning[1],
                                   "stencil_rows_per_step": batch.stencil_rows,
                                   "stencil_threads_per_strip": batch.stencil_width,
@@ -408,7 +415,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
                          "kernel": "fused_stencil", "peak_source": peak_src,
-                         "algorithmic_bytes_per_cell": stencil_bytes_cell, "cells_per_launch": cells,
+                         "algorithmic_bytes_per_cell": stencil_bytes_cell, "cells_per_launch": cells_launch,
                          "avg_launch_ms": avg_launch_s * 1e3},
             "step_roofline": {"bytes_per_cell_step": step_bytes,
                               "achieved_gbs": value * 1e9 * step_bytes / world / 1e9,

@@ -152,7 +152,8 @@ def _kernel_times(handle, is_batch: int) -> dict:
 class Batch:
     """Many domains advanced together (``cel_batch``)."""
 
-    def __init__(self, members, form: str | int = "mixed"):
+    def __init__(self, members, form: str | int = "mixed", lanes: int = 0):
+        """``lanes``: how many lanes the members are split into (0 = the library's default)."""
         f = FORMS[form] if isinstance(form, str) else int(form)
         self.form = f
         self.members = list(members)
@@ -164,7 +165,7 @@ class Batch:
         bnx = (C.c_int * n)(*[z.shape[1] for z in self._z])
         bny = (C.c_int * n)(*[z.shape[0] for z in self._z])
         h = C.c_void_p()
-        check(lib().cel_batch_create(n, pp, zz, bnx, bny, f, C.byref(h)))
+        check(lib().cel_batch_create_lanes(n, pp, zz, bnx, bny, f, int(lanes), C.byref(h)))
         self.h = h
         self.n = n
         self.shapes = [(p.ny + 4, p.nx + 4) for p in self._params]
@@ -183,6 +184,10 @@ class Batch:
     @property
     def cells(self) -> int:
         return int(lib().cel_batch_cells(self.h))
+
+    @property
+    def lanes(self) -> int:
+        return int(lib().cel_batch_lanes(self.h))
 
     def set_stream(self, stream_ptr: int | None):
         check(lib().cel_batch_set_stream(self.h, C.c_void_p(stream_ptr or 0)))

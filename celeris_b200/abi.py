@@ -181,6 +181,9 @@ def _declare(L: C.CDLL) -> None:
         "cel_batch_add_solitary_wave": (i, [vp, i, C.c_double, C.c_double, C.c_double, C.c_double]),
         "cel_batch_create": (i, [i, C.POINTER(C.POINTER(Params)), C.POINTER(fp), C.POINTER(i),
                                  C.POINTER(i), i, C.POINTER(vp)]),
+        "cel_batch_create_lanes": (i, [i, C.POINTER(C.POINTER(Params)), C.POINTER(fp), C.POINTER(i),
+                                       C.POINTER(i), i, i, C.POINTER(vp)]),
+        "cel_batch_lanes": (i, [vp]),
         "cel_batch_destroy": (i, [vp]),
         "cel_batch_set_stream": (i, [vp, vp]),
         "cel_batch_step": (i, [vp, i]),
@@ -233,7 +236,8 @@ EXPORTED = [
     "cel_reset_timestep", "cel_timestep", "cel_timesteps", "cel_physical_steps", "cel_get_stats",
     "cel_add_solitary_wave", "cel_get_water_height", "cel_synchronize", "cel_set_bathymetry",
     "cel_batch_set_bathymetry", "cel_batch_add_solitary_wave",
-    "cel_batch_create", "cel_batch_destroy", "cel_batch_set_stream", "cel_batch_step",
+    "cel_batch_create", "cel_batch_create_lanes", "cel_batch_lanes", "cel_batch_destroy", "cel_batch_set_stream",
+    "cel_batch_step",
     "cel_batch_stats", "cel_batch_stats_current", "cel_batch_get_state", "cel_batch_set_state", "cel_batch_get_aux",
     "cel_batch_use_graph", "cel_batch_cells", "cel_batch_set_timestep", "cel_batch_launches_per_step", "cel_set_tuning", "cel_batch_set_tuning",
     "cel_batch_get_tuning", "cel_batch_set_stencil_rows", "cel_batch_set_stencil_width", "cel_batch_stencil_width",

@@ -27,6 +27,7 @@ UNITS = [
     ("logio.cpp", []),
     ("spectrum.cpp", []),
     ("capi.cpp", []),
+    ("lanes.cpp", []),
     ("plain.cu", ["-fmad=false", "-prec-div=true", "-prec-sqrt=true"]),
     ("fused.cu", ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]),
 ]

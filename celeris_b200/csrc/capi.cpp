@@ -321,12 +321,20 @@ int cel_engine_kernel_timing(cel_engine* h, int enable) {
 // ---- batches -------------------------------------------------------------------------------
 int cel_batch_create(int n, const cel_params* const* params, const float* const* bathy, const int* bnx,
                      const int* bny, int form, cel_batch** out) {
+    return cel_batch_create_lanes(n, params, bathy, bnx, bny, form, 0, out);
+}
+
+int cel_batch_create_lanes(int n, const cel_params* const* params, const float* const* bathy, const int* bnx,
+                           const int* bny, int form, int lanes, cel_batch** out) {
     if (n <= 0 || !params || !out || !bathy || !bnx || !bny) { set_error("bad batch arguments"); return CEL_ERR_ARG; }
+    if (lanes < 0) { set_error("lanes must be >= 0 (0 = the default)"); return CEL_ERR_ARG; }
+    for (int i = 0; i < n; ++i)
+        if (!params[i]) { set_error("null member parameters"); return CEL_ERR_ARG; }
     if (form != CEL_FORM_FUSED && form != CEL_FORM_MIXED) { set_error("batches use CEL_FORM_FUSED or CEL_FORM_MIXED"); return CEL_ERR_ARG; }
     if (int st = need_device()) return st;
     CEL_GUARD_BEGIN
     std::string err;
-    cel_batch* b = cel::batch_create(n, params, bathy, bnx, bny, form, err);
+    cel_batch* b = cel::batch_create(n, params, bathy, bnx, bny, form, lanes, err);
     if (!b) { set_error(err); return CEL_ERR_ARG; }
     *out = b;
     return CEL_OK;
@@ -407,19 +415,26 @@ int cel_batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* ms) {
 }
 int cel_batch_kernel_timing(cel_batch* b, int enable) {
     BAT(b);
-    cel::batch_timer(b)->enabled = enable != 0;
+    cel::batch_kernel_timing(b, enable != 0);
     return CEL_OK;
 }
+
+int cel_batch_lanes(const cel_batch* b) { return b ? cel::batch_lanes(b) : 0; }
 
 int cel_kernel_times(void* handle, int is_batch, char (*names)[64], double* total_ms, long long* launches, int cap,
                      int* n) {
     if (!handle || !n) { set_error("null argument"); return CEL_ERR_ARG; }
     CEL_GUARD_BEGIN
-    cel::KernelTimer* t = is_batch ? cel::batch_timer(static_cast<cel_batch*>(handle))
-                                   : static_cast<cel_engine*>(handle)->impl->timer();
-    t->collect();
+    std::vector<cel::KernelTimer::Rec> recs;
+    if (is_batch) {
+        recs = cel::batch_kernel_records(static_cast<cel_batch*>(handle));
+    } else {
+        cel::KernelTimer* t = static_cast<cel_engine*>(handle)->impl->timer();
+        t->collect();
+        recs = t->recs;
+    }
     int k = 0;
-    for (const auto& r : t->recs) {
+    for (const auto& r : recs) {
         if (k >= cap) break;
         if (names) std::snprintf(names[k], 64, "%s", r.name.c_str());
         if (total_ms) total_ms[k] = r.ms;

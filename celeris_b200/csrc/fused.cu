@@ -2082,7 +2082,7 @@ struct Idx {
 
 }  // namespace cel
 
-struct cel_batch {
+struct cel_lane {
     int form = CEL_FORM_FUSED;
     bool mixed = false;
     std::vector<cel::Member> mem;
@@ -2116,6 +2116,7 @@ struct cel_batch {
     bool any_friction = false;
     float* dt_table = nullptr;         // per-member time step on the device
     float* dt_host = nullptr;          // pinned mirror of dt_table
+    cudaEvent_t dt_copied = nullptr;   // recorded after each upload of dt_host
     bool adaptive = false;              // adaptive time steps: dt chosen per member on the device
     cel::DtCtl* ctl = nullptr;          // per-member dt controllers (adaptive batches)
     unsigned int* cfl_now = nullptr;    // per-member max CFL rate of the current state (float bits)
@@ -2172,7 +2173,7 @@ int encode_row_map(CUtensorMap* m, const float* plane, int NX, int NY, int P, st
     return CEL_OK;
 }
 
-int dalloc(cel_batch* b, void** ptr, size_t bytes, std::string& err) {
+int dalloc(cel_lane* b, void** ptr, size_t bytes, std::string& err) {
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) { err = std::string("cudaMalloc: ") + cudaGetErrorString(e); return CEL_ERR_CUDA; }
@@ -2191,7 +2192,7 @@ int dalloc(cel_batch* b, void** ptr, size_t bytes, std::string& err) {
 
 // Uploads a member's state (RGBA texels); `lo3`, when given, holds the mixed form's low words
 // (3 per texel), else they start at zero.
-int upload_state(cel_batch* b, int i, const float* rgba, std::string& err, const float* lo3 = nullptr) {
+int upload_state(cel_lane* b, int i, const float* rgba, std::string& err, const float* lo3 = nullptr) {
     b->step_stats_valid = false;
     Member& m = b->mem[i];
     const MemberDev& d = b->hdev[i];
@@ -2231,7 +2232,7 @@ March2Kernel march2_kernel(bool mixed, bool adapt, int w) {
                  : (adapt ? k_march2<false, true, 128> : k_march2<false, false, 128>);
 }
 
-int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
+int launch_pass(cel_lane* b, const PassArgs& pa, std::string& err) {
     // the launch checks below read the runtime's last-error state: drop what calls outside this pass
     // left there (they reported it, or ignored it, where they happened)
     (void)cudaGetLastError();
@@ -2298,7 +2299,7 @@ int launch_pass(cel_batch* b, const PassArgs& pa, std::string& err) {
 // <logData> output after a physical step (engine.cpp:1488-1493): each member whose step count is a
 // multiple of its logStep writes the state after the step with the time at the step's start, here
 // the member's FP64 clock minus the step's dt, rounded to float.
-int log_after_step(cel_batch* b, std::string& err) {
+int log_after_step(cel_lane* b, std::string& err) {
     if (!b->any_log) return CEL_OK;
     const int count = b->sch.last_count;
     for (size_t i = 0; i < b->mem.size(); ++i) {
@@ -2306,7 +2307,7 @@ int log_after_step(cel_batch* b, std::string& err) {
         const cel_log& lg = m.p.log;
         if (!lg.do_log || count % lg.log_step != 0) continue;
         std::vector<float> host(size_t(m.hs.NX) * m.hs.NY * 4);
-        if (int e = batch_get_state(b, int(i), host.data(), err)) return e;
+        if (int e = lane_get_state(b, int(i), host.data(), err)) return e;
         double t_end = 0;
         float last_dt = b->step_dt[i];   // the dt the clock advanced by at the end of the step
         B_TRY(cudaMemcpyAsync(&t_end, b->hdev[i].time64, sizeof(double), cudaMemcpyDeviceToHost, b->stream));
@@ -2322,7 +2323,7 @@ int log_after_step(cel_batch* b, std::string& err) {
 
 // Adaptive batches: the CFL rate of every member's current state (before the first pass and
 // before each adaptive predictor), then each member's dt for this pass.
-int choose_dt_device(cel_batch* b, bool first_of_step, std::string& err) {
+int choose_dt_device(cel_lane* b, bool first_of_step, std::string& err) {
     const int n = int(b->mem.size());
     const int scheme = b->sch.time_scheme;
     const bool need_cfl = !b->dt_started || scheme == CEL_SCHEME_PREDICTOR_ADAPTIVE;
@@ -2339,7 +2340,7 @@ int choose_dt_device(cel_batch* b, bool first_of_step, std::string& err) {
 }
 
 // One pass with the host state machine; updates the buffer indices.
-int run_pass(cel_batch* b, bool first_of_step, std::string& err) {
+int run_pass(cel_lane* b, bool first_of_step, std::string& err) {
     Scheme& s = b->sch;
     Idx& ix = b->ix;
     if (b->adaptive) {
@@ -2384,14 +2385,14 @@ int run_pass(cel_batch* b, bool first_of_step, std::string& err) {
     return CEL_OK;
 }
 
-int run_physical_step(cel_batch* b, std::string& err) {
+int run_physical_step(cel_lane* b, std::string& err) {
     if (int e = run_pass(b, true, err)) return e;
     while (b->sch.time_scheme == CEL_SCHEME_CORRECTOR)
         if (int e = run_pass(b, false, err)) return e;
     return CEL_OK;
 }
 
-void free_graphs(cel_batch* b) {
+void free_graphs(cel_lane* b) {
     for (cudaGraphExec_t g : b->graphs) cudaGraphExecDestroy(g);
     b->graphs.clear();
     b->graph_idx.clear();
@@ -2399,7 +2400,7 @@ void free_graphs(cel_batch* b) {
 }
 
 // Captures one graph per physical step until the buffer-rotation state repeats.
-int build_graphs(cel_batch* b, std::string& err) {
+int build_graphs(cel_lane* b, std::string& err) {
     free_graphs(b);
     Scheme s0 = b->sch;
     Idx i0 = b->ix;
@@ -2465,7 +2466,7 @@ cudaError_t allow_max_dynamic_smem(const void* kernel) {
     return e;
 }
 
-int configure_work(cel_batch* b, int cw, int mh, int rps, int mw, std::string& err) {
+int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, std::string& err) {
     if (rps != 1 && rps != 2) { err = "stencil rows per step must be 1 or 2"; return CEL_ERR_ARG; }
     if (mw != 128 && mw != 96) { err = "stencil width must be 128 or 96 threads"; return CEL_ERR_ARG; }
     if (rps == 1) mw = MW;   // the one-row stencil has one width
@@ -2546,9 +2547,9 @@ int configure_work(cel_batch* b, int cw, int mh, int rps, int mw, std::string& e
     return CEL_OK;
 }
 
-cel_batch* batch_create(int n, const cel_params* const* params, const float* const* bathy, const int* bnx,
+cel_lane* lane_create(int n, const cel_params* const* params, const float* const* bathy, const int* bnx,
                         const int* bny, int form, std::string& err) {
-    std::unique_ptr<cel_batch> b(new cel_batch());
+    std::unique_ptr<cel_lane> b(new cel_lane());
     b->form = form;
     b->mixed = (form == CEL_FORM_MIXED);
     const int N0 = params[0]->correction_steps;
@@ -2823,7 +2824,7 @@ cel_batch* batch_create(int n, const cel_params* const* params, const float* con
     return b.release();
 }
 
-void batch_destroy(cel_batch* b) {
+void lane_destroy(cel_lane* b) {
     if (!b) return;
     free_graphs(b);
     if (b->stream) cudaStreamSynchronize(b->stream);
@@ -2835,11 +2836,12 @@ void batch_destroy(cel_batch* b) {
     if (b->side) cudaStreamDestroy(b->side);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->dt_copied) cudaEventDestroy(b->dt_copied);
     delete b;
     (void)cudaGetLastError();   // teardown has no caller to report to; leave no stale error behind
 }
 
-int batch_set_stream(cel_batch* b, cudaStream_t s, std::string& err) {
+int lane_set_stream(cel_lane* b, cudaStream_t s, std::string& err) {
     B_TRY(cudaStreamSynchronize(b->stream));
     free_graphs(b);
     if (b->own_stream) cudaStreamDestroy(b->stream);
@@ -2849,7 +2851,7 @@ int batch_set_stream(cel_batch* b, cudaStream_t s, std::string& err) {
     return CEL_OK;
 }
 
-int batch_step(cel_batch* b, int nsteps, std::string& err) {
+int lane_step(cel_lane* b, int nsteps, std::string& err) {
     for (int k = 0; k < nsteps; ++k) {
         const bool bootstrap = b->sch.timestep_count < 3;
         if (b->use_graph && !bootstrap) {
@@ -2883,7 +2885,7 @@ int batch_step(cel_batch* b, int nsteps, std::string& err) {
     return CEL_OK;
 }
 
-int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
+int lane_stats(cel_lane* b, cel_stats* out, bool current, std::string& err) {
     const size_t n = b->mem.size();
     const bool at_step = !current && b->step_stats_valid;
     if (!at_step) {
@@ -2940,7 +2942,7 @@ int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
     return CEL_OK;
 }
 
-int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err) {
+int lane_get_state(cel_lane* b, int i, float* rgba, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     Member& m = b->mem[i];
     const MemberDev& d = b->hdev[i];
@@ -2965,7 +2967,7 @@ int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err) {
     return CEL_OK;
 }
 
-int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err) {
+int lane_set_state(cel_lane* b, int i, const float* rgba, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     return upload_state(b, i, rgba, err);
 }
@@ -2974,7 +2976,7 @@ int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err) {
 // (w - BA_old + BA_new; in double on the compensated state of the mixed form), the bottom planes
 // are resampled from the new grid, the aux planes are cleared; the Thomas factors stay those of
 // the old bottom, as the reference keeps its coefficient textures until a remesh.
-int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, std::string& err) {
+int lane_set_bathymetry(cel_lane* b, int i, const float* z, int bnx, int bny, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     if (!z || bnx < 2 || bny < 2) { err = "bathymetry grid needs at least 2 x 2 values"; return CEL_ERR_ARG; }
     Member& m = b->mem[i];
@@ -3014,7 +3016,7 @@ int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, 
 }
 
 // addSolitaryWave (engine.cpp:2154-2219) on member i; theta in degrees
-int batch_add_solitary_wave(cel_batch* b, int i, double H, double theta_deg, double xc, double yc, std::string& err) {
+int lane_add_solitary_wave(cel_lane* b, int i, double H, double theta_deg, double xc, double yc, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     const HostSetup& hs = b->mem[i].hs;
     const float th = float(theta_deg) * 3.14159274101257324f / 180.0f;
@@ -3029,7 +3031,7 @@ int batch_add_solitary_wave(cel_batch* b, int i, double H, double theta_deg, dou
     return CEL_OK;
 }
 
-int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err) {
+int lane_get_aux(cel_lane* b, int i, float* rgba, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     Member& m = b->mem[i];
     const MemberDev& d = b->hdev[i];
@@ -3047,44 +3049,47 @@ int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err) {
     return CEL_OK;
 }
 
-int batch_use_graph(cel_batch* b, bool enable, std::string& err) {
+int lane_use_graph(cel_lane* b, bool enable, std::string& err) {
     (void)err;
     if (!enable) free_graphs(b);
     b->use_graph = enable;
     return CEL_OK;
 }
 
-long long batch_cells(const cel_batch* b) { return b->cells; }
+long long lane_cells(const cel_lane* b) { return b->cells; }
 
-int batch_set_timestep(cel_batch* b, const float* dt, std::string& err) {
+int lane_set_timestep(cel_lane* b, const float* dt, std::string& err) {
     if (b->adaptive) { err = "an adaptive batch chooses its time steps on the device"; return CEL_ERR_STATE; }
     // the uniform time step of each member (the reference's "uniform time step" setting,
     // uploaded with the constant buffers before every pass, engine.cpp:1728-1750)
-    for (size_t i = 0; i < b->mem.size(); ++i) {
+    for (size_t i = 0; i < b->mem.size(); ++i)
         if (!(dt[i] > 0.f)) { err = "time steps must be > 0"; return CEL_ERR_ARG; }
-        b->dt_host[i] = dt[i];
-    }
+    // the previous upload reads the same pinned buffer: let it finish before the buffer changes
+    if (!b->dt_copied) B_TRY(cudaEventCreateWithFlags(&b->dt_copied, cudaEventDisableTiming));
+    B_TRY(cudaEventSynchronize(b->dt_copied));
+    for (size_t i = 0; i < b->mem.size(); ++i) b->dt_host[i] = dt[i];
     B_TRY(cudaMemcpyAsync(b->dt_table, b->dt_host, sizeof(float) * b->mem.size(), cudaMemcpyHostToDevice, b->stream));
+    B_TRY(cudaEventRecord(b->dt_copied, b->stream));
     return CEL_OK;
 }
 
-int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err) {
+int lane_set_tuning(cel_lane* b, int tx, int ty, int pcr, std::string& err) {
     (void)pcr;   // the solves have no cyclic-reduction stage to hand over from (Thomas factors + scans)
     return configure_work(b, tx > 0 ? tx : b->cw, ty > 0 ? ty : b->mh, b->rows_per_step, b->mw, err);
 }
 
-int batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rps) {
+int lane_get_tuning(const cel_lane* b, int* tx, int* ty, int* rps) {
     if (tx) *tx = b->cw;
     if (ty) *ty = b->mh;
     if (rps) *rps = b->rows_per_step;
     return CEL_OK;
 }
 
-int batch_set_stencil_rows(cel_batch* b, int rps, std::string& err) {
+int lane_set_stencil_rows(cel_lane* b, int rps, std::string& err) {
     return configure_work(b, b->cw, b->mh, rps, rps == 2 ? b->mw : MW, err);
 }
 
-int batch_set_stencil_width(cel_batch* b, int threads, std::string& err) {
+int lane_set_stencil_width(cel_lane* b, int threads, std::string& err) {
     if (b->rows_per_step != 2 && threads != MW) {
         err = "the one-row stencil runs 128-thread strips; select two rows per step first";
         return CEL_ERR_ARG;
@@ -3092,49 +3097,18 @@ int batch_set_stencil_width(cel_batch* b, int threads, std::string& err) {
     return configure_work(b, b->cw, b->mh, b->rows_per_step, threads, err);
 }
 
-int batch_stencil_width(const cel_batch* b) { return b->mw; }
+int lane_stencil_width(const cel_lane* b) { return b->mw; }
 
-// Times `steps` physical steps for every candidate (band width, strip height), in the launch mode
-// the batch is set to (graph replay or direct), two rounds in turn, and keeps the fastest by its
-// better round.  The ensemble advances by every step taken here.
-int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, std::string& err) {
-    if (steps < 1) { err = "autotune needs at least one step per candidate"; return CEL_ERR_ARG; }
-    std::vector<int4> cand;   // band width, strip height, stencil rows per step, stencil width
-    for (int2 v : {make_int2(1, 128), make_int2(2, 128), make_int2(2, 96)})
-        for (int cw : {1, 8, 16, 32})
-            if (cw == 1 || sizeof(float) * size_t(b->max_ny) * cw + 8192 <= 227 * 1024)
-                for (int mh : {32, 64, 128}) cand.push_back(make_int4(cw, mh, v.x, v.y));
-    std::vector<double> best(cand.size(), 1e300);
-    cudaEvent_t e0, e1;
-    B_TRY(cudaEventCreate(&e0));
-    B_TRY(cudaEventCreate(&e1));
-    int rc = CEL_OK;
-    for (int round = 0; round < 2 && !rc; ++round)
-        for (size_t k = 0; k < cand.size() && !rc; ++k) {
-            if ((rc = configure_work(b, cand[k].x, cand[k].y, cand[k].z, cand[k].w, err))) break;
-            if ((rc = batch_step(b, 2, err))) break;   // warm-up (captures the graphs in graph mode)
-            cudaEventRecord(e0, b->stream);
-            if ((rc = batch_step(b, steps, err))) break;
-            cudaEventRecord(e1, b->stream);
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            best[k] = std::min(best[k], double(ms) / steps);
-        }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (rc) return rc;
-    const size_t kb = size_t(std::min_element(best.begin(), best.end()) - best.begin());
-    if ((rc = configure_work(b, cand[kb].x, cand[kb].y, cand[kb].z, cand[kb].w, err))) return rc;
-    if (tx) *tx = cand[kb].x;
-    if (ty) *ty = cand[kb].y;
-    if (best_ms) *best_ms = best[kb];
-    return CEL_OK;
+cudaStream_t lane_stream(const cel_lane* b) { return b->stream; }
+int lane_members(const cel_lane* b) { return int(b->mem.size()); }
+int lane_max_ny(const cel_lane* b) { return b->max_ny; }
+int lane_configure(cel_lane* b, int cw, int mh, int rps, int mw, std::string& err) {
+    return configure_work(b, cw, mh, rps, mw, err);
 }
 
-KernelTimer* batch_timer(cel_batch* b) { return &b->tm; }
+KernelTimer* lane_timer(cel_lane* b) { return &b->tm; }
 
-int batch_launches_per_step(const cel_batch* b) {
+int lane_launches_per_step(const cel_lane* b) {
     int per_pass = 3;  // stencil, row solve, column solve
     for (int s = 0; s < 4; ++s)
         if (b->nbitems[s] > 0) per_pass += b->two_phase[s] ? 2 : 1;
@@ -3148,11 +3122,11 @@ namespace {
 
 class FusedEngine : public EngineIface {
 public:
-    cel_batch* b = nullptr;
+    cel_lane* b = nullptr;
     cel_params p{};
     std::vector<float> bathy;
     int bnx = 0, bny = 0, form = CEL_FORM_FUSED;
-    ~FusedEngine() override { batch_destroy(b); }
+    ~FusedEngine() override { lane_destroy(b); }
     int make() {
         const cel_params* pp = &p;
         const float* bz = bathy.empty() ? nullptr : bathy.data();
@@ -3161,27 +3135,27 @@ public:
             if (int st = read_cbf(p.bathymetry_path, &tmp, bnx, bny, err)) return st;
             bz = tmp.data();
         }
-        b = batch_create(1, &pp, &bz, &bnx, &bny, form, err);
+        b = lane_create(1, &pp, &bz, &bnx, &bny, form, err);
         if (b) b->elapsed_src = &log_elapsed;
         return b ? CEL_OK : CEL_ERR_ARG;
     }
     int remesh() override {
-        batch_destroy(b);
+        lane_destroy(b);
         b = nullptr;
         return make();
     }
-    int set_state(const float* rgba) override { return batch_set_state(b, 0, rgba, err); }
-    int get_state(float* rgba) override { return batch_get_state(b, 0, rgba, err); }
+    int set_state(const float* rgba) override { return lane_set_state(b, 0, rgba, err); }
+    int get_state(float* rgba) override { return lane_get_state(b, 0, rgba, err); }
     int get_bottom(float* b3) override {
         const HostSetup& hs = b->mem[0].hs;
         for (size_t i = 0; i < hs.BA.size(); ++i) { b3[3 * i] = hs.BY[i]; b3[3 * i + 1] = hs.BX[i]; b3[3 * i + 2] = hs.BA[i]; }
         return CEL_OK;
     }
-    int get_aux(float* rgba) override { return batch_get_aux(b, 0, rgba, err); }
+    int get_aux(float* rgba) override { return lane_get_aux(b, 0, rgba, err); }
     int reset_timestep(float, float, cel_stats* out) override {
         if (!b->adaptive) b->sch.choose_dt(0.f);
         if (!out) return CEL_OK;
-        return batch_stats(b, out, true, err);
+        return lane_stats(b, out, true, err);
     }
     int timestep() override { return run_pass(b, b->sch.time_scheme != CEL_SCHEME_CORRECTOR, err); }
     int timesteps(int n) override {
@@ -3189,10 +3163,10 @@ public:
             if (int e = run_pass(b, b->sch.time_scheme != CEL_SCHEME_CORRECTOR, err)) return e;
         return CEL_OK;
     }
-    int physical_steps(int n) override { return batch_step(b, n, err); }
-    int get_stats(cel_stats* out) override { return batch_stats(b, out, true, err); }
+    int physical_steps(int n) override { return lane_step(b, n, err); }
+    int get_stats(cel_stats* out) override { return lane_stats(b, out, true, err); }
     int add_solitary_wave(double Hh, double theta_deg, double xc, double yc) override {
-        return batch_add_solitary_wave(b, 0, Hh, theta_deg, xc, yc, err);
+        return lane_add_solitary_wave(b, 0, Hh, theta_deg, xc, yc, err);
     }
     // the block's depth sum is taken from the current state, in GetStats' order (compute.hlsl:1331-1345)
     int water_height(float x, float y, float* out) override {
@@ -3200,7 +3174,7 @@ public:
         const float W = float(p.width), L = float(p.length);
         if (hs.nx < 4 || hs.ny < 4) { err = "getWaterHeight needs at least one 4x4 block"; return CEL_ERR_STATE; }
         std::vector<float> st(size_t(hs.NX) * hs.NY * 4);
-        if (int e = batch_get_state(b, 0, st.data(), err)) return e;
+        if (int e = lane_get_state(b, 0, st.data(), err)) return e;
         int ix = 0, iy = 0;
         water_height_block(hs.nx, hs.ny, W, L, x, y, ix, iy);
         float sum_h = 0.f;
@@ -3213,19 +3187,19 @@ public:
         return CEL_OK;
     }
     int set_bathymetry(const float* z, int gx, int gy) override {
-        if (int st = batch_set_bathymetry(b, 0, z, gx, gy, err)) return st;
+        if (int st = lane_set_bathymetry(b, 0, z, gx, gy, err)) return st;
         bathy.assign(z, z + size_t(gx) * gy);   // a remesh starts over from the new grid
         bnx = gx;
         bny = gy;
         return CEL_OK;
     }
-    int set_stream(cudaStream_t s) override { return batch_set_stream(b, s, err); }
+    int set_stream(cudaStream_t s) override { return lane_set_stream(b, s, err); }
     int synchronize() override {
         cudaError_t e = cudaStreamSynchronize(b->stream);
         if (e != cudaSuccess) { err = cudaGetErrorString(e); return CEL_ERR_CUDA; }
         return CEL_OK;
     }
-    int set_tuning(int tx, int ty, int pcr) override { return batch_set_tuning(b, tx, ty, pcr, err); }
+    int set_tuning(int tx, int ty, int pcr) override { return lane_set_tuning(b, tx, ty, pcr, err); }
     KernelTimer* timer() override { return &b->tm; }
     int nx() const override { return p.nx; }
     int ny() const override { return p.ny; }

@@ -233,6 +233,15 @@ int cel_set_bathymetry(cel_engine* h, const float* bathy, int bnx, int bny);
  * (compute.hlsl:766-780); a step needs no host readback and replays from a CUDA graph. */
 int cel_batch_create(int n, const cel_params* const* params, const float* const* bathy,
                      const int* bnx, const int* bny, int form, cel_batch** out);
+/* cel_batch_create with the member set split into `lanes` lanes (0 = the default: 2 for two or
+ * more members).  Each lane is advanced by its own launches and CUDA graphs on its own stream,
+ * ordered against the batch stream at every call; lanes run side by side, so one lane's small
+ * boundary launches and kernel tails overlap another lane's stencil.  Members are assigned by
+ * interior cell count (largest first, to the lane with the fewest cells); results do not depend
+ * on the split.  No counterpart in the reference. */
+int cel_batch_create_lanes(int n, const cel_params* const* params, const float* const* bathy,
+                           const int* bnx, const int* bny, int form, int lanes, cel_batch** out);
+int cel_batch_lanes(const cel_batch* b);                 /* lanes of a batch (0 for NULL) */
 int cel_batch_destroy(cel_batch* b);
 int cel_batch_set_stream(cel_batch* b, void* cuda_stream);
 int cel_batch_step(cel_batch* b, int nsteps);            /* physical steps, all members */

@@ -133,6 +133,16 @@ def test_new_entry_points_refuse_null_handles(celeris):
     assert L.cel_spectrum_waves(None, 9.81, 0, None, None) == 1
     assert L.cel_log_dump(None, None, 0.0, 0.0) == 1
     assert L.cel_write_hotstart(None, None, None) == 1
+    assert L.cel_batch_lanes(None) == 0
+    # a negative lane count is refused before any device work
+    p = abi.Params()
+    assert L.cel_params_default(C.byref(p)) == 0
+    pp = (C.POINTER(abi.Params) * 1)(C.pointer(p))
+    zz = (C.POINTER(C.c_float) * 1)(C.cast(z, C.POINTER(C.c_float)))
+    dims = (C.c_int * 1)(4)
+    h = C.c_void_p()
+    assert L.cel_batch_create_lanes(1, pp, zz, dims, dims, 2, -1, C.byref(h)) == 1
+    assert b"lanes" in L.cel_last_error()
 
 
 EXAMPLES = os.environ.get("CELERIS_REFERENCE", "/root/reference") + "/msvc/Examples"
