@@ -29,6 +29,9 @@ int lane_members(const cel_lane* b);
 int lane_max_ny(const cel_lane* b);
 int lane_step(cel_lane* b, int nsteps, std::string& err);
 int lane_stats(cel_lane* b, cel_stats* out, bool current, std::string& err);
+// lane_stats in two halves: enqueue the statistics pass and the read-back copies; then wait and convert
+int lane_stats_enqueue(cel_lane* b, bool current, std::string& err);
+int lane_stats_finish(cel_lane* b, cel_stats* out, bool current, std::string& err);
 int lane_get_state(cel_lane* b, int i, float* rgba, std::string& err);
 int lane_set_state(cel_lane* b, int i, const float* rgba, std::string& err);
 int lane_get_aux(cel_lane* b, int i, float* rgba, std::string& err);

@@ -2119,6 +2119,7 @@ struct cel_lane {
     cudaEvent_t dt_copied = nullptr;   // recorded after each upload of dt_host
     bool adaptive = false;              // adaptive time steps: dt chosen per member on the device
     cel::DtCtl* ctl = nullptr;          // per-member dt controllers (adaptive batches)
+    std::vector<cel::DtCtl> ctl_host;   // their read-back copy (statistics)
     unsigned int* cfl_now = nullptr;    // per-member max CFL rate of the current state (float bits)
     bool dt_started = false;            // the controllers have made their first choice
     size_t smem_rows = 0, smem_cols = 0;
@@ -2886,6 +2887,13 @@ int lane_step(cel_lane* b, int nsteps, std::string& err) {
 }
 
 int lane_stats(cel_lane* b, cel_stats* out, bool current, std::string& err) {
+    if (int e = lane_stats_enqueue(b, current, err)) return e;
+    return lane_stats_finish(b, out, current, err);
+}
+
+// The statistics pass (when the step's own totals do not describe the current state) and the
+// read-back copies, on the lane's stream; lane_stats_finish waits for them.
+int lane_stats_enqueue(cel_lane* b, bool current, std::string& err) {
     const size_t n = b->mem.size();
     const bool at_step = !current && b->step_stats_valid;
     if (!at_step) {
@@ -2903,8 +2911,18 @@ int lane_stats(cel_lane* b, cel_stats* out, bool current, std::string& err) {
         B_TRY(cudaMemcpyAsync(h + head, b->stats_now_all, n * STATS_N * sizeof(double), cudaMemcpyDeviceToHost,
                               b->stream));
     }
-    std::vector<DtCtl> ctl(b->adaptive ? n : 0);
-    if (b->adaptive) B_TRY(cudaMemcpyAsync(ctl.data(), b->ctl, n * sizeof(DtCtl), cudaMemcpyDeviceToHost, b->stream));
+    b->ctl_host.resize(b->adaptive ? n : 0);
+    if (b->adaptive)
+        B_TRY(cudaMemcpyAsync(b->ctl_host.data(), b->ctl, n * sizeof(DtCtl), cudaMemcpyDeviceToHost, b->stream));
+    return CEL_OK;
+}
+
+int lane_stats_finish(cel_lane* b, cel_stats* out, bool current, std::string& err) {
+    const size_t n = b->mem.size();
+    const bool at_step = !current && b->step_stats_valid;
+    const double* h = b->rb_host;
+    const size_t head = 1 + n;
+    const std::vector<DtCtl>& ctl = b->ctl_host;
     B_TRY(cudaStreamSynchronize(b->stream));
     const double late = h[0];
     const double* t64 = h + 1;

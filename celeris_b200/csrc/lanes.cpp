@@ -193,15 +193,19 @@ int batch_step(cel_batch* b, int nsteps, std::string& err) {
 }
 
 int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
+    // every lane's read-back is queued before the first wait, so the copies overlap.  No fork or
+    // join: the statistics read only what the lanes' own streams wrote, and the call returns after
+    // everything it read has arrived.
+    for (cel_lane* ln : b->lanes)
+        if (int e = lane_stats_enqueue(ln, current, err)) return e;
     std::vector<cel_stats> tmp;
-    size_t l = 0;
-    return each(b, err, [&](cel_lane* ln) {
-        const std::vector<int>& ms = b->members[l++];
+    for (size_t l = 0; l < b->lanes.size(); ++l) {
+        const std::vector<int>& ms = b->members[l];
         tmp.resize(ms.size());
-        if (int e = lane_stats(ln, tmp.data(), current, err)) return e;
+        if (int e = lane_stats_finish(b->lanes[l], tmp.data(), current, err)) return e;
         for (size_t k = 0; k < ms.size(); ++k) out[ms[k]] = tmp[k];
-        return int(CEL_OK);
-    });
+    }
+    return CEL_OK;
 }
 
 int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err) {
@@ -238,14 +242,19 @@ long long batch_cells(const cel_batch* b) {
 }
 
 int batch_set_timestep(cel_batch* b, const float* dt, std::string& err) {
+    // No fork or join: each lane copies the host values into its pinned buffer and uploads them on
+    // its own stream, ahead of its next step.  Every value is checked first, so that a refused
+    // call changes no lane.
+    for (size_t i = 0; i < b->lane_of.size(); ++i)
+        if (!(dt[i] > 0.f)) { err = "time steps must be > 0"; return CEL_ERR_ARG; }
     std::vector<float> part;
-    size_t l = 0;
-    return each(b, err, [&](cel_lane* ln) {
-        const std::vector<int>& ms = b->members[l++];
+    for (size_t l = 0; l < b->lanes.size(); ++l) {
+        const std::vector<int>& ms = b->members[l];
         part.resize(ms.size());
         for (size_t k = 0; k < ms.size(); ++k) part[k] = dt[ms[k]];
-        return lane_set_timestep(ln, part.data(), err);   // copies into the lane's pinned buffer
-    });
+        if (int e = lane_set_timestep(b->lanes[l], part.data(), err)) return e;
+    }
+    return CEL_OK;
 }
 
 int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err) {

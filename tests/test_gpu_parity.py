@@ -176,6 +176,26 @@ def test_lanes_change_concurrency_not_results(celeris, adaptive):
             assert t[i]["timestep"] == t1[i]["timestep"]
 
 
+def test_refused_time_steps_change_no_lane(celeris):
+    """A per-member time step array with one invalid entry is refused as a whole: no lane takes
+    the valid entries (the bad entry is tried at every member, so it lands in every lane)."""
+    members = [_case(k, nx=40 + 8 * i, ny=24, N=1)[:4] for i, k in enumerate(["solid", "mixed", "sponge"])]
+    a = celeris.Batch([(m[0], m[1]) for m in members], "mixed", lanes=2)
+    b = celeris.Batch([(m[0], m[1]) for m in members], "mixed", lanes=2)
+    a.step(5)
+    b.step(5)
+    half = np.array([0.5 * m[0].timestep for m in members], dtype=np.float32)
+    for j in range(len(members)):
+        bad = half.copy()
+        bad[j] = -1.0
+        with pytest.raises(celeris.CelError, match="> 0"):
+            a.set_timestep(bad)
+    a.step(5)
+    b.step(5)
+    for i in range(len(members)):
+        np.testing.assert_array_equal(a.state(i), b.state(i))
+
+
 def test_batch_graph_replay_matches_direct(celeris):
     members = [_case(k, nx=48, ny=32, N=1)[:4] for k in ["mixed", "sponge", "irregular"]]
     b1 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
