@@ -7,6 +7,8 @@
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -194,6 +196,25 @@ def test_refused_time_steps_change_no_lane(celeris):
     b.step(5)
     for i in range(len(members)):
         np.testing.assert_array_equal(a.state(i), b.state(i))
+
+
+def test_batch_member_index_checks(celeris):
+    """Member indices are the caller's whatever the lane split; one outside [0, n) is an argument
+    error for every per-member call, and the batch stays usable."""
+    members = [_case(k, nx=40, ny=24, N=1)[:4] for k in ["solid", "mixed", "sponge"]]
+    b = celeris.Batch([(m[0], m[1]) for m in members], "mixed", lanes=2)
+    z = members[0][1]
+    L = celeris.lib()
+    buf = np.zeros((28, 44, 4), dtype=np.float32)
+    for i in (-1, 3):
+        assert L.cel_batch_get_state(b.h, i, buf.ctypes.data_as(C.POINTER(C.c_float))) == 1
+        assert b"range" in L.cel_last_error()
+        with pytest.raises(celeris.CelError, match="range"):
+            b.add_solitary_wave(i, 0.1, 0.0, 10.0, 10.0)
+        with pytest.raises(celeris.CelError, match="range"):
+            b.set_bathymetry(i, z)
+    b.step(3)
+    assert all(st["health"] == 0 for st in b.stats())
 
 
 def test_batch_graph_replay_matches_direct(celeris):
