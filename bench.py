@@ -3,8 +3,9 @@
 
 Default workload: configuration C4 — a 64-domain uneven ensemble (sizes drawn by seed from
 256^2, 512x256, 1024x512, 1024^2, 2048x512; seeded slopes, bumps and sine wave-makers) advanced
-by the batched mixed-precision form (one launch per phase for all domains, each physical step a
-replayed CUDA graph), with correctionStepsNum = 1 (AB3 predictor + AM4 corrector).
+by the batched mixed-precision form (one launch per phase for the domains of each lane, each
+physical step a replayed CUDA graph per lane, two lanes side by side on concurrent streams),
+with correctionStepsNum = 1 (AB3 predictor + AM4 corrector).
 
 One JSON line on rank 0:
   value     whole-job Gcell-steps/s with the state resident in HBM (device clock, CUDA events,
@@ -12,7 +13,8 @@ One JSON line on rank 0:
   e2e       the same through the public C ABI with, every step, a host->device upload of the
             per-member time steps from pinned memory and a device->host read of the step's
             statistics (mass, energy, CFL — what resetTimestep reads back every pass);
-  roofline  the dominant kernel (the fused stencil) timed live with CUDA events on its stream;
+  roofline  the dominant kernel (the fused stencil) timed live with CUDA events on its stream
+            (lanes one after another while timed, so each launch's span is its own);
   cpu_baseline  the FP32 transcription (OpenMP, all host threads) on a bounded sample.
 ``--impl reference`` times the CPU implementation of the path (the reference's own shader code
 compiled for the CPU when that build is present, else the FP32 transcription) on the same
