@@ -3,8 +3,8 @@
 // The members are split into lanes of about equal interior cell counts; each lane is a complete
 // batched engine (fused.cu) with its own stream, work lists and CUDA graphs.  Lane 0 runs on the
 // batch's stream (the caller's, once set); every other lane has its own non-blocking stream that
-// waits for the batch stream at the start of each call (fork) and that the batch stream waits for
-// at its end (join), so to the caller a batch behaves as one stream-ordered object.  A step
+// waits for the batch stream at the start of each call (a fork) and that the batch stream waits
+// for at its end (a join), so to the caller a batch behaves as one stream-ordered object.  A step
 // launches the lanes' graphs in turn, one physical step at a time, and the GPU runs them side by
 // side: one lane's boundary strips, clock advance and kernel tails, which leave most SMs idle,
 // overlap another lane's stencil.  Every member's arithmetic is the same in any lane, so the
@@ -47,7 +47,7 @@ namespace {
 cudaStream_t batch_stream(const cel_batch* g) { return lane_stream(g->lanes[0]); }
 
 // lanes 1.. wait for the work the batch stream holds so far
-int fork(cel_batch* g, std::string& err) {
+int fork_lanes(cel_batch* g, std::string& err) {
     if (g->lanes.size() < 2) return CEL_OK;
     G_TRY(cudaEventRecord(g->ev_fork, batch_stream(g)));
     for (size_t l = 1; l < g->lanes.size(); ++l) G_TRY(cudaStreamWaitEvent(lane_stream(g->lanes[l]), g->ev_fork, 0));
@@ -55,7 +55,7 @@ int fork(cel_batch* g, std::string& err) {
 }
 
 // the batch stream waits for the work of lanes 1..
-int join(cel_batch* g, std::string& err) {
+int join_lanes(cel_batch* g, std::string& err) {
     for (size_t l = 1; l < g->lanes.size(); ++l) {
         G_TRY(cudaEventRecord(g->ev_lane[l], lane_stream(g->lanes[l])));
         G_TRY(cudaStreamWaitEvent(batch_stream(g), g->ev_lane[l], 0));
@@ -66,12 +66,12 @@ int join(cel_batch* g, std::string& err) {
 // f(lane) for every lane, between a fork and a join
 template <class F>
 int each(cel_batch* g, std::string& err, F f) {
-    if (int e = fork(g, err)) return e;
+    if (int e = fork_lanes(g, err)) return e;
     int rc = CEL_OK;
     for (cel_lane* l : g->lanes)
         if ((rc = f(l))) break;
     std::string jerr;
-    const int rj = join(g, jerr);
+    const int rj = join_lanes(g, jerr);
     if (!rc && rj) err = jerr;
     return rc ? rc : rj;
 }
@@ -85,10 +85,10 @@ int check_member(const cel_batch* g, int i, std::string& err) {
 template <class F>
 int on_member(cel_batch* g, int i, std::string& err, F f) {
     if (int e = check_member(g, i, err)) return e;
-    if (int e = fork(g, err)) return e;
+    if (int e = fork_lanes(g, err)) return e;
     const int rc = f(g->lanes[g->lane_of[i]], g->slot_of[i]);
     std::string jerr;
-    const int rj = join(g, jerr);
+    const int rj = join_lanes(g, jerr);
     if (!rc && rj) err = jerr;
     return rc ? rc : rj;
 }
@@ -172,7 +172,7 @@ int batch_set_stream(cel_batch* b, cudaStream_t s, std::string& err) {
 
 int batch_step(cel_batch* b, int nsteps, std::string& err) {
     if (nsteps < 0) { err = "negative step count"; return CEL_ERR_ARG; }
-    if (int e = fork(b, err)) return e;
+    if (int e = fork_lanes(b, err)) return e;
     const size_t L = b->lanes.size();
     if (b->timing && L > 1) {
         // kernel timing: each lane takes all its steps after the previous lane has finished, so
@@ -189,7 +189,7 @@ int batch_step(cel_batch* b, int nsteps, std::string& err) {
             for (cel_lane* l : b->lanes)
                 if (int e = lane_step(l, 1, err)) return e;
     }
-    return join(b, err);
+    return join_lanes(b, err);
 }
 
 int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err) {
