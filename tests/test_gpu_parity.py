@@ -217,6 +217,32 @@ def test_batch_member_index_checks(celeris):
     assert all(st["health"] == 0 for st in b.stats())
 
 
+def test_lanes_follow_the_callers_stream(celeris):
+    """A 2-lane batch moved onto a caller's stream mid-run and back (lane 0 runs on it, lane 1
+    forks from it and joins it; the switch drains lane 1 and recaptures lane 0's graphs): the
+    same fields as a batch that stays on its own stream."""
+    import torch
+    members = [_case(k, nx=48 + 8 * i, ny=32, N=1)[:4] for i, k in enumerate(["solid", "mixed", "sponge", "irregular"])]
+    ref = celeris.Batch([(m[0], m[1]) for m in members], "mixed", lanes=2)
+    ref.use_graph(True)
+    ref.step(30)
+    b = celeris.Batch([(m[0], m[1]) for m in members], "mixed", lanes=2)
+    b.use_graph(True)
+    b.step(10)
+    s = torch.cuda.Stream()
+    b.set_stream(s.cuda_stream)
+    b.step(10)
+    done = torch.cuda.Event()
+    done.record(s)
+    done.synchronize()
+    after = b.stats()
+    b.set_stream(None)
+    b.step(10)
+    for i in range(len(members)):
+        np.testing.assert_array_equal(b.state(i), ref.state(i))
+    assert all(st["health"] == 0 for st in after)
+
+
 def test_batch_graph_replay_matches_direct(celeris):
     members = [_case(k, nx=48, ny=32, N=1)[:4] for k in ["mixed", "sponge", "irregular"]]
     b1 = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
