@@ -47,8 +47,8 @@ extern "C" {
 
 /* Solver forms */
 #define CEL_FORM_PLAIN 0  /* FP32, one kernel per reference pass and per CR level */
-#define CEL_FORM_FUSED 1  /* FP32, fused stencil + PCR/Thomas tridiagonal */
-#define CEL_FORM_MIXED 2  /* fused, FP16 coefficients, compensated state, FP64 time/reductions */
+#define CEL_FORM_FUSED 1  /* FP32, fused stencil + Thomas factors solved as scans */
+#define CEL_FORM_MIXED 2  /* fused, compensated (two-sum) state, FP64 clock and reductions */
 
 /* Time schemes (settings.hpp:298: enum TimeIntegrationScheme) */
 #define CEL_SCHEME_EULER 0

@@ -172,3 +172,42 @@ def test_reference_example_inputs_parse(celeris):
     ready = seen.get("conical_island_ready.cml")
     if ready is not None:
         assert ready.log.do_log == 1 and ready.log.n_gauges == 5 and ready.log.n_ranges == 2
+
+
+def test_cpp_engine_adapter_compiles_and_links(tmp_path, celeris):
+    """include/celeris_b200_engine.hpp, the ShallowWaterEngine stand-in a host program includes,
+    compiles against the C header and links the built library.  Without a GPU, creating an engine
+    throws the library's message as a C++ exception; with one, the engine is created."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no g++")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.dirname(abi.LIB_PATH)
+    (tmp_path / "case.cml").write_text("<E><gridSize nx = 4 ny = 4></gridSize></E>")
+    (tmp_path / "host.cpp").write_text(r"""
+#include "celeris_b200_engine.hpp"
+#include <cstdio>
+int main(int argc, char** argv) {
+    std::vector<float> z(16, -1.0f);
+    try {
+        CelerisB200Engine e(argv[1], z, 4, 4);
+        std::printf("created %d\n", e.params().nx);
+    } catch (const std::exception& ex) {
+        std::printf("error: %s\n", ex.what());
+    }
+    std::printf("version %s\n", cel_version());
+    return 0;
+}
+""")
+    exe = tmp_path / "host"
+    cmd = [gxx, "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(root, "include"), str(tmp_path / "host.cpp"),
+           "-L", libdir, "-lceleris_b200", "-Wl,-rpath," + libdir, "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe), str(tmp_path / "case.cml")], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    lines = out.stdout.splitlines()
+    assert lines[0] == "created 4" or lines[0].startswith("error: "), lines
+    assert lines[-1].startswith("version ")
