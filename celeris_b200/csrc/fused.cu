@@ -1746,6 +1746,72 @@ __device__ float3 irregular_tree(const BoundaryDesc& b, const float4* waves, flo
     return stk[0];
 }
 
+// The same pairwise tree restricted to the aligned power-of-two range of components [m0, m1),
+// continuing from `carry`, the sum of the aligned range of carry_size components just before m0
+// (carry_size 0: none).  Padding components (m >= nreal) are blocks of sea level in eta and 0 in
+// hu, hv; every block sum is an exact power-of-two multiple of the sea level, so any grouping of
+// them rounds identically.
+__device__ float3 irregular_range(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, double t64,
+                                  bool use64, float dh, float g, int nreal, int m0, int m1, float3 carry,
+                                  int carry_size) {
+    float3 stk[17];
+    int sz[17];
+    int top = 0;
+    if (carry_size > 0) { stk[0] = carry; sz[0] = carry_size; top = 1; }
+    int m = m0;
+    while (m < m1) {
+        float3 v;
+        int s;
+        if (m < nreal) {
+            float e, hu, hv;
+            const float4 wv = waves[b.wave_offset + m];
+            if (use64) sine_wave_t64(xx, yy, t64, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
+            else sine_wave(xx, yy, t, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
+            v = make_float3(e + b.sea_level, hu, hv);
+            s = 1;
+        } else {
+            s = (m == 0) ? m1 : (m & -m);
+            while (m + s > m1) s >>= 1;
+            v = make_float3(float(s) * b.sea_level, 0.f, 0.f);
+        }
+        m += s;
+        stk[top] = v;
+        sz[top] = s;
+        ++top;
+        while (top >= 2 && sz[top - 1] == sz[top - 2]) {
+            const float3 r = stk[top - 1], l = stk[top - 2];
+            stk[top - 2] = make_float3(l.x + r.x, l.y + r.y, l.z + r.z);
+            sz[top - 2] *= 2;
+            --top;
+        }
+    }
+    return stk[0];
+}
+
+// irregular_tree with the work spread over a warp (all 32 lanes call it; lane 0's result is the
+// sum).  The real components lie in [0, R), R the smallest power of two >= their count: the lanes
+// take equal aligned parts of it, a pairwise shuffle tree joins the parts in the same tree shape,
+// and the padding up to nleaf follows on top.  The result is bit-identical to irregular_tree.
+__device__ float3 irregular_warp(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, double t64,
+                                 bool use64, float dh, float g, int lane) {
+    const float3 zero = make_float3(0.f, 0.f, 0.f);
+    const int nreal = (dh > CEL_MIN_DEPTH) ? min(b.n_waves, b.nleaf) : 0;
+    if (nreal == 0) return irregular_range(b, waves, xx, yy, t, t64, use64, dh, g, 0, 0, b.nleaf, zero, 0);
+    int R = 1;
+    while (R < nreal) R <<= 1;
+    const int A = min(32, R), per = R / A;
+    float3 v = zero;
+    if (lane < A) v = irregular_range(b, waves, xx, yy, t, t64, use64, dh, g, nreal, lane * per, (lane + 1) * per, zero, 0);
+    for (int off = 1; off < A; off <<= 1) {   // A is the same on every lane
+        const float ox = __shfl_down_sync(0xffffffffu, v.x, off);
+        const float oy = __shfl_down_sync(0xffffffffu, v.y, off);
+        const float oz = __shfl_down_sync(0xffffffffu, v.z, off);
+        if ((lane & (2 * off - 1)) == 0) v = make_float3(v.x + ox, v.y + oy, v.z + oz);
+    }
+    if (R < b.nleaf) v = irregular_range(b, waves, xx, yy, t, t64, use64, dh, g, nreal, R, b.nleaf, v, R);
+    return v;
+}
+
 __device__ void uts_lookup(const float* tab, int n, float t, float out[3]) {
     // timeSeriesHelper (engine.cpp:1882-1904) for a table sorted by time: the first row at or
     // after t (from row 1 on), linear interpolation from the row before; zero past the end.
@@ -1766,6 +1832,7 @@ __device__ void uts_lookup(const float* tab, int n, float t, float out[3]) {
 
 constexpr int BND_CPT = 4;
 constexpr int BND_CELLS = 256 * BND_CPT;
+constexpr int BND_IRR_CELLS = 256 / 32;   // irregular wave-maker strips: one cell per warp
 
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ mems, const int2* __restrict__ items,
@@ -1821,6 +1888,29 @@ __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ 
                 HU[gi[k]] = gam * vu[k];
                 HV[gi[k]] = gam * vv[k];
                 if (MIXED) { M.L[out][0][gi[k]] = gam * l0[k]; M.L[out][1][gi[k]] = gam * l1[k]; M.L[out][2][gi[k]] = gam * l2[k]; }
+            }
+            continue;
+        }
+        if (b.type == CEL_BC_IRREGULAR && phase == 0) {
+            // one cell per warp, its components spread over the lanes (BND_IRR_CELLS per item)
+            const int lane = threadIdx.x & 31;
+            const int cell = wi.y + (threadIdx.x >> 5);
+            if (cell >= sw * sh) continue;   // warp-uniform
+            const int x = x0 + cell % sw, y = y0 + cell / sw;
+            const size_t gi = size_t(y) * P + x;
+            const bool colwise = (side == 1 || side == 3);
+            const int along = colwise ? y : x;
+            const int lim = colwise ? c.ny : c.nx;
+            float3 r = make_float3(0.f, 0.f, 0.f);
+            if (along >= 2 && along < lim + 2) {
+                const float dh = fmaxf(0.f, b.sea_level - M.BA[gi]);
+                const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
+                const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
+                r = irregular_warp(b, M.waves, xx, yy, *M.time32, *M.time64, MIXED, dh, c.g, lane);
+            }
+            if (lane == 0) {
+                W[gi] = r.x; HU[gi] = r.y; HV[gi] = r.z;
+                if (MIXED) { M.L[out][0][gi] = 0.f; M.L[out][1][gi] = 0.f; M.L[out][2][gi] = 0.f; }
             }
             continue;
         }
@@ -2726,7 +2816,9 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
                 d.nuts[s] = bb.n_uts;
             }
             const int cellsn = (s == 0 || s == 2) ? NX * std::min(bb.width, NY) : std::min(bb.width, NX) * NY;
-            for (int c0 = 0; c0 < cellsn; c0 += (bb.type == CEL_BC_SPONGE ? BND_CELLS : 256)) bitems[s].push_back(make_int2(i, c0));
+            for (int c0 = 0; c0 < cellsn;
+                 c0 += (bb.type == CEL_BC_SPONGE ? BND_CELLS : bb.type == CEL_BC_IRREGULAR ? BND_IRR_CELLS : 256))
+                bitems[s].push_back(make_int2(i, c0));
             // a solid strip wider than 2 reads ghost cells of its own strip: compute, then write
             if (bb.type == CEL_BC_SOLID && bb.width >= 3) b->two_phase[s] = true;
         }
