@@ -17,6 +17,16 @@ oracle/_ref/ (git-ignored; they travel with the tree like the other built librar
   unchanged (plus a small ``boost/scoped_array.hpp`` stand-in and ``ref_host.cpp``), giving the
   reference's own ``.cbf`` reader and bathymetry sampling (BY/BX/BA).
 
+* ``libref_spectrum.so``: the reference's spectrum wave-maker, ``generateSpectrumWaves``
+  (``engine.cpp:3559-3776``), cut out of ``engine.cpp`` by brace matching and turned into a free
+  function by four textual substitutions (the engine's gravity setting, Boost's ``lgamma``, the log
+  folder and the clock seed of ``srand``; see ``ref_spectrum.cpp``), then compiled with
+  ``ref_spectrum.cpp``.  The rest of ``engine.cpp`` is never compiled.
+
+It also copies the reference's example inputs (``msvc/Examples``: ``.cml`` settings, ``.cbf``
+grids, wave and time-series files) to ``oracle/_ref/examples``, where the tests that parse and
+run them look; nothing else reads the reference tree.
+
 ``engine.cpp`` itself is not buildable here (Direct3D 11, Windows headers, Boost), so the pass
 schedule driving the shader is the oracle's restatement of it.
 
@@ -27,6 +37,7 @@ from __future__ import annotations
 
 import os
 import re
+import shutil
 import subprocess
 import sys
 
@@ -66,6 +77,36 @@ def transform_hlsl(src: str) -> str:
     return s
 
 
+def extract_function(src: str, head: str) -> str:
+    """The text of the function whose definition starts with `head`, through its closing brace."""
+    i = src.index(head)
+    k = src.index("{", i)
+    depth = 0
+    while True:
+        if src[k] == "{":
+            depth += 1
+        elif src[k] == "}":
+            depth -= 1
+            if depth == 0:
+                return src[i:k + 1]
+        k += 1
+
+
+def transform_spectrum(fn: str) -> str:
+    subs = [
+        (r"std::string\s+ShallowWaterEngine::generateSpectrumWaves\s*\(", "static std::string ref_generateSpectrumWaves("),
+        (r"GetSetting\s*\(\s*\"gravity\"\s*\)", "ref_gravity"),
+        (r"boost::math::lgamma\s*<\s*float\s*>\s*\(", "ref_lgammaf("),
+        (r"initSetting\.logPath", "ref_log_path"),
+        (r"srand\s*\(\s*time\s*\(\s*0\s*\)\s*\)", "srand(ref_seed)"),
+    ]
+    for pat, rep in subs:
+        fn, n = re.subn(pat, rep, fn)
+        if n == 0:
+            raise RuntimeError("spectrum extraction: pattern not found: " + pat)
+    return fn
+
+
 def run(cmd):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -95,6 +136,17 @@ def build(ref_root: str | None = None) -> bool:
     run([CXX, *FLAGS, "-include", "cstring", "-include", "string", "-I", os.path.join(OUT, "shim"), "-I", ref_root,
          os.path.join(ref_root, "terrain_heightfield.cpp"), os.path.join(ref_root, "settings.cpp"),
          os.path.join(HERE, "ref_host.cpp"), "-o", os.path.join(OUT, "libref_host.so")])
+    # the spectrum wave-maker, cut out of engine.cpp
+    with open(os.path.join(ref_root, "engine.cpp"), encoding="latin-1") as f:
+        eng = f.read().replace("\r\n", "\n")
+    fn = transform_spectrum(extract_function(eng, "std::string ShallowWaterEngine::generateSpectrumWaves("))
+    with open(os.path.join(OUT, "spectrum_ref.inc"), "w") as f:
+        f.write("// generated from the reference's engine.cpp (generateSpectrumWaves) by oracle/ref_build.py\n" + fn)
+    run([CXX, *FLAGS, "-include", "cstring", "-include", "string", "-I", OUT, "-I", ref_root,
+         os.path.join(HERE, "ref_spectrum.cpp"), "-o", os.path.join(OUT, "libref_spectrum.so")])
+    examples = os.path.join(ref_root, "msvc", "Examples")
+    if os.path.isdir(examples):
+        shutil.copytree(examples, os.path.join(OUT, "examples"), dirs_exist_ok=True)
     return True
 
 

@@ -145,7 +145,8 @@ def test_new_entry_points_refuse_null_handles(celeris):
     assert b"lanes" in L.cel_last_error()
 
 
-EXAMPLES = os.environ.get("CELERIS_REFERENCE", "/root/reference") + "/msvc/Examples"
+# the reference's example inputs, copied next to its checkers by oracle/ref_build.py
+EXAMPLES = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "examples")
 
 
 @pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="the reference's example folder is not present")

@@ -100,7 +100,8 @@ def test_terrain_change_matches_reference_shader():
     np.testing.assert_array_equal(out[0], out[1])
 
 
-EXAMPLES = os.environ.get("CELERIS_REFERENCE", "/root/reference") + "/msvc/Examples"
+# the reference's example inputs, copied next to its checkers by oracle/ref_build.py
+EXAMPLES = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "examples")
 
 
 @pytest.mark.skipif(not (os.path.exists(REF_SHADER) and os.path.isdir(EXAMPLES)),
