@@ -172,6 +172,23 @@ def ensemble_member(nx: int, ny: int, rng: np.random.Generator, correction_steps
     return p, B.astype(np.float32), nx, ny
 
 
+def c4_sizes(members: int = 64, first_member: int = 0) -> list:
+    """(nx, ny) of C4 members first_member .. first_member+members-1, without building them."""
+    return [C4_SIZES[int(np.random.default_rng(12345 + 4000 + m).integers(0, len(C4_SIZES)))]
+            for m in range(first_member, first_member + members)]
+
+
+def c5_sizes(members: int = 1024, first_member: int = 0) -> list:
+    """(nx, ny) of C5 members first_member .. first_member+members-1, without building them."""
+    sizes = list(range(128, 513, 32))
+    out = []
+    for m in range(first_member, first_member + members):
+        rng = np.random.default_rng(12345 + 5000 + m)
+        nx = sizes[int(rng.integers(0, len(sizes)))]
+        out.append((nx, sizes[int(rng.integers(0, len(sizes)))]))
+    return out
+
+
 def config4(members: int = 64, correction_steps: int = 1, first_member: int = 0):
     """C4: 64 domains with sizes drawn by seed from C4_SIZES (``first_member`` offsets the seeds,
     e.g. per rank of a multi-GPU run)."""

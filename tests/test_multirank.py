@@ -1,9 +1,11 @@
 """The multi-GPU path's host logic on CPU ranks (gloo, world size 2).
 
-bench.py shards the ensemble by domain: rank r runs members r*count .. r*count+count-1 of the
-seeded list (weak scaling, no collective inside a step), and the job's rate is every rank's
-cells over the slowest rank's time.  Here two CPU processes check both: the shards are the
-right, disjoint slices of one ensemble, and the max/sum reductions give the job rate.
+bench.py shards ensembles by domain, with no collective inside a step.  Weak scaling: rank r runs
+members r*count .. r*count+count-1 of the seeded list.  Strong scaling: one fixed ensemble is split
+over the ranks by cost (interior cells, largest member first to the least-loaded rank).  The job's
+rate is every rank's cells over the slowest rank's time.  Here two CPU processes check the weak
+shards (the right, disjoint slices of one ensemble), the strong shards (disjoint, complete and
+balanced to within 5 % of the cells) and the max/sum reductions that give the job rate.
 """
 from __future__ import annotations
 
@@ -76,3 +78,48 @@ def test_ensemble_shards_and_job_rate():
         assert ms_max == 11.0                                  # the slowest rank's time
         assert tot == total                                    # every rank's cells
         assert abs(rate - total * 100 / (11.0 / 1e3) / 1e9) < 1e-9
+
+
+def _rank_strong(rank: int, world: int, port: int, out):
+    sys.path.insert(0, ROOT)
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        members, _ = bench.members_for("c4", rank, 16, world, "strong")
+        mine = [(int(p.nx), int(p.ny), float(np.asarray(z, np.float64).sum())) for p, z, _, _ in members]
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        out.put((rank, gathered))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_strong_scaling_splits_one_ensemble_by_cost():
+    from celeris_b200 import cases
+    from celeris_b200.shards import partition_by_cost
+    world, port = 2, _port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank_strong, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    gathered = res[0][1]
+    assert gathered == res[1][1]                               # both ranks see the same shards
+    whole = [(int(p.nx), int(p.ny), float(np.asarray(z, np.float64).sum())) for p, z, _, _ in cases.config4(16)]
+    flat = [m for shard in gathered for m in shard]
+    assert sorted(flat) == sorted(whole)                       # disjoint and complete
+    cells = [sum(nx * ny for nx, ny, _ in shard) for shard in gathered]
+    assert max(cells) <= 1.05 * sum(cells) / world             # balanced
+    # the full 64-member ensemble over 2, 4 and 8 ranks
+    sizes = [nx * ny for nx, ny in cases.c4_sizes(64)]
+    for w in (2, 4, 8):
+        shards = partition_by_cost(sizes, w)
+        assert sorted(i for s in shards for i in s) == list(range(64))
+        load = [sum(sizes[i] for i in s) for s in shards]
+        assert max(load) <= 1.05 * sum(sizes) / w, (w, load)
