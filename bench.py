@@ -18,8 +18,10 @@ One JSON line on rank 0:
   cpu_baseline  the FP32 transcription (OpenMP, all host threads) on a bounded sample.
 ``--impl reference`` times the CPU implementation of the path (the reference's own shader code
 compiled for the CPU when that build is present, else the FP32 transcription) on the same
-metric.  Multi-GPU (torchrun): every rank runs its own ensemble (weak scaling), no collective in
-the step.
+metric, over every member of the workload.  Multi-GPU (torchrun): with ``--scaling weak`` (the
+default) rank r runs members r*count .. r*count+count-1 of the seeded list, so each GPU holds a
+full ensemble; with ``--scaling strong`` one ensemble is split over the ranks by cost (interior
+cells, largest first to the least-loaded rank).  No collective runs inside a step.
 """
 from __future__ import annotations
 
@@ -61,11 +63,26 @@ def parse():
     ap.add_argument("--band-width", type=int, default=0, help="force the column band width after tuning (0 keeps it)")
     ap.add_argument("--strip-height", type=int, default=0, help="force the stencil strip height after tuning (0 keeps it)")
     ap.add_argument("--tune-steps", type=int, default=6, help="steps per autotuner candidate (0 keeps the defaults)")
+    ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
+                    help="weak: a full ensemble per GPU; strong: one ensemble split over the GPUs by cost")
+    ap.add_argument("--accuracy-steps", type=int, default=-1,
+                    help="FP64-oracle check of one sampled member after the run (-1: when the oracle can "
+                         "finish it in about a minute, 0: skip)")
     return ap.parse_args()
 
 
-def members_for(cfg: str, rank: int, count: int):
+def members_for(cfg: str, rank: int, count: int, world: int = 1, scaling: str = "weak"):
+    """This rank's members and the workload's name.  Weak scaling gives every rank its own seeded
+    block of `count` members; strong scaling splits one ensemble of `count` members over `world`
+    ranks by cost (celeris_b200.shards)."""
     from celeris_b200 import cases
+    if scaling == "strong" and cfg in ("c4", "c5"):
+        from celeris_b200.shards import partition_by_cost
+        sizes = cases.c4_sizes(count) if cfg == "c4" else cases.c5_sizes(count)
+        mine = partition_by_cost([nx * ny for nx, ny in sizes], world)[rank]
+        build = cases.config4 if cfg == "c4" else cases.config5
+        return [build(1, 1, first_member=k)[0] for k in mine], \
+            f"{cfg.upper()} {count}-domain ensemble split over {world} GPU(s) by cost (members {mine[0]}..)"
     if cfg == "c4":
         return cases.config4(count, 1, first_member=rank * count), \
             f"C4 {count}-domain uneven ensemble (256^2..2048x512, dx=1 m, slope+bumps, sine wave-maker, N/S solid, E sponge)"
@@ -113,12 +130,24 @@ class Clocks:
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.index, self.q = index, q
         self.f = open(self.path, "w")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
                                        "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+
+    def once(self):
+        """One sample now.  Called right after the timed work is queued (the GPU is busy with it),
+        so that even a timed region shorter than the sampling period has a sample under load."""
+        try:
+            r = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.q}", "--format=csv,noheader,nounits"],
+                               capture_output=True, text=True, timeout=20)
+            self.f.write(r.stdout)
+            self.f.flush()
+        except Exception:
+            pass
 
     def stop(self) -> dict:
         if self.p is None:
@@ -166,6 +195,34 @@ def cpu_sample(seconds: float, members):
     return rate, O.threads("f32"), f"{n} physical steps of one {p.nx}x{p.ny} member (FP32 transcription, OpenMP)"
 
 
+def sampled_member_accuracy(batch, members, steps_cap: int):
+    """The smallest member of the benchmarked batch, as it stands after every step the run took,
+    against the FP64 oracle stepped as many times from the same initial condition: eta RMS over the
+    interior (m) and the relative difference of the FP64 water volume.  The member's FP64 clock
+    gives its step count exactly (it sums the float time step once per step).  Skipped when the
+    oracle would need more than about a minute (steps_cap < 0) or more than steps_cap steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    k = min(range(len(members)), key=lambda i: members[i][0].nx * members[i][0].ny)
+    p, z, bnx, bny = members[k]
+    st = batch.stats_current()[k]
+    dt = float(np.float32(p.timestep))
+    nsteps = int(round(st["total_time"] / dt))
+    o = O.Oracle(p, z, bnx, bny, "f64")
+    t_probe = o.time_physical_steps(4)
+    limit = steps_cap if steps_cap > 0 else int(60.0 / max(t_probe / 4, 1e-6))
+    if nsteps > limit:
+        return {"member": k, "steps": nsteps, "skipped": f"the FP64 oracle would need {nsteps} steps (cap {limit})"}
+    o.physical_steps(nsteps - 4)
+    ref = o.state()
+    got = batch.state(k)
+    d = got[2:-2, 2:-2, 0].astype(np.float64) - ref[2:-2, 2:-2, 0]
+    m_ref = o.reset_timestep()["mass_full"]
+    return {"member": k, "size": [int(p.nx), int(p.ny)], "steps": nsteps,
+            "eta_rms_m": float(np.sqrt(np.mean(d * d))), "eta_max_abs_m": float(np.max(np.abs(d))),
+            "mass_rel_diff": float(abs(st["mass_full"] - m_ref) / m_ref), "health": int(st["health"])}
+
+
 def member_k(cfg: str, k: int):
     """Member k of a workload alone (without building the others)."""
     from celeris_b200 import cases
@@ -176,40 +233,49 @@ def member_k(cfg: str, k: int):
     return members_for(cfg, 0, 1)[0][0]
 
 
-def _ref_worker(cfg, k, seconds, barrier, out):
-    """One process of the reference arm: the reference-shader build stepping member k."""
+def _ref_worker(cfg, ks, seconds, barrier, out):
+    """One process of the reference arm: the reference-shader build stepping members `ks` in turn,
+    each for an equal share of `seconds` (one domain at a time per process)."""
     sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
     import oracle as O
-    p, z, bnx, bny = member_k(cfg, k)
-    o = O.Oracle(p, z, bnx, bny, "ref")
-    o.physical_steps(1)
     barrier.wait(timeout=600)
-    steps, t = 0, 0.0
-    while t < seconds:
-        t += o.time_physical_steps(1)
-        steps += 1
-    out.put((k, p.nx * p.ny, steps, t))
+    work, t = 0, 0.0
+    for k in ks:
+        p, z, bnx, bny = member_k(cfg, k)
+        o = O.Oracle(p, z, bnx, bny, "ref")
+        o.physical_steps(1)
+        tk, steps = 0.0, 0
+        while tk < seconds / len(ks) or steps == 0:
+            tk += o.time_physical_steps(1)
+            steps += 1
+        work += p.nx * p.ny * steps
+        t += tk
+        del o
+    out.put((ks, work, t))
 
 
 def reference_pool(cfg: str, count: int, seconds: float):
-    """The reference-shader build on every host core at once: one spawned process per core, each
-    stepping a different member (the build's texture bindings are process-wide, as a D3D
-    context's are, so one process runs one domain).  Rate = all cell-steps / the longest time."""
+    """The reference-shader build on every host core at once: one spawned process per core, the
+    workload's members dealt out to them in turn (member k to process k mod cores), each process
+    stepping its members one after another (the build's texture bindings are process-wide, as a D3D
+    context's are, so one process runs one domain at a time).  Rate = all cell-steps / the longest
+    process time."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     cores = max(1, min(len(os.sched_getaffinity(0)), count))
     barrier, out = ctx.Barrier(cores), ctx.Queue()
-    procs = [ctx.Process(target=_ref_worker, args=(cfg, k, seconds, barrier, out)) for k in range(cores)]
+    shares = [list(range(c, count, cores)) for c in range(cores)]
+    procs = [ctx.Process(target=_ref_worker, args=(cfg, ks, seconds, barrier, out)) for ks in shares]
     for q in procs:
         q.start()
-    res = [out.get(timeout=1800) for _ in procs]
+    res = [out.get(timeout=3600) for _ in procs]
     for q in procs:
         q.join(timeout=60)
-    work = sum(cells * steps for _, cells, steps, _ in res)
-    t = max(t for *_, t in res)
-    steps = sum(r[2] for r in res)
-    sample = (f"{steps} physical steps over members 0..{cores - 1} ({cores} processes at once, one member each; "
-              f"the reference's compute.hlsl compiled for the CPU)")
+    work = sum(r[1] for r in res)
+    t = max(r[2] for r in res)
+    sample = (f"all {count} members, about {seconds / max(len(s) for s in shares):.1f} s of stepping each "
+              f"({cores} processes at once, members dealt out in turn; the reference's compute.hlsl compiled "
+              f"for the CPU)")
     return work / t, cores, sample
 
 
@@ -224,7 +290,10 @@ def reference_arm(args):
     # the reference's own compute.hlsl compiled for the CPU (oracle/_ref, built from the reference
     # sources), when that build is present, on all host cores
     if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_shader.so")):
-        rate, cores, sample = reference_pool(args.config, len(members), max(1.0, args.cpu_seconds))
+        # about 4 s of stepping per member on each process, whatever the member count
+        cores = max(1, min(len(os.sched_getaffinity(0)), len(members)))
+        per_proc = -(-len(members) // cores)
+        rate, cores, sample = reference_pool(args.config, len(members), max(1.0, args.cpu_seconds / 3.0) * per_proc)
         kind = "reference"
     else:   # the FP32 restatement with OpenMP
         rate, cores, sample = cpu_sample(max(1.0, args.cpu_seconds), members)
@@ -257,7 +326,7 @@ def main():
     dev = torch.cuda.current_device()
     import celeris_b200 as cb
 
-    members, workload = members_for(args.config, rank, args.members)
+    members, workload = members_for(args.config, rank, args.members, world, args.scaling)
     for m in members:
         if args.correction_steps >= 0:
             m[0].correction_steps = args.correction_steps
@@ -295,6 +364,7 @@ def main():
     e0.record(stream)
     batch.step(args.steps)
     e1.record(stream)
+    clk.once()   # the steps are queued and running
     torch.cuda.synchronize()
     clocks = clk.stop()
     ms = e0.elapsed_time(e1)
@@ -304,7 +374,7 @@ def main():
     # ---- end to end through the C ABI: pinned dt upload + stats readback every step -------
     n = batch.n
     dt_pinned = torch.tensor([float(np.float32(m[0].timestep)) for m in members], dtype=torch.float32).pin_memory()
-    e2e_steps = max(5, args.steps // 4)
+    e2e_steps = args.steps
     barrier()
     t0 = time.perf_counter()
     e0.record(stream)
@@ -369,37 +439,45 @@ def main():
     shares = {k: round(v[0] / total_kernel_ms, 4) for k, v in kt.items()} if total_kernel_ms > 0 else {}
     step_bytes = cb.byte_model(args.form, N)[1]
 
-    # ---- per-domain plain FP32 form (the comparison form) ---------------------------------
-    plain = None
-    if not args.no_plain and rank == 0 and args.config in ("c4", "c5"):
-        engines = [cb.Engine(m[0], m[1], "plain") for m in members]
+    # ---- per-domain forms (the comparison): each member its own engine, launched one after another
+    def per_domain(form: str, psteps: int = 30):
+        engines = [cb.Engine(m[0], m[1], form) for m in members]
         for e in engines:
             e.set_stream(stream.cuda_stream)
         for e in engines:
             e.physical_steps(3)
         torch.cuda.synchronize()
-        psteps = 10
         e0.record(stream)
         for _ in range(psteps):
             for e in engines:
                 e.physical_steps(1)
         e1.record(stream)
         torch.cuda.synchronize()
-        plain = cells * psteps / (e0.elapsed_time(e1) / 1e3) / 1e9
-        del engines
+        rate = cells * psteps / (e0.elapsed_time(e1) / 1e3) / 1e9
+        for e in engines:
+            e.close()
+        return rate
 
-    # ---- CPU baseline (rank 0, N=1) ---------------------------------------------------------
-    cpu = None
+    plain = fused_pd = None
+    if not args.no_plain and rank == 0 and args.config in ("c4", "c5"):
+        plain = per_domain("plain")          # the reference's pass structure, FP32
+        fused_pd = per_domain("fused")       # this design's kernels, FP32, but one domain per launch set
+
+    # ---- CPU leg (rank 0, N=1): the FP32 transcription timed, and the FP64 oracle as the checker
+    # of one sampled member of the benchmarked batch ------------------------------------------------
+    cpu = accuracy = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0:
         rate, cores, sample = cpu_sample(args.cpu_seconds, members)
         cpu = {"value": rate / 1e9, "unit": "Gcell-steps/s", "cores": cores, "kind": "port", "sample": sample}
+        if args.accuracy_steps != 0 and not args.adaptive:
+            accuracy = sampled_member_accuracy(batch, members, args.accuracy_steps)
 
     if rank == 0:
         out = {
             "metric": "Gcell-steps/s", "value": value, "unit": "Gcell-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload, "form": args.form, "members_per_gpu": len(members),
                        "cells_per_gpu": cells, "correction_steps": N, "adaptive": bool(args.adaptive), "cuda_graph": not args.no_graph,
@@ -411,7 +489,12 @@ def main():
                                   "stencil_rows_per_step": batch.stencil_rows,
                                   "stencil_threads_per_strip": batch.stencil_width,
                                   "autotuned": tuned is not None,
-                                  "pcr_switch": "none (Thomas factors + scans; no cyclic-reduction stage)"}},
+                                  "pcr_switch": {
+                                      "column_chunks": batch.col_chunks,
+                                      "rows_per_chunk_tallest_member": -(-max(m[0].ny for m in members) // batch.col_chunks),
+                                      "meaning": "column solver: L and U sweeps split into this many chunks per "
+                                                 "column, joined by warp-shuffle recursive doubling, each chunk "
+                                                 "swept serially (Thomas)"}}},
             "e2e": {"value": e2e_value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -429,6 +512,9 @@ def main():
             "cpu_baseline": cpu,
             "plain_per_domain": plain,
             "vs_plain_per_domain": (value / world / plain) if plain else None,
+            "fused_per_domain": fused_pd,
+            "vs_fused_per_domain": (value / world / fused_pd) if fused_pd else None,
+            "accuracy": accuracy,
         }
         print(json.dumps(out), flush=True)
     batch.close()

@@ -239,9 +239,15 @@ class Batch:
         z = np.ascontiguousarray(z, dtype=np.float32)
         check(lib().cel_batch_set_bathymetry(self.h, i, _fp(z), z.shape[1], z.shape[0]))
 
-    def set_tuning(self, band_width: int = 0, strip_height: int = 0):
-        """Column-solver band width (8/16/32) and stencil strip height (0 keeps the current value)."""
-        check(lib().cel_batch_set_tuning(self.h, band_width, strip_height, 0))
+    def set_tuning(self, band_width: int = 0, strip_height: int = 0, chunks: int = 0):
+        """Column-solver band width (1/8/16/32), stencil strip height and the column solver's chunks
+        per column (0 keeps the current value)."""
+        check(lib().cel_batch_set_tuning(self.h, band_width, strip_height, chunks))
+
+    @property
+    def col_chunks(self) -> int:
+        """Chunks per column of the column solver (rows per chunk = ceil(ny / chunks))."""
+        return int(lib().cel_batch_col_chunks(self.h))
 
     @property
     def tuning(self) -> tuple:

@@ -190,6 +190,7 @@ def _declare(L: C.CDLL) -> None:
         "cel_batch_stats": (i, [vp, C.POINTER(Stats)]),
         "cel_batch_stats_current": (i, [vp, C.POINTER(Stats)]),
         "cel_batch_get_tuning": (i, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "cel_batch_col_chunks": (i, [vp]),
         "cel_batch_set_stencil_rows": (i, [vp, i]),
         "cel_batch_set_stencil_width": (i, [vp, i]),
         "cel_batch_stencil_width": (i, [vp]),
@@ -240,7 +241,7 @@ EXPORTED = [
     "cel_batch_step",
     "cel_batch_stats", "cel_batch_stats_current", "cel_batch_get_state", "cel_batch_set_state", "cel_batch_get_aux",
     "cel_batch_use_graph", "cel_batch_cells", "cel_batch_set_timestep", "cel_batch_launches_per_step", "cel_set_tuning", "cel_batch_set_tuning",
-    "cel_batch_get_tuning", "cel_batch_set_stencil_rows", "cel_batch_set_stencil_width", "cel_batch_stencil_width",
+    "cel_batch_get_tuning", "cel_batch_col_chunks", "cel_batch_set_stencil_rows", "cel_batch_set_stencil_width", "cel_batch_stencil_width",
     "cel_batch_autotune",
     "cel_batch_kernel_timing", "cel_engine_kernel_timing", "cel_kernel_times", "cel_byte_model", "cel_stats_noalloc",
 ]

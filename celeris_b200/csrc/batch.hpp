@@ -45,8 +45,10 @@ int lane_get_tuning(const cel_lane* b, int* tx, int* ty, int* rps);
 int lane_set_stencil_rows(cel_lane* b, int rps, std::string& err);
 int lane_set_stencil_width(cel_lane* b, int threads, std::string& err);
 int lane_stencil_width(const cel_lane* b);
-// column band width, strip height, stencil rows per step, stencil width in one call
-int lane_configure(cel_lane* b, int cw, int mh, int rps, int mw, std::string& err);
+// column band width, strip height, stencil rows per step, stencil width, column solver threads in one call
+int lane_configure(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::string& err);
+int lane_col_threads(const cel_lane* b);
+int lane_col_chunks(const cel_lane* b);   // chunks per column of the column solver (1: serial columns)
 KernelTimer* lane_timer(cel_lane* b);
 int lane_launches_per_step(const cel_lane* b);
 void byte_model(int form, int correction_steps, double& stencil_bytes, double& step_bytes);
@@ -70,6 +72,7 @@ long long batch_cells(const cel_batch* b);
 int batch_set_timestep(cel_batch* b, const float* dt, std::string& err);
 int batch_set_tuning(cel_batch* b, int tx, int ty, int pcr, std::string& err);
 int batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rps);
+int batch_col_chunks(const cel_batch* b);
 int batch_set_stencil_rows(cel_batch* b, int rps, std::string& err);
 int batch_set_stencil_width(cel_batch* b, int threads, std::string& err);
 int batch_stencil_width(const cel_batch* b);

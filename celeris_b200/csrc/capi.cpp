@@ -400,6 +400,7 @@ int cel_batch_get_tuning(const cel_batch* b, int* tx, int* ty, int* rows_per_ste
     if (!b) { set_error("null batch"); return CEL_ERR_ARG; }
     return cel::batch_get_tuning(b, tx, ty, rows_per_step);
 }
+int cel_batch_col_chunks(const cel_batch* b) { return b ? cel::batch_col_chunks(b) : 0; }
 int cel_batch_set_stencil_width(cel_batch* b, int threads) {
     BAT(b);
     CEL_GUARD_BEGIN BRET(cel::batch_set_stencil_width(b, threads, err)); CEL_GUARD_END

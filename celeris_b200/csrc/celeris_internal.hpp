@@ -83,6 +83,8 @@ struct BoundaryDesc {
     int n_waves;
     int nleaf;          // 2^(K-1): components summed by the reference's pairwise tree
     int wave_offset;    // into the engine's device wave table (float4 per component)
+    // the same settings unrounded, for the compensated form's FP64 strip values
+    double sea_level64, amplitude64, period64, theta64;
 };
 
 SimConsts make_consts(const cel_params& p, const HostSetup& s, int pitch);

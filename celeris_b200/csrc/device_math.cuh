@@ -119,22 +119,5 @@ __device__ __forceinline__ void sine_wave(float x, float y, float t, float d, fl
     hv = c * t_sin(th) * e;
 }
 
-// The same with the phase omega*t evaluated in FP64 and reduced modulo 2*pi before the FP32
-// sine (the mixed form's wave-maker phase).
-__device__ __forceinline__ void sine_wave_t64(float x, float y, double t, float d, float amp, float period,
-                                              float th, float phase, float g, float& e, float& hu, float& hv) {
-    const double omega_d = 2.0 * 3.14159265358979323846 / double(period);
-    const float omega = float(omega_d);
-    const float k = omega * omega / (g * sqrtf(tanhf(omega * omega * d / g)));
-    const float c = omega / k;
-    const float kx = cosf(th) * x * k;
-    const float ky = sinf(th) * y * k;
-    double ph = omega_d * t;
-    ph -= 6.283185307179586476925 * floor(ph / 6.283185307179586476925);
-    e = amp * sinf(float(ph) - kx - ky + phase);
-    hu = c * cosf(th) * e;
-    hv = c * sinf(th) * e;
-}
-
 }  // namespace
 }  // namespace cel

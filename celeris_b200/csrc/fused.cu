@@ -43,18 +43,19 @@ namespace cel {
 namespace {
 
 constexpr int TX = 32, TY = 16;
-// column solver threads per CTA: CW columns x (NTC/CW) chunks.  1024 threads at one CTA per SM
-// (64 registers) measured slower on C4 than 512 at two: 10.07 with 32-column bands and 9.67 with
-// 16, against 10.34 Gcell-steps/s; a CTA's barriers and carry scans then stall the whole SM.
-#ifndef CEL_COLS_THREADS
-#define CEL_COLS_THREADS 512
-#endif
-constexpr int NTC = CEL_COLS_THREADS;
-// column solver CTAs per SM the build targets: 2 (64 registers, no spills); 1 lets the compiler take
-// about 100 registers and run one CTA per SM, 3 spills (measured on C4: 8.9 / 10.3 / 9.2 Gcell-steps/s)
+// column solver threads per CTA: CW columns x (NT/CW) chunks, NT 256 or 512 (a tuning choice; the
+// chunk length is the solver's switch point from the parallel carry scan to serial sweeps).  1024
+// threads at one CTA per SM (64 registers) measured slower on C4 than 512 at two: 10.07 with
+// 32-column bands and 9.67 with 16, against 10.34 Gcell-steps/s; a CTA's barriers and carry scans
+// then stall the whole SM.
+constexpr int NTC_DEFAULT = 512;
+// column solver CTAs per SM the build targets at 512 threads: 2 (64 registers, no spills); 1 lets
+// the compiler take about 100 registers and run one CTA per SM, 3 spills (measured on C4: 8.9 / 10.3
+// / 9.2 Gcell-steps/s).  256-thread CTAs target twice as many, at the same 64 registers.
 #ifndef CEL_COLS_MIN_CTAS
 #define CEL_COLS_MIN_CTAS 2
 #endif
+constexpr int cols_min_ctas(int nt) { return CEL_COLS_MIN_CTAS * 512 / nt; }
 constexpr int STATS_N = 12;
 
 // stats accumulator layout
@@ -82,9 +83,12 @@ struct MemberDev {
     const float* FYF[3];    // y-systems: c', inv_den, m
     BoundaryDesc bd[4];     // N, E, S, W
     const float4* waves;
+    const double* waves64;  // the same components in FP64, 4 per component (compensated form)
     const float* uts[4];    // (t, eta, hu, hv) tables, float
+    const double* uts64[4]; // the same tables in FP64 (compensated form)
     int nuts[4];
-    float* strip;
+    double dx64, dy64, g64; // grid spacing and gravity in FP64 (the compensated form's strip values)
+    float* strip;           // two-phase strips: 3 floats per cell (6 with the low words)
     double* stats;
     double* stats_now;
     double* time64;
@@ -203,6 +207,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     for (int k = 0; k < polls; ++k)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+// After a wait gave up: before the CTA exits, wait (bounded) for the copies still in flight into its
+// ring, i.e. on every slot for the phase of the last row requested into it.  Rows carry sequence
+// numbers 0, 1, ... in request order; row q goes to slot q % ring and completes phase (q / ring) & 1.
+__device__ __forceinline__ void drain_ring(unsigned long long* bars, int ring, unsigned requested) {
+    for (int s = 0; s < ring; ++s) {
+        if (requested <= unsigned(s)) continue;
+        const unsigned q = unsigned(s) + unsigned(ring) * ((requested - 1u - unsigned(s)) / unsigned(ring));
+        (void)mbar_wait_bounded(&bars[s], (q / unsigned(ring)) & 1u, 1 << 22);
+    }
 }
 __device__ __forceinline__ void tma_row(float* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
     asm volatile(
@@ -359,6 +373,7 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
     }
     __syncthreads();
     unsigned seq = 0;          // rows requested by this CTA so far (the same value in every thread)
+    unsigned requested = 0;    // thread 0: sequence number of the last row it requested, plus one
     bool tma_late = false;
     const float* W = ring;
     const float* HU = ring + FSTR;
@@ -407,7 +422,10 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
         const float* __restrict__ Lbase = B + (9 + 3 * (corr ? pa.cur : pa.in)) * PL;
         float* __restrict__ Lout = B + (9 + 3 * pa.out) * PL;
 
+        const unsigned seq0 = seq;
         auto issue = [&](int row, int sl_) {   // one thread: request the 6 fields of a row into slot sl_
+            if (tma_late) return;                // a wait gave up: request nothing more
+            requested = seq0 + unsigned(row - (y0 - 2)) + 1u;
             mbar_expect_tx(&bars[sl_], ROW_BYTES);
             float* dst = ring + sl_ * RSTR;
             tma_row(dst, tm + pa.in * 3 + 0, xs, row, &bars[sl_]);
@@ -437,7 +455,6 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
         float eh = 0.f, eu = 0.f, ev = 0.f;       // east face of row t (this column), from the last step
         float ypv0 = 0.f, ypv1 = 0.f, ypv2 = 0.f; // y flux below the current row
 
-        const unsigned seq0 = seq;
         const int sA = int(seq0 % RING), sB = next_slot(sA), sC = next_slot(sB);  // rows y0-2, y0-1, y0
 
         __syncthreads();  // the previous strip is done with shared memory
@@ -676,7 +693,10 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
     }
     // a bounded TMA wait that gave up anywhere in this CTA marks the whole pass (the host reports
     // it as a CUDA error of the batch)
-    if (__syncthreads_or(tma_late) && tid == 0) atomic_max_nonneg(pa.late_flag, 1.0);
+    if (__syncthreads_or(tma_late) && tid == 0) {
+        drain_ring(bars, RING, requested);
+        atomic_max_nonneg(pa.late_flag, 1.0);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -835,6 +855,7 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
     }
     __syncthreads();
     unsigned seq = 0;          // rows requested by this CTA so far (the same value in every thread)
+    unsigned requested = 0;    // thread 0: sequence number of the last row it requested, plus one
     bool tma_late = false;
     const float* W = ring;
     const float* HU = ring + FSTR2;
@@ -888,6 +909,8 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
         auto slot_of = [&](int r) { return int((seq0 + unsigned(r - (y0 - 2))) % RING2); };
         auto par_of = [&](int r) { return ((seq0 + unsigned(r - (y0 - 2))) / RING2) & 1u; };
         auto issue = [&](int row) {   // one thread: request the 6 fields of a row into its slot
+            if (tma_late) return;       // a wait gave up: request nothing more
+            requested = seq0 + unsigned(row - (y0 - 2)) + 1u;
             const int sl_ = slot_of(row);
             const int ry = min(row, NYm1);          // rows past the domain are never used; load the last
             mbar_expect_tx(&bars[sl_], ROW_BYTES);
@@ -1235,7 +1258,10 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
             }
         }
     }
-    if (__syncthreads_or(tma_late) && tid == 0) atomic_max_nonneg(pa.late_flag, 1.0);
+    if (__syncthreads_or(tma_late) && tid == 0) {
+        drain_ring(bars, RING2, requested);
+        atomic_max_nonneg(pa.late_flag, 1.0);
+    }
 }
 
 // Stats of the current state only (resetTimestep on demand).
@@ -1463,13 +1489,16 @@ __global__ void __launch_bounds__(256) k_rows(const MemberDev* __restrict__ mems
     }
 }
 
-template <bool MIXED, int CW>
-__global__ void __launch_bounds__(NTC, CEL_COLS_MIN_CTAS) k_cols(const MemberDev* __restrict__ mems, const int2* __restrict__ bands,
+template <bool MIXED, int CW, int NT>
+__global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev* __restrict__ mems, const int2* __restrict__ bands,
                                               int nbands, PassArgs pa) {
     // Column (y) solves: a CTA takes a band of CW adjacent columns, thread (c, k) runs chunk k of
-    // column c; a half warp reads CW consecutive floats of one row.  Every loop over a chunk's rows
-    // issues the loads of CU rows before using them, so each thread keeps several rows of
-    // requests in flight (the recurrences themselves are serial).
+    // column c; CW consecutive threads read CW consecutive floats of one row.  Every loop over a
+    // chunk's rows issues the loads of CU rows before using them, so each thread keeps several rows
+    // of requests in flight (the recurrences themselves are serial).  The chunks' transfer maps are
+    // joined by recursive doubling over the chunks of a column (warp shuffles), i.e. parallel
+    // reduction of the L and U sweeps down to chunks of ceil(ny / NCH) rows swept serially.
+    constexpr int NTC = NT;
     constexpr int NCH = NTC / CW;
     // carry scans: one warp per column; each of the first LN lanes holds G consecutive chunks
     constexpr int G = NCH >= 32 ? NCH / 32 : 1;
@@ -1705,45 +1734,40 @@ __global__ void __launch_bounds__(128) k_cols_serial(const MemberDev* __restrict
 
 // ---------------------------------------------------------------------------------------------
 // Boundary strips (compute.hlsl:985-1309), one side per launch over every member.
-// work item: {member, first strip cell}; 256 strip cells per item, or BND_CELLS for a sponge strip,
-// whose threads take BND_CPT cells each and issue all their loads before the first store (the
-// narrow strips of the other kinds keep one cell per thread, so they still spread over the SMs).
+// work item: {member, first strip cell}; 256 strip cells per item, BND_CELLS for a sponge strip
+// (its threads take BND_CPT cells each and issue all their loads before the first store), and
+// BND_IRR_CELLS for an irregular wave-maker strip (one cell per warp, its components spread over
+// the lanes).  The narrow strips of the other kinds keep one cell per thread, so they still spread
+// over the SMs.
 // phase 0: compute and write in place; 1: compute into the member's scratch; 2: copy back.
+// The compensated form evaluates the sponge, sine, irregular and time-series values in FP64 and
+// stores them as a float pair (value + low word), so the strips keep the state's precision.
 // ---------------------------------------------------------------------------------------------
-__device__ float3 irregular_tree(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, double t64,
-                                 bool use64, float dh, float g) {
-    float3 stk[17];
-    int sz[17];
-    int top = 0;
-    const int nreal = (dh > CEL_MIN_DEPTH) ? min(b.n_waves, b.nleaf) : 0;
-    int m = 0;
-    while (m < b.nleaf) {
-        float3 v;
-        int s;
-        if (m < nreal) {
-            float e, hu, hv;
-            const float4 wv = waves[b.wave_offset + m];
-            if (use64) sine_wave_t64(xx, yy, t64, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
-            else sine_wave(xx, yy, t, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
-            v = make_float3(e + b.sea_level, hu, hv);
-            s = 1;
-        } else {
-            s = (m == 0) ? b.nleaf : (m & -m);
-            while (m + s > b.nleaf) s >>= 1;
-            v = make_float3(float(s) * b.sea_level, 0.f, 0.f);
-        }
-        m += s;
-        stk[top] = v;
-        sz[top] = s;
-        ++top;
-        while (top >= 2 && sz[top - 1] == sz[top - 2]) {
-            const float3 r = stk[top - 1], l = stk[top - 2];
-            stk[top - 2] = make_float3(l.x + r.x, l.y + r.y, l.z + r.z);
-            sz[top - 2] *= 2;
-            --top;
-        }
-    }
-    return stk[0];
+constexpr double CEL_PI_D = 3.14159265358979323846;
+constexpr double CEL_MIN_DEPTH_D = 0.0001;   // compute.hlsl:1062
+
+// v as a float pair: hi = v rounded, lo = the rest rounded
+__device__ __forceinline__ void split_hl(double v, float& hi, float& lo) {
+    hi = float(v);
+    lo = float(v - double(hi));
+}
+
+// SpongeFunction (compute.hlsl:1056-1059) in FP64
+__device__ __forceinline__ double sponge_fn_d(double L, double x) {
+    return 0.5 + 0.5 * cos(CEL_PI_D * fmax(L - x, 0.0) / L);
+}
+
+// sineWave with Eckart's wavenumber (compute.hlsl:1080-1101) in FP64
+__device__ __forceinline__ void sine_wave_d(double x, double y, double t, double d, double amp, double period, double th,
+                                            double phase, double g, double& e, double& hu, double& hv) {
+    const double omega = 2.0 * CEL_PI_D / period;
+    const double k = omega * omega / (g * sqrt(tanh(omega * omega * d / g)));
+    const double c = omega / k;
+    double sth, cth;
+    sincos(th, &sth, &cth);
+    e = amp * sin(omega * t - cth * x * k - sth * y * k + phase);
+    hu = c * cth * e;
+    hv = c * sth * e;
 }
 
 // The same pairwise tree restricted to the aligned power-of-two range of components [m0, m1),
@@ -1751,9 +1775,8 @@ __device__ float3 irregular_tree(const BoundaryDesc& b, const float4* waves, flo
 // (carry_size 0: none).  Padding components (m >= nreal) are blocks of sea level in eta and 0 in
 // hu, hv; every block sum is an exact power-of-two multiple of the sea level, so any grouping of
 // them rounds identically.
-__device__ float3 irregular_range(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, double t64,
-                                  bool use64, float dh, float g, int nreal, int m0, int m1, float3 carry,
-                                  int carry_size) {
+__device__ float3 irregular_range(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, float dh,
+                                  float g, int nreal, int m0, int m1, float3 carry, int carry_size) {
     float3 stk[17];
     int sz[17];
     int top = 0;
@@ -1765,8 +1788,7 @@ __device__ float3 irregular_range(const BoundaryDesc& b, const float4* waves, fl
         if (m < nreal) {
             float e, hu, hv;
             const float4 wv = waves[b.wave_offset + m];
-            if (use64) sine_wave_t64(xx, yy, t64, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
-            else sine_wave(xx, yy, t, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
+            sine_wave(xx, yy, t, dh, wv.x, wv.y, wv.z, wv.w, g, e, hu, hv);
             v = make_float3(e + b.sea_level, hu, hv);
             s = 1;
         } else {
@@ -1788,55 +1810,113 @@ __device__ float3 irregular_range(const BoundaryDesc& b, const float4* waves, fl
     return stk[0];
 }
 
-// irregular_tree with the work spread over a warp (all 32 lanes call it; lane 0's result is the
-// sum).  The real components lie in [0, R), R the smallest power of two >= their count: the lanes
-// take equal aligned parts of it, a pairwise shuffle tree joins the parts in the same tree shape,
-// and the padding up to nleaf follows on top.  The result is bit-identical to irregular_tree.
-__device__ float3 irregular_warp(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, double t64,
-                                 bool use64, float dh, float g, int lane) {
+// The irregular wave-maker value (compute.hlsl:1196-1212: the components' sineWave values summed
+// over a balanced pairwise tree of nleaf leaves, the first n_waves real, the rest sea level) with
+// the work spread over a warp (all 32 lanes call it; lane 0's result is the sum).  The real
+// components lie in [0, R), R the smallest power of two >= their count: the lanes take equal
+// aligned parts of it, a pairwise shuffle tree joins the parts in the same tree shape, and the
+// padding up to nleaf follows on top, so the result is bit-identical to the sequential tree.
+__device__ float3 irregular_warp(const BoundaryDesc& b, const float4* waves, float xx, float yy, float t, float dh,
+                                 float g, int lane) {
     const float3 zero = make_float3(0.f, 0.f, 0.f);
     const int nreal = (dh > CEL_MIN_DEPTH) ? min(b.n_waves, b.nleaf) : 0;
-    if (nreal == 0) return irregular_range(b, waves, xx, yy, t, t64, use64, dh, g, 0, 0, b.nleaf, zero, 0);
+    if (nreal == 0) return irregular_range(b, waves, xx, yy, t, dh, g, 0, 0, b.nleaf, zero, 0);
     int R = 1;
     while (R < nreal) R <<= 1;
     const int A = min(32, R), per = R / A;
     float3 v = zero;
-    if (lane < A) v = irregular_range(b, waves, xx, yy, t, t64, use64, dh, g, nreal, lane * per, (lane + 1) * per, zero, 0);
+    if (lane < A) v = irregular_range(b, waves, xx, yy, t, dh, g, nreal, lane * per, (lane + 1) * per, zero, 0);
     for (int off = 1; off < A; off <<= 1) {   // A is the same on every lane
         const float ox = __shfl_down_sync(0xffffffffu, v.x, off);
         const float oy = __shfl_down_sync(0xffffffffu, v.y, off);
         const float oz = __shfl_down_sync(0xffffffffu, v.z, off);
         if ((lane & (2 * off - 1)) == 0) v = make_float3(v.x + ox, v.y + oy, v.z + oz);
     }
-    if (R < b.nleaf) v = irregular_range(b, waves, xx, yy, t, t64, use64, dh, g, nreal, R, b.nleaf, v, R);
+    if (R < b.nleaf) v = irregular_range(b, waves, xx, yy, t, dh, g, nreal, R, b.nleaf, v, R);
     return v;
 }
 
-__device__ void uts_lookup(const float* tab, int n, float t, float out[3]) {
-    // timeSeriesHelper (engine.cpp:1882-1904) for a table sorted by time: the first row at or
-    // after t (from row 1 on), linear interpolation from the row before; zero past the end.
-    out[0] = out[1] = out[2] = 0.f;
+// The irregular wave-maker value in FP64 (compensated form): the nleaf leaves sum to
+// sum_i (e_i + sea level) + (nleaf - n) sea level = sum_i e_i + nleaf sea level.  Lanes take the
+// components lane, lane + 32, ...; a shuffle tree joins them; every lane gets the sums.
+__device__ void irregular_warp_d(const BoundaryDesc& b, const double* waves, double xx, double yy, double t,
+                                 double dh, double g, int lane, double out[3]) {
+    const int nreal = (dh > CEL_MIN_DEPTH_D) ? min(b.n_waves, b.nleaf) : 0;
+    double e = 0.0, u = 0.0, v = 0.0;
+    for (int m = lane; m < nreal; m += 32) {
+        const double* wv = waves + 4 * size_t(b.wave_offset + m);
+        double ei, ui, vi;
+        sine_wave_d(xx, yy, t, dh, wv[0], wv[1], wv[2], wv[3], g, ei, ui, vi);
+        e += ei; u += ui; v += vi;
+    }
+    for (int off = 16; off; off >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, off);
+        u += __shfl_xor_sync(0xffffffffu, u, off);
+        v += __shfl_xor_sync(0xffffffffu, v, off);
+    }
+    out[0] = e + double(b.nleaf) * b.sea_level64;
+    out[1] = u;
+    out[2] = v;
+}
+
+// timeSeriesHelper (engine.cpp:1882-1904) for a table sorted by time: the first row at or after t
+// (from row 1 on), linear interpolation from the row before; zero past the end.
+template <typename T>
+__device__ void uts_lookup(const T* tab, int n, T t, T out[3]) {
+    out[0] = out[1] = out[2] = T(0);
     int lo = 1, hi = n;  // first index in [1, n) with tab.t >= t, or n
     while (lo < hi) {
         const int mid = (lo + hi) / 2;
         if (tab[4 * mid] < t) lo = mid + 1; else hi = mid;
     }
     if (lo >= n) return;
-    const float t0 = tab[4 * (lo - 1)], t1 = tab[4 * lo];
-    const float m = (t - t0) / (t1 - t0);
+    const T t0 = tab[4 * (lo - 1)], t1 = tab[4 * lo];
+    const T m = (t - t0) / (t1 - t0);
     for (int q = 0; q < 3; ++q) {
-        const float v0 = tab[4 * (lo - 1) + q + 1], v1 = tab[4 * lo + q + 1];
+        const T v0 = tab[4 * (lo - 1) + q + 1], v1 = tab[4 * lo + q + 1];
         out[q] = v0 + (v1 - v0) * m;
     }
+}
+
+// Sponge length and distance of strip texel (x, y) on `side` (compute.hlsl:1011-1060)
+template <typename T>
+__device__ __forceinline__ void sponge_geometry(int side, int x, int y, int NX, int NY, int width, T dx, T dy, T& L,
+                                                T& dist) {
+    if (side == 3) { L = T(width) * dx; dist = T(x) * dx; }
+    else if (side == 1) { L = T(width) * dx; dist = T(NX - x) * dx; }
+    else if (side == 2) { L = T(width) * dy; dist = T(y) * dy; }
+    else { L = T(width) * dy; dist = T(NY - y) * dy; }
+}
+
+// The sponge's damping factor at one texel in FP64 (compensated form)
+__device__ __forceinline__ double sponge_gamma_d(const MemberDev& M, const BoundaryDesc& b, int side, int x, int y,
+                                                 float ba) {
+    double L, dist;
+    sponge_geometry(side, x, y, M.c.NX, M.c.NY, b.width, M.dx64, M.dy64, L, dist);
+    const double dh = fmax(CEL_MIN_DEPTH_D, b.sea_level64 - double(ba));
+    return sponge_fn_d(L, dist) / sponge_fn_d(L, dist + sqrt(M.g64 * dh) * double(*M.dtp));
+}
+
+// The sponged texel (hi, lo) pairs in place: eta scaled about the sea level, hu and hv scaled
+__device__ __forceinline__ void sponge_apply_d(double gam, double sl, float& w, float& lw, float& u, float& lu, float& v,
+                                               float& lv) {
+    split_hl(gam * ((double(w) + double(lw)) - sl) + sl, w, lw);
+    split_hl(gam * (double(u) + double(lu)), u, lu);
+    split_hl(gam * (double(v) + double(lv)), v, lv);
 }
 
 constexpr int BND_CPT = 4;
 constexpr int BND_CELLS = 256 * BND_CPT;
 constexpr int BND_IRR_CELLS = 256 / 32;   // irregular wave-maker strips: one cell per warp
 
+__host__ __device__ __forceinline__ int boundary_item_cells(int type) {
+    return type == CEL_BC_SPONGE ? BND_CELLS : type == CEL_BC_IRREGULAR ? BND_IRR_CELLS : 256;
+}
+
 template <bool MIXED>
-__global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ mems, const int2* __restrict__ items,
+__global__ void __launch_bounds__(256, 2) k_boundary(const MemberDev* __restrict__ mems, const int2* __restrict__ items,
                                                   int nitems, int side, int phase, int out) {
+    constexpr int SS = MIXED ? 6 : 3;   // strip floats per cell: w, hu, hv (+ their low words)
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const int2 wi = items[it];
         const MemberDev& M = mems[wi.x];
@@ -1854,82 +1934,102 @@ __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ 
         float* W = M.S[out][0];
         float* HU = M.S[out][1];
         float* HV = M.S[out][2];
+        float* LW = MIXED ? M.L[out][0] : nullptr;
+        float* LU = MIXED ? M.L[out][1] : nullptr;
+        float* LV = MIXED ? M.L[out][2] : nullptr;
+        const int cend = min(sw * sh, wi.y + boundary_item_cells(b.type));   // this item's cells end here
         if (b.type == CEL_BC_SPONGE && phase == 0) {
             // Pointwise: the loads of all the thread's cells are issued before the first store.
             const float sl = b.sea_level;
-            const float L = (side == 1 || side == 3) ? float(b.width) * c.dx : float(b.width) * c.dy;
             const float dt = *M.dtp;
             size_t gi[BND_CPT];
-            float dist[BND_CPT], vw[BND_CPT], vu[BND_CPT], vv[BND_CPT], ba[BND_CPT];
+            int cx[BND_CPT], cy[BND_CPT];
+            float vw[BND_CPT], vu[BND_CPT], vv[BND_CPT], ba[BND_CPT];
             float l0[BND_CPT], l1[BND_CPT], l2[BND_CPT];
             bool ok[BND_CPT];
 #pragma unroll
             for (int k = 0; k < BND_CPT; ++k) {
                 const int cell = wi.y + k * 256 + threadIdx.x;
-                ok[k] = cell < sw * sh;
-                const int x = x0 + cell % sw, y = y0 + cell / sw;
-                gi[k] = size_t(y) * P + x;
-                if (side == 3) dist[k] = float(x) * c.dx;
-                else if (side == 1) dist[k] = float(NX - x) * c.dx;
-                else if (side == 2) dist[k] = float(y) * c.dy;
-                else dist[k] = float(NY - y) * c.dy;
+                ok[k] = cell < cend;
+                cx[k] = x0 + cell % sw; cy[k] = y0 + cell / sw;
+                gi[k] = size_t(cy[k]) * P + cx[k];
                 vw[k] = vu[k] = vv[k] = ba[k] = l0[k] = l1[k] = l2[k] = 0.f;
                 if (ok[k]) {
                     vw[k] = W[gi[k]]; vu[k] = HU[gi[k]]; vv[k] = HV[gi[k]]; ba[k] = M.BA[gi[k]];
-                    if (MIXED) { l0[k] = M.L[out][0][gi[k]]; l1[k] = M.L[out][1][gi[k]]; l2[k] = M.L[out][2][gi[k]]; }
+                    if (MIXED) { l0[k] = LW[gi[k]]; l1[k] = LU[gi[k]]; l2[k] = LV[gi[k]]; }
                 }
             }
 #pragma unroll
             for (int k = 0; k < BND_CPT; ++k) {
                 if (!ok[k]) continue;
-                const float dh = fmaxf(CEL_MIN_DEPTH, sl - ba[k]);
-                const float gam = sponge_fn(L, dist[k]) / sponge_fn(L, dist[k] + sqrtf(c.g * dh) * dt);
-                W[gi[k]] = gam * (vw[k] - sl) + sl;
-                HU[gi[k]] = gam * vu[k];
-                HV[gi[k]] = gam * vv[k];
-                if (MIXED) { M.L[out][0][gi[k]] = gam * l0[k]; M.L[out][1][gi[k]] = gam * l1[k]; M.L[out][2][gi[k]] = gam * l2[k]; }
+                if (MIXED) {
+                    const double gam = sponge_gamma_d(M, b, side, cx[k], cy[k], ba[k]);
+                    sponge_apply_d(gam, b.sea_level64, vw[k], l0[k], vu[k], l1[k], vv[k], l2[k]);
+                    W[gi[k]] = vw[k]; HU[gi[k]] = vu[k]; HV[gi[k]] = vv[k];
+                    LW[gi[k]] = l0[k]; LU[gi[k]] = l1[k]; LV[gi[k]] = l2[k];
+                } else {
+                    float L, dist;
+                    sponge_geometry(side, cx[k], cy[k], NX, NY, b.width, c.dx, c.dy, L, dist);
+                    const float dh = fmaxf(CEL_MIN_DEPTH, sl - ba[k]);
+                    const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * dt);
+                    W[gi[k]] = gam * (vw[k] - sl) + sl;
+                    HU[gi[k]] = gam * vu[k];
+                    HV[gi[k]] = gam * vv[k];
+                }
             }
             continue;
         }
-        if (b.type == CEL_BC_IRREGULAR && phase == 0) {
+        if (b.type == CEL_BC_IRREGULAR && phase != 2) {
             // one cell per warp, its components spread over the lanes (BND_IRR_CELLS per item)
             const int lane = threadIdx.x & 31;
             const int cell = wi.y + (threadIdx.x >> 5);
-            if (cell >= sw * sh) continue;   // warp-uniform
+            if (cell >= cend) continue;   // warp-uniform
             const int x = x0 + cell % sw, y = y0 + cell / sw;
             const size_t gi = size_t(y) * P + x;
             const bool colwise = (side == 1 || side == 3);
             const int along = colwise ? y : x;
             const int lim = colwise ? c.ny : c.nx;
-            float3 r = make_float3(0.f, 0.f, 0.f);
+            float o[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};   // w, hu, hv, then their low words
             if (along >= 2 && along < lim + 2) {
-                const float dh = fmaxf(0.f, b.sea_level - M.BA[gi]);
-                const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
-                const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
-                r = irregular_warp(b, M.waves, xx, yy, *M.time32, *M.time64, MIXED, dh, c.g, lane);
+                if (MIXED) {
+                    const double dh = fmax(0.0, b.sea_level64 - double(M.BA[gi]));
+                    const double xx = (side == 1) ? double(x - NX) * M.dx64 : double(x) * M.dx64;
+                    const double yy = (side == 0) ? double(y - NY) * M.dy64 : double(y) * M.dy64;
+                    double r[3];
+                    irregular_warp_d(b, M.waves64, xx, yy, *M.time64, dh, M.g64, lane, r);
+                    for (int q = 0; q < 3; ++q) split_hl(r[q], o[q], o[3 + q]);
+                } else {
+                    const float dh = fmaxf(0.f, b.sea_level - M.BA[gi]);
+                    const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
+                    const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
+                    const float3 r = irregular_warp(b, M.waves, xx, yy, *M.time32, dh, c.g, lane);
+                    o[0] = r.x; o[1] = r.y; o[2] = r.z;
+                }
             }
             if (lane == 0) {
-                W[gi] = r.x; HU[gi] = r.y; HV[gi] = r.z;
-                if (MIXED) { M.L[out][0][gi] = 0.f; M.L[out][1][gi] = 0.f; M.L[out][2][gi] = 0.f; }
+                if (phase == 1) {
+                    for (int q = 0; q < SS; ++q) M.strip[SS * cell + q] = o[q];
+                } else {
+                    W[gi] = o[0]; HU[gi] = o[1]; HV[gi] = o[2];
+                    if (MIXED) { LW[gi] = o[3]; LU[gi] = o[4]; LV[gi] = o[5]; }
+                }
             }
             continue;
         }
         const int cpt = (b.type == CEL_BC_SPONGE) ? BND_CPT : 1;
         for (int k = 0; k < cpt; ++k) {
             const int cell = wi.y + k * 256 + threadIdx.x;
-            if (cell >= sw * sh) break;   // cells ascend with k
+            if (cell >= cend) break;   // cells ascend with k
             const int x = x0 + cell % sw, y = y0 + cell / sw;
             const size_t gi = size_t(y) * P + x;
             if (phase == 2) {
-                W[gi] = M.strip[3 * cell]; HU[gi] = M.strip[3 * cell + 1]; HV[gi] = M.strip[3 * cell + 2];
-                if (MIXED) { M.L[out][0][gi] = 0.f; M.L[out][1][gi] = 0.f; M.L[out][2][gi] = 0.f; }
+                W[gi] = M.strip[SS * cell]; HU[gi] = M.strip[SS * cell + 1]; HV[gi] = M.strip[SS * cell + 2];
+                if (MIXED) { LW[gi] = M.strip[SS * cell + 3]; LU[gi] = M.strip[SS * cell + 4]; LV[gi] = M.strip[SS * cell + 5]; }
                 continue;
             }
             float ow = 0.f, ou = 0.f, ov = 0.f;
             float lw = 0.f, lu = 0.f, lv = 0.f;
             const float sl = b.sea_level;
-            const double t64 = *M.time64;
-            const float t32 = *M.time32;
             if (b.type == CEL_BC_SOLID) {
                 int qx, qy;
                 solid_source(side, x, y, c.nx, c.ny, qx, qy);
@@ -1937,56 +2037,64 @@ __global__ void __launch_bounds__(256) k_boundary(const MemberDev* __restrict__ 
                 if (qx >= 0 && qy >= 0 && qx < NX && qy < NY) {
                     const size_t qi = size_t(qy) * P + qx;
                     sw_ = W[qi]; su = HU[qi]; sv = HV[qi];
-                    if (MIXED) { lw_ = M.L[out][0][qi]; lu_ = M.L[out][1][qi]; lv_ = M.L[out][2][qi]; }
+                    if (MIXED) { lw_ = LW[qi]; lu_ = LU[qi]; lv_ = LV[qi]; }
                 }
                 ow = sw_; lw = lw_;
                 ou = (side == 1 || side == 3) ? -su : su; lu = (side == 1 || side == 3) ? -lu_ : lu_;
                 ov = (side == 0 || side == 2) ? -sv : sv; lv = (side == 0 || side == 2) ? -lv_ : lv_;
             } else if (b.type == CEL_BC_SPONGE) {
-                const float dh = fmaxf(CEL_MIN_DEPTH, sl - M.BA[gi]);
-                float L, dist;
-                if (side == 3) { L = float(b.width) * c.dx; dist = float(x) * c.dx; }
-                else if (side == 1) { L = float(b.width) * c.dx; dist = float(NX - x) * c.dx; }
-                else if (side == 2) { L = float(b.width) * c.dy; dist = float(y) * c.dy; }
-                else { L = float(b.width) * c.dy; dist = float(NY - y) * c.dy; }
-                const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * (*M.dtp));
-                ow = gam * (W[gi] - sl) + sl;
-                ou = gam * HU[gi];
-                ov = gam * HV[gi];
-                if (MIXED) { lw = gam * M.L[out][0][gi]; lu = gam * M.L[out][1][gi]; lv = gam * M.L[out][2][gi]; }
-            } else if (b.type == CEL_BC_SINEWAVE) {
-                const float dh = fmaxf(0.f, sl - M.BA[gi]);
-                const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
-                const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
-                float e = 0.f, hu = 0.f, hv = 0.f;
-                if (dh > CEL_MIN_DEPTH) {
-                    if (MIXED) sine_wave_t64(xx, yy, t64, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
-                    else sine_wave(xx, yy, t32, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
+                ow = W[gi]; ou = HU[gi]; ov = HV[gi];
+                if (MIXED) {
+                    lw = LW[gi]; lu = LU[gi]; lv = LV[gi];
+                    sponge_apply_d(sponge_gamma_d(M, b, side, x, y, M.BA[gi]), b.sea_level64, ow, lw, ou, lu, ov, lv);
+                } else {
+                    float L, dist;
+                    sponge_geometry(side, x, y, NX, NY, b.width, c.dx, c.dy, L, dist);
+                    const float dh = fmaxf(CEL_MIN_DEPTH, sl - M.BA[gi]);
+                    const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * (*M.dtp));
+                    ow = gam * (ow - sl) + sl;
+                    ou = gam * ou;
+                    ov = gam * ov;
                 }
-                ow = e + sl; ou = hu; ov = hv;
-            } else if (b.type == CEL_BC_UTS) {
-                float v[3];
-                uts_lookup(M.uts[side], M.nuts[side], MIXED ? float(t64) : t32, v);
-                ow = v[0] + sl; ou = v[1]; ov = v[2];
-            } else {
-                const bool colwise = (side == 1 || side == 3);
-                const int along = colwise ? y : x;
-                const int lim = colwise ? c.ny : c.nx;
-                if (along >= 2 && along < lim + 2) {
+            } else if (b.type == CEL_BC_SINEWAVE) {
+                if (MIXED) {
+                    const double dh = fmax(0.0, b.sea_level64 - double(M.BA[gi]));
+                    const double xx = (side == 1) ? double(x - NX) * M.dx64 : double(x) * M.dx64;
+                    const double yy = (side == 0) ? double(y - NY) * M.dy64 : double(y) * M.dy64;
+                    double e = 0.0, hu = 0.0, hv = 0.0;
+                    if (dh > CEL_MIN_DEPTH_D)
+                        sine_wave_d(xx, yy, *M.time64, dh, b.amplitude64, b.period64, b.theta64, 0.0, M.g64, e, hu, hv);
+                    split_hl(e + b.sea_level64, ow, lw);
+                    split_hl(hu, ou, lu);
+                    split_hl(hv, ov, lv);
+                } else {
                     const float dh = fmaxf(0.f, sl - M.BA[gi]);
                     const float xx = (side == 1) ? float(x - NX) * c.dx : float(x) * c.dx;
                     const float yy = (side == 0) ? float(y - NY) * c.dy : float(y) * c.dy;
-                    const float3 r = irregular_tree(b, M.waves, xx, yy, t32, t64, MIXED, dh, c.g);
-                    ow = r.x; ou = r.y; ov = r.z;
+                    float e = 0.f, hu = 0.f, hv = 0.f;
+                    if (dh > CEL_MIN_DEPTH) sine_wave(xx, yy, *M.time32, dh, b.amplitude, b.period, b.theta, 0.f, c.g, e, hu, hv);
+                    ow = e + sl; ou = hu; ov = hv;
+                }
+            } else if (b.type == CEL_BC_UTS) {
+                if (MIXED) {
+                    double v[3];
+                    uts_lookup<double>(M.uts64[side], M.nuts[side], *M.time64, v);
+                    split_hl(v[0] + b.sea_level64, ow, lw);
+                    split_hl(v[1], ou, lu);
+                    split_hl(v[2], ov, lv);
+                } else {
+                    float v[3];
+                    uts_lookup<float>(M.uts[side], M.nuts[side], *M.time32, v);
+                    ow = v[0] + sl; ou = v[1]; ov = v[2];
                 }
             }
             if (phase == 1) {
-                M.strip[3 * cell] = ow; M.strip[3 * cell + 1] = ou; M.strip[3 * cell + 2] = ov;
+                M.strip[SS * cell] = ow; M.strip[SS * cell + 1] = ou; M.strip[SS * cell + 2] = ov;
+                if (MIXED) { M.strip[SS * cell + 3] = lw; M.strip[SS * cell + 4] = lu; M.strip[SS * cell + 5] = lv; }
             } else {
                 W[gi] = ow; HU[gi] = ou; HV[gi] = ov;
-                if (MIXED) { M.L[out][0][gi] = lw; M.L[out][1][gi] = lu; M.L[out][2][gi] = lv; }
+                if (MIXED) { LW[gi] = lw; LU[gi] = lu; LV[gi] = lv; }
             }
-
         }
     }
 }
@@ -2222,6 +2330,7 @@ struct cel_lane {
     int graph_pos = 0;
     long long cells = 0;
     int cw = 16;                        // column solver band width (columns per CTA)
+    int cnt = 512;                      // column solver threads per CTA (chunks per column = cnt / cw)
     int mh = cel::MH_DEFAULT;           // stencil strip height (rows per CTA work item)
     int rows_per_step = 1;              // stencil rows per thread step: 1 (k_march) or 2 (k_march2)
     int mw = 128;                       // stencil CTA width in threads (k_march2: 128 or 96)
@@ -2308,10 +2417,14 @@ int upload_state(cel_lane* b, int i, const float* rgba, std::string& err, const 
 }
 
 using ColsKernel = void (*)(const MemberDev*, const int2*, int, PassArgs);
-ColsKernel cols_kernel(bool mixed, int cw) {
-    if (cw == 32) return mixed ? k_cols<true, 32> : k_cols<false, 32>;
-    if (cw == 16) return mixed ? k_cols<true, 16> : k_cols<false, 16>;
-    return mixed ? k_cols<true, 8> : k_cols<false, 8>;
+template <int NT>
+ColsKernel cols_kernel_nt(bool mixed, int cw) {
+    if (cw == 32) return mixed ? k_cols<true, 32, NT> : k_cols<false, 32, NT>;
+    if (cw == 16) return mixed ? k_cols<true, 16, NT> : k_cols<false, 16, NT>;
+    return mixed ? k_cols<true, 8, NT> : k_cols<false, 8, NT>;
+}
+ColsKernel cols_kernel(bool mixed, int cw, int nt) {
+    return nt == 256 ? cols_kernel_nt<256>(mixed, cw) : cols_kernel_nt<512>(mixed, cw);
 }
 
 using March2Kernel = void (*)(const MemberDev*, const int4*, int, PassArgs);
@@ -2351,8 +2464,8 @@ int launch_pass(cel_lane* b, const PassArgs& pa, std::string& err) {
             if (b->mixed) k_cols_serial<true><<<b->grid_cols, 128, 0, b->side>>>(b->ddev, b->bands, b->nbands, pa);
             else k_cols_serial<false><<<b->grid_cols, 128, 0, b->side>>>(b->ddev, b->bands, b->nbands, pa);
         } else {
-            auto* kc = cols_kernel(b->mixed, b->cw);
-            kc<<<b->grid_cols, NTC, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+            auto* kc = cols_kernel(b->mixed, b->cw, b->cnt);
+            kc<<<b->grid_cols, b->cnt, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
         }
     }
     {
@@ -2557,7 +2670,8 @@ cudaError_t allow_max_dynamic_smem(const void* kernel) {
     return e;
 }
 
-int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, std::string& err) {
+int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::string& err) {
+    if (nt != 256 && nt != 512) { err = "column solver threads must be 256 or 512"; return CEL_ERR_ARG; }
     if (rps != 1 && rps != 2) { err = "stencil rows per step must be 1 or 2"; return CEL_ERR_ARG; }
     if (mw != 128 && mw != 96) { err = "stencil width must be 128 or 96 threads"; return CEL_ERR_ARG; }
     if (rps == 1) mw = MW;   // the one-row stencil has one width
@@ -2604,6 +2718,7 @@ int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, std::string& er
     b->nmtiles = int(mt.size());
     b->nbands = int(bd.size());
     b->cw = cw;
+    b->cnt = nt;
     b->mh = mh;
     b->mw = mw;
     b->smem_cols = smem_cols;
@@ -2611,9 +2726,9 @@ int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, std::string& er
     if (cw == 1) {
         b->grid_cols = (b->nbands + 127) / 128;
     } else {
-        ColsKernel kc = cols_kernel(b->mixed, cw);
+        ColsKernel kc = cols_kernel(b->mixed, cw, nt);
         B_TRY(allow_max_dynamic_smem(reinterpret_cast<const void*>(kc)));
-        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc, NTC, smem_cols));
+        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc, nt, smem_cols));
         b->grid_cols = std::max(1, std::min(b->nbands, b->sms * std::max(occ, 1) * 4));
     }
     // both variants of the stencil (fixed and adaptive predictor) run on the same grid
@@ -2672,6 +2787,7 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
     b->mem.resize(n);
     b->hdev.resize(n);
     std::vector<float4> waves;
+    std::vector<double> waves64;
     {
         void* p = nullptr;
         const size_t nd = 1 + size_t(n) + 2 * size_t(n) * STATS_N;
@@ -2725,6 +2841,9 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
         std::memset(&d, 0, sizeof(d));
         d.c = make_consts(m.p, m.hs, m.P);
         d.P = m.P;
+        d.dx64 = m.p.width / double(m.hs.nx - 1);
+        d.dy64 = m.p.length / double(m.hs.ny - 1);
+        d.g64 = m.p.gravity;
         b->dt_host[i] = float(m.p.timestep);
         d.dtp = b->dt_table + i;
         d.ab = b->ctl ? b->ctl[i].ab : nullptr;
@@ -2799,13 +2918,17 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
             bd.type = bb.type; bd.width = bb.width;
             bd.sea_level = float(bb.sea_level); bd.amplitude = float(bb.amplitude);
             bd.period = float(bb.period); bd.theta = float(bb.theta);
+            bd.sea_level64 = bb.sea_level; bd.amplitude64 = bb.amplitude;
+            bd.period64 = bb.period; bd.theta64 = bb.theta;
             bd.n_waves = bb.type == CEL_BC_IRREGULAR ? bb.n_waves : 0;
             const int Kn = (s == 0 || s == 2) ? m.hs.Ky : m.hs.Kx;
             bd.nleaf = 1 << (Kn - 1);
             bd.wave_offset = int(waves.size());
-            for (int k = 0; k < bd.n_waves; ++k)
+            for (int k = 0; k < bd.n_waves; ++k) {
                 waves.push_back(make_float4(float(bb.waves[k][0]), float(bb.waves[k][1]), float(bb.waves[k][2]),
                                             float(bb.waves[k][3])));
+                for (int q = 0; q < 4; ++q) waves64.push_back(bb.waves[k][q]);
+            }
             if (bb.type == CEL_BC_UTS) {
                 m.uts_host[s].resize(size_t(bb.n_uts) * 4);
                 for (int k = 0; k < 4 * bb.n_uts; ++k) m.uts_host[s][k] = float(bb.uts[k]);
@@ -2813,12 +2936,13 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
                 if (dalloc(b.get(), &up, m.uts_host[s].size() * sizeof(float), err)) return nullptr;
                 cudaMemcpy(up, m.uts_host[s].data(), m.uts_host[s].size() * sizeof(float), cudaMemcpyHostToDevice);
                 d.uts[s] = static_cast<float*>(up);
+                if (dalloc(b.get(), &up, size_t(bb.n_uts) * 4 * sizeof(double), err)) return nullptr;
+                cudaMemcpy(up, bb.uts, size_t(bb.n_uts) * 4 * sizeof(double), cudaMemcpyHostToDevice);
+                d.uts64[s] = static_cast<double*>(up);
                 d.nuts[s] = bb.n_uts;
             }
             const int cellsn = (s == 0 || s == 2) ? NX * std::min(bb.width, NY) : std::min(bb.width, NX) * NY;
-            for (int c0 = 0; c0 < cellsn;
-                 c0 += (bb.type == CEL_BC_SPONGE ? BND_CELLS : bb.type == CEL_BC_IRREGULAR ? BND_IRR_CELLS : 256))
-                bitems[s].push_back(make_int2(i, c0));
+            for (int c0 = 0; c0 < cellsn; c0 += boundary_item_cells(bb.type)) bitems[s].push_back(make_int2(i, c0));
             // a solid strip wider than 2 reads ghost cells of its own strip: compute, then write
             if (bb.type == CEL_BC_SOLID && bb.width >= 3) b->two_phase[s] = true;
         }
@@ -2829,7 +2953,8 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
                 strip = std::max(strip, size_t((s == 0 || s == 2) ? NX * std::min(w, NY) : std::min(w, NX) * NY));
             }
             void* sp = nullptr;
-            if (dalloc(b.get(), &sp, std::max<size_t>(strip, 1) * 3 * sizeof(float), err)) return nullptr;
+            const size_t per_cell = b->mixed ? 6 : 3;   // w, hu, hv (+ their low words)
+            if (dalloc(b.get(), &sp, std::max<size_t>(strip, 1) * per_cell * sizeof(float), err)) return nullptr;
             d.strip = static_cast<float*>(sp);
         }
         // work lists
@@ -2845,6 +2970,10 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
         if (dalloc(b.get(), &wp, waves.size() * sizeof(float4), err)) return nullptr;
         cudaMemcpy(wp, waves.data(), waves.size() * sizeof(float4), cudaMemcpyHostToDevice);
         for (auto& d : b->hdev) d.waves = static_cast<float4*>(wp);
+        if (waves64.empty()) waves64.assign(4, 0.0);
+        if (dalloc(b.get(), &wp, waves64.size() * sizeof(double), err)) return nullptr;
+        cudaMemcpy(wp, waves64.data(), waves64.size() * sizeof(double), cudaMemcpyHostToDevice);
+        for (auto& d : b->hdev) d.waves64 = static_cast<double*>(wp);
     }
     // Sort tiles and lines so that large domains are scheduled first (load balance).
     auto upload_list = [&](auto& v, auto** dst, int& cnt) -> int {
@@ -2883,7 +3012,7 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
     }
     {   // column bands of 16 columns (8 for tall domains: shared-memory capacity), strips of 64 rows
         const int cw = (size_t(max_ny) * 16 * sizeof(float) + 8192 <= 227 * 1024) ? 16 : 8;
-        if (configure_work(b.get(), cw, MH_DEFAULT, 1, MW, err)) return nullptr;
+        if (configure_work(b.get(), cw, MH_DEFAULT, 1, MW, NTC_DEFAULT, err)) return nullptr;
     }
     b->sch.reset(*params[0]);
     cudaMemcpy(b->dt_table, b->dt_host, sizeof(float) * n, cudaMemcpyHostToDevice);
@@ -3184,8 +3313,11 @@ int lane_set_timestep(cel_lane* b, const float* dt, std::string& err) {
 }
 
 int lane_set_tuning(cel_lane* b, int tx, int ty, int pcr, std::string& err) {
-    (void)pcr;   // the solves have no cyclic-reduction stage to hand over from (Thomas factors + scans)
-    return configure_work(b, tx > 0 ? tx : b->cw, ty > 0 ? ty : b->mh, b->rows_per_step, b->mw, err);
+    // pcr: chunks per column of the column solver (the carry scan joins that many chunks; each is
+    // swept serially), so the CTA has pcr x band width threads; 0 keeps the threads per CTA
+    const int cw = tx > 0 ? tx : b->cw;
+    const int nt = (pcr > 0 && cw > 1) ? pcr * cw : b->cnt;
+    return configure_work(b, cw, ty > 0 ? ty : b->mh, b->rows_per_step, b->mw, nt, err);
 }
 
 int lane_get_tuning(const cel_lane* b, int* tx, int* ty, int* rps) {
@@ -3195,8 +3327,10 @@ int lane_get_tuning(const cel_lane* b, int* tx, int* ty, int* rps) {
     return CEL_OK;
 }
 
+int lane_col_chunks(const cel_lane* b) { return b->cw > 1 ? b->cnt / b->cw : 1; }
+
 int lane_set_stencil_rows(cel_lane* b, int rps, std::string& err) {
-    return configure_work(b, b->cw, b->mh, rps, rps == 2 ? b->mw : MW, err);
+    return configure_work(b, b->cw, b->mh, rps, rps == 2 ? b->mw : MW, b->cnt, err);
 }
 
 int lane_set_stencil_width(cel_lane* b, int threads, std::string& err) {
@@ -3204,7 +3338,7 @@ int lane_set_stencil_width(cel_lane* b, int threads, std::string& err) {
         err = "the one-row stencil runs 128-thread strips; select two rows per step first";
         return CEL_ERR_ARG;
     }
-    return configure_work(b, b->cw, b->mh, b->rows_per_step, threads, err);
+    return configure_work(b, b->cw, b->mh, b->rows_per_step, threads, b->cnt, err);
 }
 
 int lane_stencil_width(const cel_lane* b) { return b->mw; }
@@ -3212,9 +3346,10 @@ int lane_stencil_width(const cel_lane* b) { return b->mw; }
 cudaStream_t lane_stream(const cel_lane* b) { return b->stream; }
 int lane_members(const cel_lane* b) { return int(b->mem.size()); }
 int lane_max_ny(const cel_lane* b) { return b->max_ny; }
-int lane_configure(cel_lane* b, int cw, int mh, int rps, int mw, std::string& err) {
-    return configure_work(b, cw, mh, rps, mw, err);
+int lane_configure(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::string& err) {
+    return configure_work(b, cw, mh, rps, mw, nt, err);
 }
+int lane_col_threads(const cel_lane* b) { return b->cnt; }
 
 KernelTimer* lane_timer(cel_lane* b) { return &b->tm; }
 

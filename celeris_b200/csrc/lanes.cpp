@@ -273,25 +273,21 @@ int batch_set_stencil_width(cel_batch* b, int threads, std::string& err) {
 
 int batch_stencil_width(const cel_batch* b) { return lane_stencil_width(b->lanes[0]); }
 
-// Times `steps` physical steps of the whole batch (all lanes side by side) for every candidate
-// (column band width, strip height, stencil rows per step, stencil width), in the launch mode the
-// batch is set to, two rounds in turn, and keeps the fastest by its better round.  Every lane
-// takes the same candidate and the same steps, so the members stay in step with one another.
+// Times `steps` physical steps of the whole batch (all lanes side by side) for each candidate, in
+// the launch mode the batch is set to, two rounds in turn, and keeps the fastest by its better
+// round.  The stencil and the solvers are separate kernels, so the search runs in two stages: the
+// stencil (rows per step and width x strip height) with the default solvers, then the column solver
+// (band width x chunks per column, i.e. the switch point from the carry scan to serial sweeps) with
+// the chosen stencil.  Every lane takes the same candidate and the same steps, so the members stay
+// in step with one another.
 int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, std::string& err) {
     if (steps < 1) { err = "autotune needs at least one step per candidate"; return CEL_ERR_ARG; }
     int max_ny = 0;
     for (const cel_lane* l : b->lanes) max_ny = std::max(max_ny, lane_max_ny(l));
-    struct Cand { int cw, mh, rps, mw; };
-    std::vector<Cand> cand;
-    const int variants[3][2] = {{1, 128}, {2, 128}, {2, 96}};   // stencil rows per step, stencil width
-    for (const auto& v : variants)
-        for (int cw : {1, 8, 16, 32})
-            if (cw == 1 || sizeof(float) * size_t(max_ny) * cw + 8192 <= 227 * 1024)
-                for (int mh : {32, 64, 128}) cand.push_back({cw, mh, v[0], v[1]});
+    struct Cand { int cw, mh, rps, mw, nt; };
     auto configure = [&](const Cand& c) {
-        return each(b, err, [&](cel_lane* l) { return lane_configure(l, c.cw, c.mh, c.rps, c.mw, err); });
+        return each(b, err, [&](cel_lane* l) { return lane_configure(l, c.cw, c.mh, c.rps, c.mw, c.nt, err); });
     };
-    std::vector<double> best(cand.size(), 1e300);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     G_TRY(cudaEventCreate(&e0));
     if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -301,28 +297,54 @@ int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, s
     }
     const cudaStream_t s = batch_stream(b);
     int rc = CEL_OK;
-    for (int round = 0; round < 2 && !rc; ++round)
-        for (size_t k = 0; k < cand.size() && !rc; ++k) {
-            if ((rc = configure(cand[k]))) break;
-            if ((rc = batch_step(b, 2, err))) break;   // warm-up (captures the graphs in graph mode)
-            cudaEventRecord(e0, s);
-            if ((rc = batch_step(b, steps, err))) break;
-            cudaEventRecord(e1, s);
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            best[k] = std::min(best[k], double(ms) / steps);
-        }
+    // times every candidate (two rounds) and returns the index of the fastest, or -1 on error
+    auto search = [&](const std::vector<Cand>& cand, double& best_out) -> int {
+        std::vector<double> best(cand.size(), 1e300);
+        for (int round = 0; round < 2 && !rc; ++round)
+            for (size_t k = 0; k < cand.size() && !rc; ++k) {
+                if ((rc = configure(cand[k]))) break;
+                if ((rc = batch_step(b, 2, err))) break;   // warm-up (captures the graphs in graph mode)
+                cudaEventRecord(e0, s);
+                if ((rc = batch_step(b, steps, err))) break;
+                cudaEventRecord(e1, s);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                best[k] = std::min(best[k], double(ms) / steps);
+            }
+        if (rc) return -1;
+        const size_t kb = size_t(std::min_element(best.begin(), best.end()) - best.begin());
+        best_out = best[kb];
+        return int(kb);
+    };
+    const bool cw16_fits = sizeof(float) * size_t(max_ny) * 16 + 8192 <= 227 * 1024;
+    const int cw0 = cw16_fits ? 16 : 8;
+    std::vector<Cand> stencil;
+    const int variants[3][2] = {{1, 128}, {2, 128}, {2, 96}};   // stencil rows per step, stencil width
+    for (const auto& v : variants)
+        for (int mh : {32, 64, 128}) stencil.push_back({cw0, mh, v[0], v[1], 512});
+    double ms = 0.0;
+    const int ks = search(stencil, ms);
+    std::vector<Cand> solver;
+    if (ks >= 0) {
+        const Cand st = stencil[size_t(ks)];
+        solver.push_back({1, st.mh, st.rps, st.mw, 512});
+        for (int cw : {8, 16, 32})
+            if (sizeof(float) * size_t(max_ny) * cw + 8192 <= 227 * 1024)
+                for (int nt : {256, 512}) solver.push_back({cw, st.mh, st.rps, st.mw, nt});
+    }
+    const int kb = ks >= 0 ? search(solver, ms) : -1;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    const size_t kb = size_t(std::min_element(best.begin(), best.end()) - best.begin());
-    if ((rc = configure(cand[kb]))) return rc;
-    if (tx) *tx = cand[kb].cw;
-    if (ty) *ty = cand[kb].mh;
-    if (best_ms) *best_ms = best[kb];
+    if ((rc = configure(solver[size_t(kb)]))) return rc;
+    if (tx) *tx = solver[size_t(kb)].cw;
+    if (ty) *ty = solver[size_t(kb)].mh;
+    if (best_ms) *best_ms = ms;
     return CEL_OK;
 }
+
+int batch_col_chunks(const cel_batch* b) { return lane_col_chunks(b->lanes[0]); }
 
 void batch_kernel_timing(cel_batch* b, bool enable) {
     b->timing = enable;

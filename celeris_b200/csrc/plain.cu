@@ -6,6 +6,8 @@
 #define CEL_EXACT_FP32 1
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -996,20 +998,22 @@ EngineIface* make_plain_engine(const cel_params& p, const float* bathy, int bnx,
 // Allocation-free statistics entry point.
 //
 // Some callers of this library must not allocate device memory at the moment they ask for the
-// domain statistics: code that is in the middle of a CUDA stream capture (cudaMalloc and cudaFree
-// are not capturable), frame loops where the implicit device synchronisation of cudaMalloc /
-// cudaFree would stall the frame, and host applications whose device memory is entirely handed
-// out by their own allocator.  cel_stats_noalloc computes the GetStats reduction of a state that
-// the caller already keeps in device memory, using only the fixed scratch array below: the 4x4
-// block partials and the FP64 totals.  The array is reserved on every GPU that loads the library
-// and stays there until the process exits.  All calls share it, so two calls whose work overlaps on
-// the GPU (on different streams, or from different threads) race; run them one after another.
+// domain statistics: frame loops where the device-wide synchronisation of cudaMalloc / cudaFree
+// would stall every other stream, and host applications whose device memory is entirely handed out
+// by their own allocator.  cel_stats_noalloc computes the GetStats reduction and the FP64 volume of
+// a state that the caller already keeps in device memory, using only the fixed scratch array below:
+// the 4x4 block partials, the volume partials and the FP64 totals.  The array is reserved on every
+// GPU that loads the library and stays there until the process exits.  All calls share it, so two
+// calls whose work overlaps on the GPU (on different streams, or from different threads) race; run
+// them one after another.
 // ---------------------------------------------------------------------------------------------
 namespace cel {
 namespace {
 
 constexpr int NOALLOC_MAX_BLOCKS = 65536;                  // 4x4 blocks: up to 1,048,576 cells
-constexpr int NOALLOC_FLOATS = NOALLOC_MAX_BLOCKS * 9 + 64;  // block partials + 16 doubles (32 floats)
+constexpr int NOALLOC_VOL_CTAS = 1184;                     // volume partials: 8 CTAs per SM of a B200
+// block partials (9 floats each) | volume partials (2 doubles per CTA) | 16 doubles of totals
+constexpr int NOALLOC_FLOATS = NOALLOC_MAX_BLOCKS * 9 + NOALLOC_VOL_CTAS * 4 + 32;
 static __device__ __align__(256) float g_noalloc_scratch[NOALLOC_FLOATS];
 
 // GetStats (compute.hlsl:1319-1378) reading the bottom in the public {BY, BX, BA} layout.
@@ -1041,9 +1045,39 @@ __global__ void k_getstats_b3(const float4* __restrict__ st, const float* __rest
     o[0] = sh; o[1] = sb; o[2] = shu; o[3] = shv; o[4] = sk; o[5] = mu; o[6] = mh; o[7] = mc; o[8] = mf;
 }
 
-// One CTA: FP64 totals of the block partials; every output word is written on every call.
-__global__ void k_reduce_b3(const float* __restrict__ blocks, int nb, const float4* __restrict__ st,
-                            const float* __restrict__ b3, SimConsts c, double* __restrict__ out) {
+// FP64 volume of the interior cells (and the non-finite flag), one partial per CTA: CTA k sums a
+// fixed interleaved share of the cells, so the totals do not depend on scheduling.
+__global__ void __launch_bounds__(256) k_volume_b3(const float4* __restrict__ st, const float* __restrict__ b3,
+                                                   SimConsts c, double* __restrict__ part) {
+    __shared__ double sv[8];
+    __shared__ int sb;
+    if (threadIdx.x == 0) sb = 0;
+    __syncthreads();
+    double v = 0.0;
+    int bad = 0;
+    const int n = c.nx * c.ny;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const size_t i = size_t(k / c.nx + 2) * c.NX + (k % c.nx + 2);
+        const float4 s = st[i];
+        if (!isfinite(s.x) || !isfinite(s.y) || !isfinite(s.z)) bad = 1;
+        v += fmax(0.0, double(s.x) - double(b3[3 * i + 2]));
+    }
+    for (int off = 16; off; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) sv[threadIdx.x >> 5] = v;
+    if (bad) sb = 1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += sv[w];
+        part[2 * blockIdx.x] = t;
+        part[2 * blockIdx.x + 1] = sb ? 1.0 : 0.0;
+    }
+}
+
+// One CTA: FP64 totals of the block partials and the volume partials; every output word is
+// written on every call.
+__global__ void k_reduce_b3(const float* __restrict__ blocks, int nb, const double* __restrict__ vol, int nvol,
+                            double* __restrict__ out) {
     __shared__ double sm[10][32];
     __shared__ int bad_s;
     double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -1053,12 +1087,9 @@ __global__ void k_reduce_b3(const float* __restrict__ blocks, int nb, const floa
         for (int q = 0; q < 5; ++q) v[q] += double(b[q]);
         for (int q = 5; q < 9; ++q) v[q] = fmax(v[q], double(b[q]));
     }
-    const int n = c.nx * c.ny;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const size_t i = size_t(k / c.nx + 2) * c.NX + (k % c.nx + 2);
-        const float4 s = st[i];
-        if (!isfinite(s.x) || !isfinite(s.y) || !isfinite(s.z)) bad = 1;
-        v[9] += fmax(0.0, double(s.x) - double(b3[3 * i + 2]));
+    for (int k = threadIdx.x; k < nvol; k += blockDim.x) {
+        v[9] += vol[2 * k];
+        if (vol[2 * k + 1] != 0.0) bad = 1;
     }
     if (threadIdx.x == 0) bad_s = 0;
     __syncthreads();
@@ -1089,7 +1120,8 @@ __global__ void k_reduce_b3(const float* __restrict__ blocks, int nb, const floa
 
 // Device address of the scratch array, looked up once per device (with that device current).
 constexpr int NOALLOC_MAX_DEVICES = 64;
-float* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+float* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};   // guarded by g_noalloc_mutex
+std::mutex g_noalloc_mutex;
 
 }  // namespace
 
@@ -1110,19 +1142,25 @@ extern "C" int cel_stats_noalloc(const float* d_state_rgba, const float* d_botto
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { set_error(std::string("cel_stats_noalloc: ") + cudaGetErrorString(e)); return CEL_ERR_CUDA; }
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) { set_error("cel_stats_noalloc: device index out of range"); return CEL_ERR_ARG; }
-    if (!g_noalloc_ptr[dev]) {
-        // first call on this device: resolve the array's device address (this must not happen
-        // inside a stream capture, so make the first call before capturing)
-        float* ptr = nullptr;
-        e = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr) {
-            set_error(std::string("cel_stats_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-            return CEL_ERR_CUDA;
+    float* blocks = nullptr;
+    {
+        // the array's device address on this device, resolved by the first call here (with the
+        // device current) under a lock, so that concurrent first calls do not race
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            float* ptr = nullptr;
+            e = cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr) {
+                set_error(std::string("cel_stats_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+                return CEL_ERR_CUDA;
+            }
+            g_noalloc_ptr[dev] = ptr;
         }
-        g_noalloc_ptr[dev] = ptr;
+        blocks = g_noalloc_ptr[dev];
     }
-    float* blocks = g_noalloc_ptr[dev];
-    double* totals = reinterpret_cast<double*>(blocks + size_t(NOALLOC_MAX_BLOCKS) * 9);  // 256-byte aligned
+    // volume partials after the block partials (byte offset 65,536 x 36, a multiple of 256), totals last
+    double* vol = reinterpret_cast<double*>(blocks + size_t(NOALLOC_MAX_BLOCKS) * 9);
+    double* totals = vol + 2 * NOALLOC_VOL_CTAS;
     HostSetup hs;
     hs.nx = p->nx; hs.ny = p->ny; hs.NX = p->nx + 4; hs.NY = p->ny + 4;
     hs.dx = float(p->width) / float(p->nx - 1);
@@ -1136,7 +1174,9 @@ extern "C" int cel_stats_noalloc(const float* d_state_rgba, const float* d_botto
     const float4* st = reinterpret_cast<const float4*>(d_state_rgba);
     const int nbx = p->nx / 4, nby = p->ny / 4;
     k_getstats_b3<<<grid2(nbx, nby), dim3(BX2, BY2), 0, s>>>(st, d_bottom_b3, blocks, c);
-    k_reduce_b3<<<1, 1024, 0, s>>>(blocks, int(nb), st, d_bottom_b3, c, totals);
+    const int nvol = int(std::min<long long>(NOALLOC_VOL_CTAS, (p->nx * (long long)p->ny + 255) / 256));
+    k_volume_b3<<<nvol, 256, 0, s>>>(st, d_bottom_b3, c, vol);
+    k_reduce_b3<<<1, 1024, 0, s>>>(blocks, int(nb), vol, nvol, totals);
     e = cudaGetLastError();
     if (e != cudaSuccess) { set_error(std::string("cel_stats_noalloc: ") + cudaGetErrorString(e)); return CEL_ERR_CUDA; }
     double v[11];

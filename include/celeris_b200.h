@@ -32,7 +32,7 @@ extern "C" {
 #define CEL_ERR_IO 2         /* file missing or malformed */
 #define CEL_ERR_CUDA 3       /* CUDA runtime error or no device */
 #define CEL_ERR_STATE 4      /* call not valid in the handle's current state */
-#define CEL_ERR_NUMERIC 5    /* device health flag: NaN/Inf or negative depth detected */
+#define CEL_ERR_NUMERIC 5    /* device health flag: NaN or Inf in the state (a cell below its bed is dry, not an error) */
 
 #define CEL_MAX_WAVES 1000   /* MAX_NUM_OF_IRREGULAR_WAVES (engine.hpp:214) */
 #define CEL_MAX_SOLITONS 100 /* InitSetting::MAX_NUM_SOLITARY (settings.hpp:356) */
@@ -271,12 +271,18 @@ int cel_batch_launches_per_step(const cel_batch* b);
 /* ---- tuning and measurement ------------------------------------------------------------- */
 /* Fused forms.  tile_x: column-solver band width (8, 16 or 32 columns per CTA, chunked scans; or 1:
  * one thread per column, serial sweeps, forward values kept in the right-hand-side plane); tile_y: stencil
- * strip height (rows a CTA marches, 8..1024); 0 keeps the current value.  pcr_switch is accepted
- * and ignored: the tridiagonal solves here factor each system once (Thomas) and run the sweeps as
- * scans, with no cyclic-reduction stage to hand over from.  Plain engines ignore the call. */
+ * strip height (rows a CTA marches, 8..1024); 0 keeps the current value.  pcr_switch: chunks per
+ * column of the column solver, i.e. where it switches from the parallel stage to serial sweeps.  The
+ * solves factor each system once (M = LU, engine.cpp:2612-2887 coefficients); the L and U sweeps of
+ * a column are split into that many chunks, each swept serially by one thread (Thomas), and the
+ * chunks' transfer maps are joined by recursive doubling with warp shuffles (parallel reduction of
+ * the bidiagonal sweeps).  Chunks x band width must be 256 or 512 threads; 0 keeps the current
+ * value.  Plain engines ignore the call. */
 int cel_set_tuning(cel_engine* h, int tile_x, int tile_y, int pcr_switch);
 int cel_batch_set_tuning(cel_batch* b, int tile_x, int tile_y, int pcr_switch);
 int cel_batch_get_tuning(const cel_batch* b, int* tile_x, int* tile_y, int* rows_per_step);
+/* The column solver's chunks per column (the pcr_switch above; 1 with tile_x = 1: one thread per column). */
+int cel_batch_col_chunks(const cel_batch* b);
 /* Stencil variant: 1 = one row per thread step; 2 = two rows per step as pairs, with the paired
  * single-precision instructions of sm_100 (f32x2). */
 int cel_batch_set_stencil_rows(cel_batch* b, int rows_per_step);
@@ -330,16 +336,18 @@ int cel_write_bathymetry(const cel_params* p, const float* bottom_b3, const char
 int cel_write_hotstart(const cel_params* p, const float* rgba, const char* path);
 
 /* ---- allocation-free statistics (no counterpart in the reference) ----------------------- */
-/* The resetTimestep statistics (mass, energies, momenta, maxima, CFL rate) of a state the caller
- * keeps in device memory: d_state_rgba is (nx+4)(ny+4) x {w,hu,hv,_} and d_bottom_b3 is
- * (nx+4)(ny+4) x {BY,BX,BA}, both device pointers; p supplies nx, ny, width, length, gravity and
- * epsilon; the work runs on cuda_stream (NULL = the default stream) and the call returns after the
- * result reached *out.  It never allocates: for callers that cannot call cudaMalloc at that point
- * (during a stream capture, in frame loops where an allocation's device synchronisation would
- * stall, or under an allocator that owns all device memory).  Its scratch is a fixed static device
- * array sized for at most 65,536 4x4 blocks (1,048,576 interior cells); larger domains get
- * CEL_ERR_ARG.  The first call on each device looks the array up (make it before any capture).
- * Calls share the array: calls that overlap on the GPU race. */
+/* The resetTimestep statistics (mass, energies, momenta, maxima, CFL rate, the FP64 volume) of a
+ * state the caller keeps in device memory: d_state_rgba is (nx+4)(ny+4) x {w,hu,hv,_} and
+ * d_bottom_b3 is (nx+4)(ny+4) x {BY,BX,BA}, both device pointers; p supplies nx, ny, width, length,
+ * gravity and epsilon.  The work runs on cuda_stream (NULL = the default stream); the call waits
+ * for that stream and returns once the totals are in *out.  It never allocates device or pinned
+ * memory, for callers that must not allocate when they ask: frame loops where the device-wide
+ * synchronisation of cudaMalloc / cudaFree would stall every other stream, and applications whose
+ * own allocator has reserved the device's memory.  Its scratch is a fixed static device array
+ * (about 2.4 MB on every GPU that loads the library, held until exit) sized for at most 65,536
+ * 4x4 blocks, i.e. 1,048,576 interior cells; larger domains get CEL_ERR_ARG.  The first call on
+ * each device looks up the array's address.  Every call uses the same array: calls whose work
+ * overlaps on the GPU (different streams or threads) race, so run them one after another. */
 int cel_stats_noalloc(const float* d_state_rgba, const float* d_bottom_b3, const cel_params* p, void* cuda_stream,
                       cel_stats* out);
 

@@ -6,6 +6,7 @@ separately and meet in .npz files:
   python tests/long_run.py oracle --case c3 --steps 10000 --out ref.npz   # CPU, FP64 oracle
   python tests/long_run.py gpu    --case c3 --steps 10000 --out gpu.npz   # CUDA forms
   python tests/long_run.py compare ref.npz gpu.npz                        # prints one JSON line
+  python tests/long_run.py record --out rec.json "C3=ref.npz,gpu.npz," ...  # several into one file
 
 Cases: ``c3`` (1024^2 solitary wave on the truncated cone, solid walls), ``c3wm`` (the same
 basin with the sinusoidal wave-maker), ``c1`` (512x64 flume with the sine wave-maker), and
@@ -62,7 +63,7 @@ def run_gpu_ensemble(args):
     tuned = b.autotune(4)
     # autotuning advanced the members: start over from the initial condition with the tuned setup
     b2 = cb.Batch([(m[0], m[1]) for m in members], form)
-    b2.set_tuning(tuned["band_width"], tuned["strip_height"])
+    b2.set_tuning(tuned["band_width"], tuned["strip_height"], b.col_chunks)
     b2.set_stencil_rows(b.stencil_rows)
     if b.stencil_rows == 2:
         b2.set_stencil_width(b.stencil_width)
@@ -147,8 +148,29 @@ def runup(bottom: np.ndarray, initial_dry: np.ndarray, maxdepth: np.ndarray) -> 
 
 
 def compare(args):
-    ref = np.load(args.ref)
-    gpu = np.load(args.gpu)
+    print(json.dumps(compare_files(args.ref, args.gpu, args.only)))
+
+
+def record(args):
+    """Compares several (label, FP64 record, GPU record, prefix) sets and writes them as one JSON
+    record: a list of {"case", "steps", per-form results}; a label ending in "!" marks a member
+    whose FP64 run itself goes non-finite (the comparison then stops at the last finite record)."""
+    out = {"generated_by": "tests/long_run.py record", "entries": []}
+    for spec in args.spec:
+        label, ref, gpu, only = (spec.split("=", 1)[0],) + tuple(spec.split("=", 1)[1].split(","))
+        res = compare_files(ref, gpu, only or None)
+        res["case"] = label.rstrip("!")
+        if label.endswith("!"):
+            res["fp64_nonfinite"] = True
+        out["entries"].append(res)
+    with open(args.out, "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {len(out['entries'])} entries to {args.out}")
+
+
+def compare_files(ref_path: str, gpu_path: str, only: str | None) -> dict:
+    ref = np.load(ref_path)
+    gpu = np.load(gpu_path)
     B = ref["bottom"].astype(np.float64)
     I = (slice(2, -2), slice(2, -2))
     swl = 0.0
@@ -160,8 +182,8 @@ def compare(args):
     ru_ref = runup(B[I], initial_dry, ref["maxdepth"][I])
     res["fp64_runup_m"] = ru_ref
     forms = sorted({k.split("/")[0] for k in gpu.files if "/" in k})
-    if args.only:
-        forms = [f for f in forms if f == args.only]
+    if only:
+        forms = [f for f in forms if f == only]
     for f in forms:
         d = gpu[f"{f}/eta"].astype(np.float64)[I] - swl - eta_ref
         m = gpu[f"{f}/mass"]
@@ -176,7 +198,11 @@ def compare(args):
             "mass_rel_diff_max": float(np.max(np.abs(m[:n] - m_ref[:n]) / m_ref[:n])),
             "closed_basin_drift": float(np.max(np.abs(m - m[0])) / m[0]),
         }
-    print(json.dumps(res))
+        if not np.isfinite(m_ref).all():
+            last = int(np.argmax(~np.isfinite(m_ref)))
+            res[f]["fp64_finite_records"] = last
+    res["steps"] = int(ref["every"]) * (len(m_ref) - 1)
+    return res
 
 
 def main():
@@ -192,12 +218,15 @@ def main():
         if name == "gpu":
             s.add_argument("--forms", default="mixed,fused,plain")
             s.add_argument("--members", default="0,1,4,5,6", help="c4: ensemble members to record")
+    r = sub.add_parser("record")
+    r.add_argument("--out", required=True)
+    r.add_argument("spec", nargs="+", help="label=ref.npz,gpu.npz,prefix (prefix may be empty)")
     c = sub.add_parser("compare")
     c.add_argument("ref")
     c.add_argument("gpu")
     c.add_argument("--only", default=None, help="compare one record prefix (e.g. m5 for C4 member 5)")
     a = ap.parse_args()
-    {"oracle": run_oracle, "gpu": run_gpu, "compare": compare}[a.cmd](a)
+    {"oracle": run_oracle, "gpu": run_gpu, "compare": compare, "record": record}[a.cmd](a)
 
 
 if __name__ == "__main__":
