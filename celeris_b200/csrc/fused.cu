@@ -250,7 +250,8 @@ __device__ __forceinline__ float friction_fast(float hu, float hv, float h, floa
     return f * sqrtf(hu * hu + hv * hv) * dbh * dbh;
 }
 
-struct Face { float hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, msd; };
+// face depths h, velocities u, v, and the face water levels w (h = w - face bottom)
+struct Face { float hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, wN, wE, wS, wW, msd; };
 
 // MinMod (compute.hlsl:292-296) without branches: all three positive <=> their minimum is
 // positive, all negative <=> their maximum is negative (identical results for finite inputs).
@@ -321,6 +322,7 @@ __device__ __forceinline__ void faces_at(const float* __restrict__ ring, int bm,
     correct_w_fast(BW, BE, wc, wW, wE);
     correct_w_fast(BS, BN, wc, wS, wN);
     f.hN = wN - BN; f.hE = wE - BE; f.hS = wS - BS; f.hW = wW - BW;
+    f.wN = wN; f.wE = wE; f.wS = wS; f.wW = wW;
     float q;
     q = div_by_h_fast(f.hN, c.epsilon); f.uN = q * huN; f.vN = q * hvN;
     q = div_by_h_fast(f.hE, c.epsilon); f.uE = q * huE; f.vE = q * hvE;
@@ -330,16 +332,19 @@ __device__ __forceinline__ void faces_at(const float* __restrict__ ring, int bm,
 }
 
 // KP07 flux through one face for the three equations, given the two face states (m: the side
-// with the lower index, p: the other); `xdir` selects the velocity normal to the face.
-__device__ __forceinline__ void face_flux(float hm, float um, float vm, float hp, float up, float vp, float g,
-                                          float hg, bool xdir, float out[3]) {
+// with the lower index, p: the other); `xdir` selects the velocity normal to the face.  Both
+// sides of a face share its bottom, so the depth jump hp - hm equals the jump of the face water
+// levels wp - wm; it is taken from those, which keep the bits of eta that a depth of several metres
+// rounds away in single precision (at an open boundary that jump carries the mass exchange).
+__device__ __forceinline__ void face_flux(float hm, float um, float vm, float wm, float hp, float up, float vp,
+                                          float wp, float g, float hg, bool xdir, float out[3]) {
     const float cm = sqrtf(g * hm), cpp = sqrtf(g * hp);
     const float nm = xdir ? um : vm, np = xdir ? up : vp;
     const float ap = fmaxf(fmaxf(nm + cm, np + cpp), 0.f);
     const float am = fminf(fminf(nm - cm, np - cpp), 0.f);
     const float qp = hp * np, qm = hm * nm;          // normal mass fluxes
     float Fp[3], Fm[3], dU[3];
-    Fp[0] = qp; Fm[0] = qm; dU[0] = hp - hm;
+    Fp[0] = qp; Fm[0] = qm; dU[0] = wp - wm;
     if (xdir) {
         Fp[1] = hp * (up * up + hg * hp); Fm[1] = hm * (um * um + hg * hm); dU[1] = hp * up - hm * um;
         Fp[2] = qp * vp; Fm[2] = qm * vm; dU[2] = hp * vp - hm * vm;
@@ -362,7 +367,7 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
     __shared__ __align__(128) float ring[6 * FSTR];
     __shared__ float dring[RING * DSTR];  // still-water depth max(0, sea level - BA) of each ring row
     __shared__ __align__(8) unsigned long long bars[RING];
-    __shared__ float fW[2][3][MW];       // [row parity][hW, uW, vW][thread]: west faces for the x flux
+    __shared__ float fW[2][4][MW];       // [row parity][hW, uW, vW, wW][thread]: west faces for the x flux
     __shared__ float xb[3][MW];          // x flux at the thread's east face, this row
     constexpr int OFF = MIXED ? 18 : 9;
     constexpr int iR0 = OFF + 3, iH0 = OFF + 5, iAUX = OFF + 25;
@@ -451,8 +456,8 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
         double mfull = 0.0;
         float mx[4] = {0.f, 0.f, 0.f, 0.f};
         bool bad = false;
-        float nh = 0.f, nu = 0.f, nv = 0.f;       // north face of the previous row (this column)
-        float eh = 0.f, eu = 0.f, ev = 0.f;       // east face of row t (this column), from the last step
+        float nh = 0.f, nu = 0.f, nv = 0.f, nw = 0.f;   // north face of the previous row (this column)
+        float eh = 0.f, eu = 0.f, ev = 0.f, ew = 0.f;   // east face of row t (this column), from the last step
         float ypv0 = 0.f, ypv1 = 0.f, ypv2 = 0.f; // y flux below the current row
 
         const int sA = int(seq0 % RING), sB = next_slot(sA), sC = next_slot(sB);  // rows y0-2, y0-1, y0
@@ -519,7 +524,7 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
             Face f;
             faces_at(ring, bm, b0, bp, c, f);
             const int par1 = (t + 1) & 1;
-            fW[par1][0][tid] = f.hW; fW[par1][1][tid] = f.uW; fW[par1][2][tid] = f.vW;
+            fW[par1][0][tid] = f.hW; fW[par1][1][tid] = f.uW; fW[par1][2][tid] = f.vW; fW[par1][3][tid] = f.wW;
             if (aux_ok) {
                 const float md = fmaxf((f.hN + f.hE + f.hS + f.hW) * 0.25f, aux_old.x);
                 const float bw = (f.msd > M.tan_thr) ? 1.0f : aux_old.y;   // atan(msd) > threshold
@@ -527,13 +532,14 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
             }
             const float g = c.g, hg = c.half_g;
             float yf[3];   // y flux at the north face of row t: north face of row t vs south face of row t+1
-            face_flux(nh, nu, nv, f.hS, f.uS, f.vS, g, hg, false, yf);
+            face_flux(nh, nu, nv, nw, f.hS, f.uS, f.vS, f.wS, g, hg, false, yf);
             // ---- x flux at the east face of (xc, t): east face of row t (registers) vs west face of (xc+1, t)
             const int par = t & 1;
             {
                 const int tn = min(tid + 1, MW - 1);
                 float xo[3];
-                face_flux(eh, eu, ev, fW[par][0][tn], fW[par][1][tn], fW[par][2][tn], g, hg, true, xo);
+                face_flux(eh, eu, ev, ew, fW[par][0][tn], fW[par][1][tn], fW[par][2][tn], fW[par][3][tn], g, hg, true,
+                          xo);
                 xb[0][tid] = xo[0]; xb[1][tid] = xo[1]; xb[2][tid] = xo[2];
             }
             __syncthreads();  // (B)
@@ -635,8 +641,8 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
                 }
             }
             ypv0 = yf[0]; ypv1 = yf[1]; ypv2 = yf[2];
-            nh = f.hN; nu = f.uN; nv = f.vN;
-            eh = f.hE; eu = f.uE; ev = f.vE;
+            nh = f.hN; nu = f.uN; nv = f.vN; nw = f.wN;
+            eh = f.hE; eu = f.uE; ev = f.vE; ew = f.wE;
             // advance the ring window: rows t-1 .. t+3 become t-2 .. t+2
             o2m = o1m; o1m = o0; o0 = o1p; o1p = o2p;
             o2p = (o2p + RSTR == RING * RSTR) ? 0 : o2p + RSTR;
@@ -754,15 +760,15 @@ __device__ __forceinline__ f2 div_by_h2(f2 h, float eps) {
     return mul2(mul2(S2(1.41421354f), h), P2(rsqrtf(t.x), rsqrtf(t.y)));
 }
 
-struct Face2 { f2 hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, msd; };
+struct Face2 { f2 hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, wN, wE, wS, wW, msd; };
 // what the next step needs of a pair's faces: north and east faces of both rows, south face of
-// the second row
+// the second row (depth, velocities, water level)
 struct Carry2 {
-    f2 hN, uN, vN, hE, uE, vE;
-    float hS1, uS1, vS1;
+    f2 hN, uN, vN, wN, hE, uE, vE, wE;
+    float hS1, uS1, vS1, wS1;
     __device__ __forceinline__ void set(const Face2& f) {
-        hN = f.hN; uN = f.uN; vN = f.vN; hE = f.hE; uE = f.uE; vE = f.vE;
-        hS1 = f.hS.y; uS1 = f.uS.y; vS1 = f.vS.y;
+        hN = f.hN; uN = f.uN; vN = f.vN; wN = f.wN; hE = f.hE; uE = f.uE; vE = f.vE; wE = f.wE;
+        hS1 = f.hS.y; uS1 = f.uS.y; vS1 = f.vS.y; wS1 = f.wS.y;
     }
 };
 
@@ -791,6 +797,7 @@ __device__ __forceinline__ void faces_at2(const float* __restrict__ ring, int om
     correct_w2(BW, BE, wc, wW, wE);
     correct_w2(BS, BN, wc, wS, wN);
     f.hN = sub2(wN, BN); f.hE = sub2(wE, BE); f.hS = sub2(wS, BS); f.hW = sub2(wW, BW);
+    f.wN = wN; f.wE = wE; f.wS = wS; f.wW = wW;
     f2 q;
     q = div_by_h2(f.hN, c.epsilon); f.uN = mul2(q, huN); f.vN = mul2(q, hvN);
     q = div_by_h2(f.hE, c.epsilon); f.uE = mul2(q, huE); f.vE = mul2(q, hvE);
@@ -800,8 +807,9 @@ __device__ __forceinline__ void faces_at2(const float* __restrict__ ring, int om
 }
 
 // KP07 fluxes through a pair of faces (m: lower-index side, p: the other); xdir selects the normal.
-__device__ __forceinline__ void face_flux2(f2 hm, f2 um, f2 vm, f2 hp, f2 up, f2 vp, float g, float hg, bool xdir,
-                                           f2 out[3]) {
+// The depth jump is taken from the face water levels, as in face_flux.
+__device__ __forceinline__ void face_flux2(f2 hm, f2 um, f2 vm, f2 wm, f2 hp, f2 up, f2 vp, f2 wp, float g, float hg,
+                                           bool xdir, f2 out[3]) {
     const f2 cm = P2(sqrtf(g * hm.x), sqrtf(g * hm.y)), cpp = P2(sqrtf(g * hp.x), sqrtf(g * hp.y));
     const f2 nm = xdir ? um : vm, np = xdir ? up : vp;
     const f2 ap = max2(max2(add2(nm, cm), add2(np, cpp)), S2(0.f));
@@ -809,7 +817,7 @@ __device__ __forceinline__ void face_flux2(f2 hm, f2 um, f2 vm, f2 hp, f2 up, f2
     const f2 qp = mul2(hp, np), qm = mul2(hm, nm);
     const f2 hgv = S2(hg);
     f2 Fp[3], Fm[3], dU[3];
-    Fp[0] = qp; Fm[0] = qm; dU[0] = sub2(hp, hm);
+    Fp[0] = qp; Fm[0] = qm; dU[0] = sub2(wp, wm);
     if (xdir) {
         Fp[1] = mul2(hp, fma2(hgv, hp, mul2(up, up))); Fm[1] = mul2(hm, fma2(hgv, hm, mul2(um, um)));
         dU[1] = sub2(mul2(hp, up), mul2(hm, um));
@@ -844,7 +852,7 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
     extern __shared__ __align__(128) float ring[];   // 6 * FSTR2 floats (dynamic: the total passes 48 KB)
     __shared__ float dring[RING2 * RSTR];   // still-water depth of each ring row (same stride as the ring)
     __shared__ __align__(8) unsigned long long bars[RING2];
-    __shared__ float fW[2][2][3][TW];       // [step parity][row of the pair][hW, uW, vW][thread]
+    __shared__ float fW[2][2][4][TW];       // [step parity][row of the pair][hW, uW, vW, wW][thread]
     __shared__ float xb[2][3][TW];          // [row of the pair][component][thread]
     constexpr int OFF = MIXED ? 18 : 9;
     constexpr int iR0 = OFF + 3, iH0 = OFF + 5, iAUX = OFF + 25;
@@ -961,6 +969,7 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
             const int pp = 1;   // parity of step -1
             fW[pp][0][0][tid] = fq.hW.x; fW[pp][0][1][tid] = fq.uW.x; fW[pp][0][2][tid] = fq.vW.x;
             fW[pp][1][0][tid] = fq.hW.y; fW[pp][1][1][tid] = fq.uW.y; fW[pp][1][2][tid] = fq.vW.y;
+            fW[pp][0][3][tid] = fq.wW.x; fW[pp][1][3][tid] = fq.wW.y;
         }
         {   // aux of row y0-1 (the ghost row y = 1 belongs to the first strip)
             const int gy = y0 - 1;
@@ -1031,6 +1040,7 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
             const int npar = (j + 1) & 1, par = j & 1;
             fW[npar][0][0][tid] = f.hW.x; fW[npar][0][1][tid] = f.uW.x; fW[npar][0][2][tid] = f.vW.x;
             fW[npar][1][0][tid] = f.hW.y; fW[npar][1][1][tid] = f.uW.y; fW[npar][1][2][tid] = f.vW.y;
+            fW[npar][0][3][tid] = f.wW.x; fW[npar][1][3][tid] = f.wW.y;
             {
                 const f2 md = mul2(add2(add2(f.hN, f.hE), add2(f.hS, f.hW)), S2(0.25f));
                 if (aux_ok[0]) {
@@ -1044,14 +1054,14 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
             }
             const float g = c.g, hg = c.half_g;
             f2 yf[3];   // north faces of rows t, t+1: (N(t) vs S(t+1)), (N(t+1) vs S(t+2))
-            face_flux2(fp.hN, fp.uN, fp.vN, P2(fp.hS1, f.hS.x), P2(fp.uS1, f.uS.x), P2(fp.vS1, f.vS.x), g, hg,
-                       false, yf);
+            face_flux2(fp.hN, fp.uN, fp.vN, fp.wN, P2(fp.hS1, f.hS.x), P2(fp.uS1, f.uS.x), P2(fp.vS1, f.vS.x),
+                       P2(fp.wS1, f.wS.x), g, hg, false, yf);
             {   // x fluxes of rows t, t+1 at this thread's east face
                 const int tn = min(tid + 1, TW - 1);
                 f2 xo[3];
-                face_flux2(fp.hE, fp.uE, fp.vE, P2(fW[par][0][0][tn], fW[par][1][0][tn]),
-                           P2(fW[par][0][1][tn], fW[par][1][1][tn]), P2(fW[par][0][2][tn], fW[par][1][2][tn]), g,
-                           hg, true, xo);
+                face_flux2(fp.hE, fp.uE, fp.vE, fp.wE, P2(fW[par][0][0][tn], fW[par][1][0][tn]),
+                           P2(fW[par][0][1][tn], fW[par][1][1][tn]), P2(fW[par][0][2][tn], fW[par][1][2][tn]),
+                           P2(fW[par][0][3][tn], fW[par][1][3][tn]), g, hg, true, xo);
 #pragma unroll
                 for (int k = 0; k < 3; ++k) { xb[0][k][tid] = xo[k].x; xb[1][k][tid] = xo[k].y; }
             }
@@ -1740,8 +1750,9 @@ __global__ void __launch_bounds__(128) k_cols_serial(const MemberDev* __restrict
 // the lanes).  The narrow strips of the other kinds keep one cell per thread, so they still spread
 // over the SMs.
 // phase 0: compute and write in place; 1: compute into the member's scratch; 2: copy back.
-// The compensated form evaluates the sponge, sine, irregular and time-series values in FP64 and
-// stores them as a float pair (value + low word), so the strips keep the state's precision.
+// The compensated form evaluates the sine, irregular and time-series values in FP64 and applies the
+// sponge's factor to the full compensated value in FP64; it stores the results as a float pair
+// (value + low word), so the strips keep the state's precision.
 // ---------------------------------------------------------------------------------------------
 constexpr double CEL_PI_D = 3.14159265358979323846;
 constexpr double CEL_MIN_DEPTH_D = 0.0001;   // compute.hlsl:1062
@@ -1750,11 +1761,6 @@ constexpr double CEL_MIN_DEPTH_D = 0.0001;   // compute.hlsl:1062
 __device__ __forceinline__ void split_hl(double v, float& hi, float& lo) {
     hi = float(v);
     lo = float(v - double(hi));
-}
-
-// SpongeFunction (compute.hlsl:1056-1059) in FP64
-__device__ __forceinline__ double sponge_fn_d(double L, double x) {
-    return 0.5 + 0.5 * cos(CEL_PI_D * fmax(L - x, 0.0) / L);
 }
 
 // sineWave with Eckart's wavenumber (compute.hlsl:1080-1101) in FP64
@@ -1888,13 +1894,14 @@ __device__ __forceinline__ void sponge_geometry(int side, int x, int y, int NX, 
     else { L = T(width) * dy; dist = T(NY - y) * dy; }
 }
 
-// The sponge's damping factor at one texel in FP64 (compensated form)
-__device__ __forceinline__ double sponge_gamma_d(const MemberDev& M, const BoundaryDesc& b, int side, int x, int y,
-                                                 float ba) {
-    double L, dist;
-    sponge_geometry(side, x, y, M.c.NX, M.c.NY, b.width, M.dx64, M.dy64, L, dist);
-    const double dh = fmax(CEL_MIN_DEPTH_D, b.sea_level64 - double(ba));
-    return sponge_fn_d(L, dist) / sponge_fn_d(L, dist + sqrt(M.g64 * dh) * double(*M.dtp));
+// The sponge's damping factor at one texel (compute.hlsl:1011-1060), in single precision as the
+// reference evaluates it; the compensated form applies it to the full (hi, lo) value in FP64.
+__device__ __forceinline__ float sponge_gamma(const MemberDev& M, const BoundaryDesc& b, int side, int x, int y,
+                                              float ba) {
+    float L, dist;
+    sponge_geometry(side, x, y, M.c.NX, M.c.NY, b.width, M.c.dx, M.c.dy, L, dist);
+    const float dh = fmaxf(CEL_MIN_DEPTH, b.sea_level - ba);
+    return sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(M.c.g * dh) * (*M.dtp));
 }
 
 // The sponged texel (hi, lo) pairs in place: eta scaled about the sea level, hu and hv scaled
@@ -1941,7 +1948,6 @@ __global__ void __launch_bounds__(256, 2) k_boundary(const MemberDev* __restrict
         if (b.type == CEL_BC_SPONGE && phase == 0) {
             // Pointwise: the loads of all the thread's cells are issued before the first store.
             const float sl = b.sea_level;
-            const float dt = *M.dtp;
             size_t gi[BND_CPT];
             int cx[BND_CPT], cy[BND_CPT];
             float vw[BND_CPT], vu[BND_CPT], vv[BND_CPT], ba[BND_CPT];
@@ -1962,16 +1968,12 @@ __global__ void __launch_bounds__(256, 2) k_boundary(const MemberDev* __restrict
 #pragma unroll
             for (int k = 0; k < BND_CPT; ++k) {
                 if (!ok[k]) continue;
+                const float gam = sponge_gamma(M, b, side, cx[k], cy[k], ba[k]);
                 if (MIXED) {
-                    const double gam = sponge_gamma_d(M, b, side, cx[k], cy[k], ba[k]);
                     sponge_apply_d(gam, b.sea_level64, vw[k], l0[k], vu[k], l1[k], vv[k], l2[k]);
                     W[gi[k]] = vw[k]; HU[gi[k]] = vu[k]; HV[gi[k]] = vv[k];
                     LW[gi[k]] = l0[k]; LU[gi[k]] = l1[k]; LV[gi[k]] = l2[k];
                 } else {
-                    float L, dist;
-                    sponge_geometry(side, cx[k], cy[k], NX, NY, b.width, c.dx, c.dy, L, dist);
-                    const float dh = fmaxf(CEL_MIN_DEPTH, sl - ba[k]);
-                    const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * dt);
                     W[gi[k]] = gam * (vw[k] - sl) + sl;
                     HU[gi[k]] = gam * vu[k];
                     HV[gi[k]] = gam * vv[k];
@@ -2044,14 +2046,11 @@ __global__ void __launch_bounds__(256, 2) k_boundary(const MemberDev* __restrict
                 ov = (side == 0 || side == 2) ? -sv : sv; lv = (side == 0 || side == 2) ? -lv_ : lv_;
             } else if (b.type == CEL_BC_SPONGE) {
                 ow = W[gi]; ou = HU[gi]; ov = HV[gi];
+                const float gam = sponge_gamma(M, b, side, x, y, M.BA[gi]);
                 if (MIXED) {
                     lw = LW[gi]; lu = LU[gi]; lv = LV[gi];
-                    sponge_apply_d(sponge_gamma_d(M, b, side, x, y, M.BA[gi]), b.sea_level64, ow, lw, ou, lu, ov, lv);
+                    sponge_apply_d(gam, b.sea_level64, ow, lw, ou, lu, ov, lv);
                 } else {
-                    float L, dist;
-                    sponge_geometry(side, x, y, NX, NY, b.width, c.dx, c.dy, L, dist);
-                    const float dh = fmaxf(CEL_MIN_DEPTH, sl - M.BA[gi]);
-                    const float gam = sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(c.g * dh) * (*M.dtp));
                     ow = gam * (ow - sl) + sl;
                     ou = gam * ou;
                     ov = gam * ov;
