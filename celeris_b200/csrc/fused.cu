@@ -1894,14 +1894,23 @@ __device__ __forceinline__ void sponge_geometry(int side, int x, int y, int NX, 
     else { L = T(width) * dy; dist = T(NY - y) * dy; }
 }
 
-// The sponge's damping factor at one texel (compute.hlsl:1011-1060), in single precision as the
-// reference evaluates it; the compensated form applies it to the full (hi, lo) value in FP64.
+// The sponge's damping factor at one texel (compute.hlsl:1011-1060): SpongeFunction(L, d) /
+// SpongeFunction(L, d + sqrt(g h) dt) with SpongeFunction(L, x) = 0.5 + 0.5 cos(pi max(L - x, 0) / L).
+// The fused forms evaluate the same function as sin^2(pi min(x, L) / (2 L)), which it equals: near
+// x = 0 the cosine form cancels to zero in single precision, and at the strip's outermost texel over
+// dry ground (depth clamped to 1e-4 m, so the shifted distance is under a millimetre) both sponge
+// values round to 0 and their ratio is 0/0.  The compensated form applies the factor to the full
+// (hi, lo) value in FP64.
+__device__ __forceinline__ float sponge_sin2(float L, float x) {
+    const float s = sinf((0.5f * CEL_PI_F) * (fminf(x, L) / L));
+    return s * s;
+}
 __device__ __forceinline__ float sponge_gamma(const MemberDev& M, const BoundaryDesc& b, int side, int x, int y,
                                               float ba) {
     float L, dist;
     sponge_geometry(side, x, y, M.c.NX, M.c.NY, b.width, M.c.dx, M.c.dy, L, dist);
     const float dh = fmaxf(CEL_MIN_DEPTH, b.sea_level - ba);
-    return sponge_fn(L, dist) / sponge_fn(L, dist + sqrtf(M.c.g * dh) * (*M.dtp));
+    return sponge_sin2(L, dist) / sponge_sin2(L, dist + sqrtf(M.c.g * dh) * (*M.dtp));
 }
 
 // The sponged texel (hi, lo) pairs in place: eta scaled about the sea level, hu and hv scaled

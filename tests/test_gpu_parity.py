@@ -306,19 +306,23 @@ def test_batch_stats_describe_the_start_of_the_last_step(celeris):
 
 
 def test_tuning_changes_decomposition_not_results(celeris):
-    """Band width and strip height only change how the work is split: the fields agree to FP32
+    """Band width, strip height and the column solver's chunks per column (its switch point from
+    the carry scan to serial sweeps) only change how the work is split: the fields agree to FP32
     rounding (the column scans group their additions differently)."""
     members = [_case(k, nx=150 + 10 * i, ny=70 + 30 * i, N=1)[:4] for i, k in enumerate(["mixed", "sponge", "irregular"])]
     ref = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
     ref.step(30)
-    for bw, sh in [(32, 32), (8, 128), (16, 8), (1, 64)]:
+    for bw, sh, chunks in [(32, 32, 16), (32, 64, 8), (8, 128, 64), (8, 32, 32), (16, 8, 16), (16, 64, 32), (1, 64, 0)]:
         b = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
-        b.set_tuning(bw, sh)
+        b.set_tuning(bw, sh, chunks)
         assert b.tuning == (bw, sh)
+        assert b.col_chunks == (chunks if bw > 1 else 1)
         b.step(30)
         for i in range(len(members)):
             errs = field_errors(b.state(i), ref.state(i))
-            assert rel_ok(errs, 1e-5, 1e-9), (bw, sh, errs)
+            assert rel_ok(errs, 1e-5, 1e-9), (bw, sh, chunks, errs)
+    with pytest.raises(celeris.CelError):   # 16 columns x 48 chunks = 768 threads: not a solver size
+        celeris.Batch([(m[0], m[1]) for m in members], "mixed").set_tuning(16, 64, 48)
     t = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
     got = t.autotune(2)
     assert got["band_width"] in (1, 8, 16, 32) and got["strip_height"] in (32, 64, 128) and got["ms_per_step"] > 0
