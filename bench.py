@@ -62,6 +62,9 @@ def parse():
                     help="force the stencil strip threads (with two rows per step) after tuning; 0 keeps the choice")
     ap.add_argument("--band-width", type=int, default=0, help="force the column band width after tuning (0 keeps it)")
     ap.add_argument("--strip-height", type=int, default=0, help="force the stencil strip height after tuning (0 keeps it)")
+    ap.add_argument("--col-chunks", type=int, default=0,
+                    help="force the column solver's chunks per column after tuning (0 keeps it; 32/64/128 with "
+                         "--band-width 32: the cluster solver)")
     ap.add_argument("--tune-steps", type=int, default=6, help="steps per autotuner candidate (0 keeps the defaults)")
     ap.add_argument("--scaling", default="weak", choices=["weak", "strong"],
                     help="weak: a full ensemble per GPU; strong: one ensemble split over the GPUs by cost")
@@ -199,7 +202,8 @@ def sampled_member_accuracy(batch, members, steps_cap: int):
     """The smallest member of the benchmarked batch, as it stands after every step the run took,
     against the FP64 oracle stepped as many times from the same initial condition: eta RMS over the
     interior (m) and the relative difference of the FP64 water volume.  The member's FP64 clock
-    gives its step count exactly (it sums the float time step once per step).  Skipped when the
+    gives its step count exactly (it sums the float time step once per step).  Eta is compared on
+    the free surface max(w, B), the bed standing for the surface of a dry cell.  Skipped when the
     oracle would need more than about a minute (steps_cap < 0) or more than steps_cap steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -216,7 +220,9 @@ def sampled_member_accuracy(batch, members, steps_cap: int):
     o.physical_steps(nsteps - 4)
     ref = o.state()
     got = batch.state(k)
-    d = got[2:-2, 2:-2, 0].astype(np.float64) - ref[2:-2, 2:-2, 0]
+    # eta on the free surface max(w, B): the water level where there is water, the bed where dry
+    bed = o.bottom()[2:-2, 2:-2, 2]
+    d = np.maximum(got[2:-2, 2:-2, 0].astype(np.float64), bed) - np.maximum(ref[2:-2, 2:-2, 0], bed)
     m_ref = o.reset_timestep()["mass_full"]
     return {"member": k, "size": [int(p.nx), int(p.ny)], "steps": nsteps,
             "eta_rms_m": float(np.sqrt(np.mean(d * d))), "eta_max_abs_m": float(np.max(np.abs(d))),
@@ -347,8 +353,8 @@ def main():
             batch.set_stencil_rows(args.stencil_rows)
         if args.stencil_width:
             batch.set_stencil_width(args.stencil_width)
-        if args.band_width or args.strip_height:
-            batch.set_tuning(args.band_width, args.strip_height)
+        if args.band_width or args.strip_height or args.col_chunks:
+            batch.set_tuning(args.band_width, args.strip_height, args.col_chunks)
         batch.step(max(3, args.warmup))
     torch.cuda.synchronize()
 
@@ -492,9 +498,13 @@ def main():
                                   "pcr_switch": {
                                       "column_chunks": batch.col_chunks,
                                       "rows_per_chunk_tallest_member": -(-max(m[0].ny for m in members) // batch.col_chunks),
+                                      "cluster_ctas": (batch.col_chunks // 8
+                                                       if batch.tuning[0] == 32 and batch.col_chunks >= 32 else 0),
                                       "meaning": "column solver: L and U sweeps split into this many chunks per "
-                                                 "column, joined by warp-shuffle recursive doubling, each chunk "
-                                                 "swept serially (Thomas)"}}},
+                                                 "column, each swept serially (Thomas) and joined by a scan of "
+                                                 "their transfer maps (warp shuffles; with cluster_ctas > 0 "
+                                                 "through the distributed shared memory of a CTA cluster, every "
+                                                 "chunk held in registers)"}}},
             "e2e": {"value": e2e_value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

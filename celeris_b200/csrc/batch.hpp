@@ -19,6 +19,10 @@ struct cel_batch;
 
 namespace cel {
 
+// Room the banded column solver leaves beside its forward values (max_ny x band width floats of
+// dynamic shared memory) for its static shared memory: the chunks' transfer maps and carries.
+constexpr size_t COLS_STATIC_SMEM = 16384;
+
 // ---- one lane (fused.cu) ----------------------------------------------------------------------
 cel_lane* lane_create(int n, const cel_params* const* params, const float* const* bathy, const int* bnx,
                       const int* bny, int form, std::string& err);

@@ -1505,9 +1505,17 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
     // Column (y) solves: a CTA takes a band of CW adjacent columns, thread (c, k) runs chunk k of
     // column c; CW consecutive threads read CW consecutive floats of one row.  Every loop over a
     // chunk's rows issues the loads of CU rows before using them, so each thread keeps several rows
-    // of requests in flight (the recurrences themselves are serial).  The chunks' transfer maps are
-    // joined by recursive doubling over the chunks of a column (warp shuffles), i.e. parallel
-    // reduction of the L and U sweeps down to chunks of ceil(ny / NCH) rows swept serially.
+    // of requests in flight (the recurrences themselves are serial).  Three walks over a chunk:
+    //   1. down: the forward sweep from zero, y0_i (kept in shared memory), with the chunk's forward
+    //      map y_end = A y_in + y0_end and, from the same values, its backward map in terms of the
+    //      carry in: x_top = Q x_below + Z0 + Z1 y_in (Q = prod(-c'), Z0 = sum q_i y0_i,
+    //      Z1 = sum q_i P_i with q_i = prod_{j<i}(-c'_j), P_i = prod_{j<=i} m_j, since
+    //      y_i = y0_i + P_i y_in);
+    //   then the carries into every chunk of the forward sweep and, right after, of the backward
+    //   sweep, each by recursive doubling over the chunks of a column (warp shuffles), i.e. parallel
+    //   reduction of the L and U sweeps down to chunks of ceil(ny / NCH) rows swept serially;
+    //   2. down: y_i = y0_i + P_i y_in;
+    //   3. up: x_i = y_i - c'_i x_{i+1} from the chunk's carry, hv = base + x.
     constexpr int NTC = NT;
     constexpr int NCH = NTC / CW;
     // carry scans: one warp per column; each of the first LN lanes holds G consecutive chunks
@@ -1516,7 +1524,8 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
     static_assert(NCH % LN == 0, "carry scan layout");
     constexpr int CU = 8;
     extern __shared__ float cs[];
-    __shared__ float carP[NCH][CW], carY[NCH][CW], carry_in[NCH][CW];
+    __shared__ float carP[NCH][CW], carY[NCH][CW], carQ[NCH][CW], carZ0[NCH][CW], carZ1[NCH][CW];
+    __shared__ float cin_f[NCH][CW], cin_b[NCH][CW];
     const int c = threadIdx.x % CW, k = threadIdx.x / CW;
     for (int it = blockIdx.x; it < nbands; it += gridDim.x) {
         const int2 bd = bands[it];
@@ -1532,56 +1541,90 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
         const float* __restrict__ mm = M.FYF[2] + gx;
         auto at = [&](int i) { return size_t(i + 2) * P; };   // row offset of system element i
         __syncthreads();
-        float yv = 0.f, pa_ = 1.f;
+        float yv = 0.f, pa_ = 1.f, q = 1.f, z0 = 0.f, z1 = 0.f;
         if (col_ok)
             for (int i = i0; i < i1; i += CU) {
-                float mv[CU], iv[CU], rv[CU];
+                float mv[CU], iv[CU], rv[CU], cv[CU];
 #pragma unroll
                 for (int u = 0; u < CU; ++u) {
                     const bool ok = i + u < i1;
                     mv[u] = ok ? __ldg(mm + at(i + u)) : 0.f;
                     iv[u] = ok ? __ldg(inv + at(i + u)) : 0.f;
                     rv[u] = ok ? __ldg(r + at(i + u)) : 0.f;
+                    cv[u] = ok ? __ldg(cp + at(i + u)) : 0.f;
                 }
 #pragma unroll
                 for (int u = 0; u < CU; ++u)
                     if (i + u < i1) {
                         yv = iv[u] * rv[u] + mv[u] * yv;
                         pa_ *= mv[u];
+                        z0 += q * yv;
+                        z1 += q * pa_;
+                        q *= -cv[u];
                         cs[(i + u) * CW + c] = yv;
                     }
             }
         carP[k][c] = pa_;
         carY[k][c] = yv;
+        carQ[k][c] = q;
+        carZ0[k][c] = z0;
+        carZ1[k][c] = z1;
         __syncthreads();
-        // carries into the chunks of each column: warp w < CW scans column w's 32 chunk maps
+        // forward carries into the chunks of each column: warp w < CW scans column w's chunk maps;
+        // each chunk's backward map then follows from its carry
         for (int col = threadIdx.x >> 5; col < CW; col += NTC / 32) {   // warp-uniform loop
-            const int q = threadIdx.x & 31;
+            const int qq = threadIdx.x & 31;
             Affine loc{1.f, 0.f};
-            if (q < LN) {
+            if (qq < LN) {
 #pragma unroll
-                for (int g = 0; g < G; ++g) loc = compose(Affine{carP[q * G + g][col], carY[q * G + g][col]}, loc);
+                for (int g = 0; g < G; ++g) loc = compose(Affine{carP[qq * G + g][col], carY[qq * G + g][col]}, loc);
             }
             Affine inc = loc;
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
                 const Affine o = Affine{__shfl_up_sync(0xffffffffu, inc.a, off), __shfl_up_sync(0xffffffffu, inc.b, off)};
-                if (q >= off) inc = compose(inc, o);
+                if (qq >= off) inc = compose(inc, o);
             }
             const float before = __shfl_up_sync(0xffffffffu, inc.b, 1);
-            float cur = q > 0 ? before : 0.f;
-            if (q < LN) {
+            float cur = qq > 0 ? before : 0.f;
+            Affine bl{1.f, 0.f};   // this lane's chunks' backward maps composed (x_below -> x_top)
+            if (qq < LN) {
 #pragma unroll
                 for (int g = 0; g < G; ++g) {
-                    carry_in[q * G + g][col] = cur;
-                    cur = carY[q * G + g][col] + carP[q * G + g][col] * cur;
+                    const int kk = qq * G + g;
+                    cin_f[kk][col] = cur;
+                    const float zb = carZ0[kk][col] + carZ1[kk][col] * cur;
+                    carZ0[kk][col] = zb;
+                    cur = carY[kk][col] + carP[kk][col] * cur;
+                }
+#pragma unroll
+                for (int g = G - 1; g >= 0; --g) {
+                    const int kk = qq * G + g;
+                    bl = compose(Affine{carQ[kk][col], carZ0[kk][col]}, bl);
+                }
+            }
+            // backward carries: the mirrored scan from the bottom chunk up
+            Affine binc = bl;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const Affine o = Affine{__shfl_down_sync(0xffffffffu, binc.a, off), __shfl_down_sync(0xffffffffu, binc.b, off)};
+                if (qq + off < 32) binc = compose(binc, o);
+            }
+            const float after = __shfl_down_sync(0xffffffffu, binc.b, 1);
+            float xb = qq < 31 ? after : 0.f;
+            if (qq < LN) {
+#pragma unroll
+                for (int g = G - 1; g >= 0; --g) {
+                    const int kk = qq * G + g;
+                    cin_b[kk][col] = xb;
+                    xb = carZ0[kk][col] + carQ[kk][col] * xb;
                 }
             }
         }
         __syncthreads();
-        float z = 0.f, qa = 1.f;
         if (col_ok) {
-            const float cin = carry_in[k][c];
+            // walk 2: the forward values with the carry in
+            const float cin = cin_f[k][c];
             float pref = 1.f;
             for (int i = i0; i < i1; i += CU) {
                 float mv[CU];
@@ -1594,51 +1637,8 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
                         cs[(i + u) * CW + c] += pref * cin;
                     }
             }
-            for (int i = i1 - 1; i >= i0; i -= CU) {
-                float cv[CU];
-#pragma unroll
-                for (int u = 0; u < CU; ++u) cv[u] = (i - u >= i0) ? __ldg(cp + at(i - u)) : 0.f;
-#pragma unroll
-                for (int u = 0; u < CU; ++u)
-                    if (i - u >= i0) {
-                        z = cs[(i - u) * CW + c] - cv[u] * z;
-                        qa *= -cv[u];
-                        cs[(i - u) * CW + c] = z;
-                    }
-            }
-        }
-        __syncthreads();
-        carP[k][c] = qa;
-        carY[k][c] = z;
-        __syncthreads();
-        // carries from the chunks below (higher rows) in the backward sweep: the mirrored scan
-        for (int col = threadIdx.x >> 5; col < CW; col += NTC / 32) {   // warp-uniform loop
-            const int q = threadIdx.x & 31;
-            Affine loc{1.f, 0.f};
-            if (q < LN) {
-#pragma unroll
-                for (int g = G - 1; g >= 0; --g) loc = compose(Affine{carP[q * G + g][col], carY[q * G + g][col]}, loc);
-            }
-            Affine inc = loc;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const Affine o = Affine{__shfl_down_sync(0xffffffffu, inc.a, off), __shfl_down_sync(0xffffffffu, inc.b, off)};
-                if (q + off < 32) inc = compose(inc, o);
-            }
-            const float after = __shfl_down_sync(0xffffffffu, inc.b, 1);
-            float cur = q < 31 ? after : 0.f;
-            if (q < LN) {
-#pragma unroll
-                for (int g = G - 1; g >= 0; --g) {
-                    carry_in[q * G + g][col] = cur;
-                    cur = carY[q * G + g][col] + carP[q * G + g][col] * cur;
-                }
-            }
-        }
-        __syncthreads();
-        if (col_ok) {
-            const float cnext = carry_in[k][c];
-            float suf = 1.f;
+            // walk 3: the backward sweep from the carry below, hv = base + x
+            float x = cin_b[k][c];
             const int out = pa.out, base = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
             const float* __restrict__ bhi = M.S[base][2] + gx;
             float* __restrict__ ohi = M.S[out][2] + gx;
@@ -1656,8 +1656,7 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
 #pragma unroll
                 for (int u = 0; u < CU; ++u)
                     if (i - u >= i0) {
-                        suf *= -cv[u];
-                        const float x = cs[(i - u) * CW + c] + suf * cnext;
+                        x = cs[(i - u) * CW + c] - cv[u] * x;
                         if (MIXED) {
                             float hi = bh[u], lo = bl[u];
                             two_sum_add(hi, lo, x);
@@ -1740,6 +1739,176 @@ __global__ void __launch_bounds__(128) k_cols_serial(const MemberDev* __restrict
                 }
             }
     }
+}
+
+// Column (y) solves by thread-block clusters, every input read once and held in registers.  A
+// cluster of CL CTAs takes a band of 32 adjacent columns and splits its height into CL x CKC chunks
+// of at most CMC rows: warp k of the CTA of cluster rank r owns chunk r*CKC + k, lane j the column
+// x0 + j, so every load is a 128-byte row piece and a warp keeps 16 rows of its chunk in flight for
+// each array.  Per chunk the thread computes, from its registers:
+//   forward map   y_end = A y_in + b                      (A = prod m, b = chunk sweep from 0)
+//   backward map  x_top = Q x_below + Z0 + Z1 y_in        (Q = prod(-c'); Z0, Z1 from the zero-start
+//                 forward values y0_i and the running products P_i, since y_i = y0_i + P_i y_in)
+// so one exchange fixes every chunk's carry into the forward sweep, and a second one the carry from
+// below into the backward sweep.  The chunk maps are joined inside a CTA through shared memory and
+// across the cluster through distributed shared memory: each CTA pushes its aggregate into the
+// CTAs that need it (lower ranks' forward aggregates to higher ranks, higher ranks' backward
+// aggregates to lower ranks) between hardware cluster barriers.  Then each thread finishes its chunk
+// in registers (y_i = y0_i + P_i y_in, x_i = y_i - c'_i x_{i+1}, hv = base + x) and stores it.
+// Bytes per cell: m, inv, r, c', base (and its low word) in, hv (and its low word) out, each once.
+// The host guarantees ceil(ny / (CL*CKC)) <= CMC for every member of the launch.
+constexpr int CKC = 8, CMC = 16, CL_MAX = 16;
+
+__device__ __forceinline__ void cluster_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
+    return r;
+}
+// stores v into the shared-memory variable at `local` of the cluster's CTA `rank`
+__device__ __forceinline__ void dsmem_store(float* local, unsigned rank, float v) {
+    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(local));
+    unsigned ra;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(ra) : "r"(a), "r"(rank));
+    asm volatile("st.shared::cluster.f32 [%0], %1;\n" ::"r"(ra), "f"(v) : "memory");
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256, 2) k_cols_cluster(const MemberDev* __restrict__ mems,
+                                                         const int2* __restrict__ bands, PassArgs pa) {
+    __shared__ float sA[CKC][32], sB[CKC][32], sQ[CKC][32], sZ0[CKC][32], sZ1[CKC][32];
+    __shared__ float cinK[CKC][32], xK[CKC][32];
+    __shared__ float aggF[CL_MAX][2][32];   // [source rank][A, b][column]: pushed by lower ranks
+    __shared__ float aggB[CL_MAX][2][32];   // [source rank][Q, Z][column]: pushed by higher ranks
+    // every CTA of the cluster must have started before another one stores into its shared memory:
+    // arrive now, wait just before the first remote store
+    cluster_arrive_relaxed();
+    const unsigned CL = cluster_size(), rank = cluster_rank();
+    const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+    const int2 bd = bands[blockIdx.x / CL];
+    const MemberDev& M = mems[bd.x];
+    const int n = M.c.ny, P = M.P;
+    const int gx = bd.y + lane;
+    const bool col_ok = gx >= 2 && gx < M.c.nx + 2;
+    const int nch = int(CL) * CKC;
+    const int mc = (n + nch - 1) / nch;
+    const int i0 = min(n, (int(rank) * CKC + k) * mc);
+    const int cnt = min(n, i0 + mc) - i0;           // rows of this warp's chunk (warp-uniform, may be 0)
+    const size_t o0 = size_t(i0 + 2) * P + gx;      // system element i lies in row i + 2
+    const int base = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
+
+    float mv[CMC], yv[CMC], cv[CMC];
+    {
+        float iv[CMC];
+#pragma unroll
+        for (int u = 0; u < CMC; ++u) {
+            const bool ok = col_ok && u < cnt;
+            const size_t o = o0 + size_t(u) * P;
+            mv[u] = ok ? __ldg(M.FYF[2] + o) : 0.f;
+            iv[u] = ok ? __ldg(M.FYF[1] + o) : 0.f;
+            yv[u] = ok ? __ldg(M.R[1] + o) : 0.f;
+            cv[u] = ok ? __ldg(M.FYF[0] + o) : 0.f;
+        }
+        // forward sweep of the chunk from zero (y0), its map, and the backward partials
+        float y = 0.f, A = 1.f, Q = 1.f, Z0 = 0.f, Z1 = 0.f;
+#pragma unroll
+        for (int u = 0; u < CMC; ++u)
+            if (u < cnt) {
+                y = iv[u] * yv[u] + mv[u] * y;
+                yv[u] = y;
+                A *= mv[u];
+                Z0 += Q * y;
+                Z1 += Q * A;
+                Q *= -cv[u];
+            }
+        sA[k][lane] = A; sB[k][lane] = y; sQ[k][lane] = Q; sZ0[k][lane] = Z0; sZ1[k][lane] = Z1;
+    }
+    // the base state of the chunk: loaded now so that the loads overlap the exchanges
+    float bh[CMC], bl[CMC];
+#pragma unroll
+    for (int u = 0; u < CMC; ++u) {
+        const bool ok = col_ok && u < cnt;
+        const size_t o = o0 + size_t(u) * P;
+        bh[u] = ok ? M.S[base][2][o] : 0.f;
+        bl[u] = (MIXED && ok) ? M.L[base][2][o] : 0.f;
+    }
+    __syncthreads();
+    cluster_wait();   // (every CTA of the cluster has started)
+    if (k == 0) {
+        // this CTA's forward aggregate, pushed to the higher ranks
+        float A = 1.f, b = 0.f;
+        for (int q = 0; q < CKC; ++q) { b = sB[q][lane] + sA[q][lane] * b; A *= sA[q][lane]; }
+        for (unsigned r = rank + 1; r < CL; ++r) {
+            dsmem_store(&aggF[rank][0][lane], r, A);
+            dsmem_store(&aggF[rank][1][lane], r, b);
+        }
+    }
+    cluster_arrive();
+    cluster_wait();
+    if (k == 0) {
+        // carry into this CTA's first row from the ranks above, then into each chunk
+        float cur = 0.f;
+        for (unsigned r = 0; r < rank; ++r) cur = aggF[r][1][lane] + aggF[r][0][lane] * cur;
+        for (int q = 0; q < CKC; ++q) {
+            cinK[q][lane] = cur;
+            sZ0[q][lane] += sZ1[q][lane] * cur;   // the chunk's backward map: x_top = Q x_below + Z
+            cur = sB[q][lane] + sA[q][lane] * cur;
+        }
+        float Qa = 1.f, Za = 0.f;
+        for (int q = CKC - 1; q >= 0; --q) {
+            Za = sZ0[q][lane] + sQ[q][lane] * Za;
+            Qa *= sQ[q][lane];
+        }
+        for (unsigned r = 0; r < rank; ++r) {
+            dsmem_store(&aggB[rank][0][lane], r, Qa);
+            dsmem_store(&aggB[rank][1][lane], r, Za);
+        }
+    }
+    cluster_arrive();
+    cluster_wait();
+    if (k == 0) {
+        // carry from below into this CTA's last row from the ranks below it, then into each chunk
+        float cur = 0.f;
+        for (unsigned r = CL - 1; r > rank; --r) cur = aggB[r][1][lane] + aggB[r][0][lane] * cur;
+        for (int q = CKC - 1; q >= 0; --q) {
+            xK[q][lane] = cur;
+            cur = sZ0[q][lane] + sQ[q][lane] * cur;
+        }
+    }
+    __syncthreads();
+    if (!col_ok || cnt <= 0) return;
+    const float cin = cinK[k][lane];
+    float Pr = 1.f;
+#pragma unroll
+    for (int u = 0; u < CMC; ++u)
+        if (u < cnt) {
+            Pr *= mv[u];
+            yv[u] += Pr * cin;
+        }
+    float x = xK[k][lane];
+    float* __restrict__ ohi = M.S[pa.out][2];
+    float* __restrict__ olo = MIXED ? M.L[pa.out][2] : nullptr;
+#pragma unroll
+    for (int u = CMC - 1; u >= 0; --u)
+        if (u < cnt) {
+            x = yv[u] - cv[u] * x;
+            const size_t o = o0 + size_t(u) * P;
+            if (MIXED) {
+                float hi = bh[u], lo = bl[u];
+                two_sum_add(hi, lo, x);
+                ohi[o] = hi;
+                olo[o] = lo;
+            } else {
+                ohi[o] = bh[u] + x;
+            }
+        }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -2339,6 +2508,7 @@ struct cel_lane {
     long long cells = 0;
     int cw = 16;                        // column solver band width (columns per CTA)
     int cnt = 512;                      // column solver threads per CTA (chunks per column = cnt / cw)
+    int col_cl = 0;                     // cluster column solver: CTAs per cluster (0: not in use)
     int mh = cel::MH_DEFAULT;           // stencil strip height (rows per CTA work item)
     int rows_per_step = 1;              // stencil rows per thread step: 1 (k_march) or 2 (k_march2)
     int mw = 128;                       // stencil CTA width in threads (k_march2: 128 or 96)
@@ -2471,6 +2641,23 @@ int launch_pass(cel_lane* b, const PassArgs& pa, std::string& err) {
         if (b->cw == 1) {
             if (b->mixed) k_cols_serial<true><<<b->grid_cols, 128, 0, b->side>>>(b->ddev, b->bands, b->nbands, pa);
             else k_cols_serial<false><<<b->grid_cols, 128, 0, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+        } else if (b->col_cl > 0) {
+            // one cluster of col_cl CTAs per 32-column band
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(unsigned(b->nbands) * unsigned(b->col_cl));
+            cfg.blockDim = dim3(256);
+            cfg.dynamicSmemBytes = 0;
+            cfg.stream = b->side;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = unsigned(b->col_cl);
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            const MemberDev* md = b->ddev;
+            const int2* bl = b->bands;
+            B_TRY(cudaLaunchKernelEx(&cfg, b->mixed ? k_cols_cluster<true> : k_cols_cluster<false>, md, bl, pa));
         } else {
             auto* kc = cols_kernel(b->mixed, b->cw, b->cnt);
             kc<<<b->grid_cols, b->cnt, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
@@ -2679,7 +2866,37 @@ cudaError_t allow_max_dynamic_smem(const void* kernel) {
 }
 
 int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::string& err) {
-    if (nt != 256 && nt != 512) { err = "column solver threads must be 256 or 512"; return CEL_ERR_ARG; }
+    // 32-column bands with 32, 64 or 128 chunks per column (nt = chunks x 32 = 1024, 2048, 4096):
+    // the cluster solver, 8 chunks per CTA and nt / 256 CTAs per cluster
+    const int cl = (cw == 32 && (nt == 1024 || nt == 2048 || nt == 4096)) ? nt / 256 : 0;
+    if (nt != 256 && nt != 512 && cl == 0) {
+        err = "column solver chunks x band width must be 256 or 512 threads (or 32 columns x 32, 64 or 128 chunks)";
+        return CEL_ERR_ARG;
+    }
+    if (cl > 0 && b->max_ny > cl * CKC * CMC) {
+        err = "column band too tall for the cluster solver (" + std::to_string(cl * CKC * CMC) + " rows at most with " +
+              std::to_string(cl * CKC) + " chunks per column)";
+        return CEL_ERR_ARG;
+    }
+    if (cl > 0) {
+        for (auto* kk : {k_cols_cluster<true>, k_cols_cluster<false>}) {
+            if (cl > 8) B_TRY(cudaFuncSetAttribute(reinterpret_cast<const void*>(kk),
+                                                   cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(unsigned(cl));
+            cfg.blockDim = dim3(256);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = unsigned(cl);
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int nc = 0;
+            B_TRY(cudaOccupancyMaxActiveClusters(&nc, reinterpret_cast<const void*>(kk), &cfg));
+            if (nc < 1) { err = "the device cannot place a cluster of " + std::to_string(cl) + " column-solver CTAs"; return CEL_ERR_ARG; }
+        }
+    }
     if (rps != 1 && rps != 2) { err = "stencil rows per step must be 1 or 2"; return CEL_ERR_ARG; }
     if (mw != 128 && mw != 96) { err = "stencil width must be 128 or 96 threads"; return CEL_ERR_ARG; }
     if (rps == 1) mw = MW;   // the one-row stencil has one width
@@ -2687,8 +2904,8 @@ int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::st
     const int mo = mw - 2;   // output columns per strip
     if (cw != 1 && cw != 8 && cw != 16 && cw != 32) { err = "column band width must be 1, 8, 16 or 32"; return CEL_ERR_ARG; }
     if (mh < 8 || mh > 1024) { err = "strip height must be in [8, 1024]"; return CEL_ERR_ARG; }
-    const size_t smem_cols = cw == 1 ? 0 : sizeof(float) * size_t(b->max_ny) * cw;
-    if (smem_cols + 8192 > 227 * 1024) { err = "column band too wide for the tallest member (shared memory)"; return CEL_ERR_ARG; }
+    const size_t smem_cols = (cw == 1 || cl > 0) ? 0 : sizeof(float) * size_t(b->max_ny) * cw;
+    if (smem_cols + COLS_STATIC_SMEM > 227 * 1024) { err = "column band too wide for the tallest member (shared memory)"; return CEL_ERR_ARG; }
     std::vector<int4> mt;
     std::vector<int2> bd;
     for (int i = 0; i < int(b->mem.size()); ++i) {
@@ -2730,9 +2947,12 @@ int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::st
     b->mh = mh;
     b->mw = mw;
     b->smem_cols = smem_cols;
+    b->col_cl = cl;
     int occ = 1;
     if (cw == 1) {
         b->grid_cols = (b->nbands + 127) / 128;
+    } else if (cl > 0) {
+        b->grid_cols = b->nbands * cl;
     } else {
         ColsKernel kc = cols_kernel(b->mixed, cw, nt);
         B_TRY(allow_max_dynamic_smem(reinterpret_cast<const void*>(kc)));
@@ -3019,7 +3239,7 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
         b->grid_rows = std::max(1, std::min((b->nrows + wpc - 1) / wpc, b->sms * std::max(occ, 1)));
     }
     {   // column bands of 16 columns (8 for tall domains: shared-memory capacity), strips of 64 rows
-        const int cw = (size_t(max_ny) * 16 * sizeof(float) + 8192 <= 227 * 1024) ? 16 : 8;
+        const int cw = (size_t(max_ny) * 16 * sizeof(float) + COLS_STATIC_SMEM <= 227 * 1024) ? 16 : 8;
         if (configure_work(b.get(), cw, MH_DEFAULT, 1, MW, NTC_DEFAULT, err)) return nullptr;
     }
     b->sch.reset(*params[0]);

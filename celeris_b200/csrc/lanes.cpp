@@ -277,8 +277,8 @@ int batch_stencil_width(const cel_batch* b) { return lane_stencil_width(b->lanes
 // the launch mode the batch is set to, two rounds in turn, and keeps the fastest by its better
 // round.  The stencil and the solvers are separate kernels, so the search runs in two stages: the
 // stencil (rows per step and width x strip height) with the default solvers, then the column solver
-// (band width x chunks per column, i.e. the switch point from the carry scan to serial sweeps) with
-// the chosen stencil.  Every lane takes the same candidate and the same steps, so the members stay
+// (band width x chunks per column, i.e. the switch point from the carry scan to serial sweeps, and
+// the cluster solver where the tallest member fits its chunks) with the chosen stencil.  Every lane takes the same candidate and the same steps, so the members stay
 // in step with one another.
 int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, std::string& err) {
     if (steps < 1) { err = "autotune needs at least one step per candidate"; return CEL_ERR_ARG; }
@@ -317,7 +317,7 @@ int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, s
         best_out = best[kb];
         return int(kb);
     };
-    const bool cw16_fits = sizeof(float) * size_t(max_ny) * 16 + 8192 <= 227 * 1024;
+    const bool cw16_fits = sizeof(float) * size_t(max_ny) * 16 + COLS_STATIC_SMEM <= 227 * 1024;
     const int cw0 = cw16_fits ? 16 : 8;
     std::vector<Cand> stencil;
     const int variants[3][2] = {{1, 128}, {2, 128}, {2, 96}};   // stencil rows per step, stencil width
@@ -330,8 +330,12 @@ int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, s
         const Cand st = stencil[size_t(ks)];
         solver.push_back({1, st.mh, st.rps, st.mw, 512});
         for (int cw : {8, 16, 32})
-            if (sizeof(float) * size_t(max_ny) * cw + 8192 <= 227 * 1024)
+            if (sizeof(float) * size_t(max_ny) * cw + COLS_STATIC_SMEM <= 227 * 1024)
                 for (int nt : {256, 512}) solver.push_back({cw, st.mh, st.rps, st.mw, nt});
+        // the cluster solver (32-column bands, 32 or 64 chunks per column of at most 16 rows each,
+        // clusters of 4 or 8 CTAs)
+        for (int nt : {1024, 2048})
+            if (max_ny <= nt / 2) solver.push_back({32, st.mh, st.rps, st.mw, nt});
     }
     const int kb = ks >= 0 ? search(solver, ms) : -1;
     cudaEventDestroy(e0);

@@ -276,7 +276,10 @@ int cel_batch_launches_per_step(const cel_batch* b);
  * solves factor each system once (M = LU, engine.cpp:2612-2887 coefficients); the L and U sweeps of
  * a column are split into that many chunks, each swept serially by one thread (Thomas), and the
  * chunks' transfer maps are joined by recursive doubling with warp shuffles (parallel reduction of
- * the bidiagonal sweeps).  Chunks x band width must be 256 or 512 threads; 0 keeps the current
+ * the bidiagonal sweeps).  Chunks x band width must be 256 or 512 threads, or, with tile_x = 32, 32,
+ * 64 or 128 chunks: the cluster solver, where a cluster of chunks/8 CTAs holds a 32-column band with
+ * every chunk (at most 16 rows, so the tallest member must have at most 16 x chunks rows) in
+ * registers and joins the chunks' maps through distributed shared memory; 0 keeps the current
  * value.  Plain engines ignore the call. */
 int cel_set_tuning(cel_engine* h, int tile_x, int tile_y, int pcr_switch);
 int cel_batch_set_tuning(cel_batch* b, int tile_x, int tile_y, int pcr_switch);

@@ -16,7 +16,9 @@ ensemble as one batch (the production configuration, mixed form, graphs, autotun
 the members listed with ``--members``.  Every
 ``--every`` steps the FP64 total water volume (mass_full) is recorded.
 
-Reported per form: eta RMS over the interior (m), max |eta error| (m), max run-up of each side
+Reported per form: eta RMS over the interior (m) on the free surface max(w, B) (the water level
+where a cell holds water, the bed where it is dry), max |eta error| (m), the RMS of raw w as well
+(it includes dry cells, where w is no surface), max run-up of each side
 and its difference (run-up = highest bed elevation among initially dry cells whose recorded
 maximum inundation depth exceeds 1e-3 m), relative mass difference from the FP64 oracle at the
 end, max over the record, and each side's closed-basin drift |M(t) - M(0)| / M(0).
@@ -184,14 +186,20 @@ def compare_files(ref_path: str, gpu_path: str, only: str | None) -> dict:
     forms = sorted({k.split("/")[0] for k in gpu.files if "/" in k})
     if only:
         forms = [f for f in forms if f == only]
+    # the free surface max(w, B): the water level where a cell holds water, the bed where it is dry
+    # (below the bed, w is no surface: a sponge over dry land pulls it toward sea level)
+    surf_ref = np.maximum(eta_ref + swl, B[I])
     for f in forms:
-        d = gpu[f"{f}/eta"].astype(np.float64)[I] - swl - eta_ref
+        w = gpu[f"{f}/eta"].astype(np.float64)[I]
+        d = np.maximum(w, B[I]) - surf_ref
+        dw = w - swl - eta_ref
         m = gpu[f"{f}/mass"]
         n = min(len(m), len(m_ref))
         ru = runup(B[I], initial_dry, gpu[f"{f}/maxdepth"][I].astype(np.float64))
         res[f] = {
             "eta_rms_m": float(np.sqrt(np.mean(d * d))),
             "eta_max_abs_m": float(np.max(np.abs(d))),
+            "w_rms_m": float(np.sqrt(np.mean(dw * dw))),
             "runup_m": ru,
             "runup_err_m": float(abs(ru - ru_ref)),
             "mass_rel_diff_end": float(abs(m[n - 1] - m_ref[n - 1]) / m_ref[n - 1]),

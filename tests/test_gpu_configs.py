@@ -10,8 +10,12 @@ the benchmark quotes, at step counts the CPU oracle finishes in about a minute e
   and the breaking indicator;
 * C5: the 1,024-member ensemble as one batch, 16 sampled members.
 
-Each comparison checks eta RMS (the 1e-4 m bound), the relative difference of the FP64 water volume,
-the maximum-inundation aux channel and the breaking-indicator aux channel.  The indicator is a
+Each comparison checks eta RMS (the 1e-4 m bound) on the free surface max(w, B), the relative
+difference of the FP64 water volume, the maximum-inundation aux channel and the breaking-indicator
+aux channel.  The surface is the water level where a cell holds water and the bed where it is dry:
+on dry land inside a sponge, w sinks below the bed toward sea level and means nothing (C4 member 4's
+east end, where w of the last column differs by 1e-2 m between the FP32 and FP64 oracles while the
+surface agrees to 1.6e-7 m).  The indicator is a
 threshold decision followed by a decay, so single-precision and FP64 evaluations may decide
 differently where the surface slope sits at the threshold: the test bounds the fraction of cells
 that differ.
@@ -23,6 +27,7 @@ import pytest
 
 import oracle as O
 from celeris_b200 import cases
+from util import surface_rms
 
 pytestmark = pytest.mark.gpu
 
@@ -38,12 +43,13 @@ def _compare(label, state, aux, mass, p, z, bnx, bny, steps):
     m_ref = ref.reset_timestep()["mass_full"]
     I = (slice(2, -2), slice(2, -2))
     d = state[I][..., 0].astype(np.float64) - rs[I][..., 0]
-    rms = float(np.sqrt(np.mean(d * d)))
+    w_rms = float(np.sqrt(np.mean(d * d)))
+    rms = surface_rms(state, rs, ref.bottom()[..., 2])
     mass_rel = abs(mass - m_ref) / m_ref
     depth_err = float(np.max(np.abs(aux[I][..., 0].astype(np.float64) - ra[I][..., 0])))
     brk = np.abs(aux[I][..., 3].astype(np.float64) - ra[I][..., 3]) > 1e-3
     frac = float(brk.mean())
-    print(f"{label}: eta rms {rms:.3e} m, mass rel {mass_rel:.3e}, max-depth err {depth_err:.3e} m, "
+    print(f"{label}: eta rms {rms:.3e} m (w rms {w_rms:.3e} m), mass rel {mass_rel:.3e}, max-depth err {depth_err:.3e} m, "
           f"breaking differs on {frac:.2e} of cells ({int(brk.sum())}), breaking cells {int((ra[I][..., 3] > 0).sum())}")
     assert np.isfinite(state).all(), label
     assert rms <= ETA_RMS, (label, rms)

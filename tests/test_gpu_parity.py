@@ -312,7 +312,8 @@ def test_tuning_changes_decomposition_not_results(celeris):
     members = [_case(k, nx=150 + 10 * i, ny=70 + 30 * i, N=1)[:4] for i, k in enumerate(["mixed", "sponge", "irregular"])]
     ref = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
     ref.step(30)
-    for bw, sh, chunks in [(32, 32, 16), (32, 64, 8), (8, 128, 64), (8, 32, 32), (16, 8, 16), (16, 64, 32), (1, 64, 0)]:
+    for bw, sh, chunks in [(32, 32, 16), (32, 64, 8), (8, 128, 64), (8, 32, 32), (16, 8, 16), (16, 64, 32), (1, 64, 0),
+                           (32, 64, 32), (32, 32, 64), (32, 64, 128)]:   # the last three: cluster solver
         b = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
         b.set_tuning(bw, sh, chunks)
         assert b.tuning == (bw, sh)
@@ -323,6 +324,9 @@ def test_tuning_changes_decomposition_not_results(celeris):
             assert rel_ok(errs, 1e-5, 1e-9), (bw, sh, chunks, errs)
     with pytest.raises(celeris.CelError):   # 16 columns x 48 chunks = 768 threads: not a solver size
         celeris.Batch([(m[0], m[1]) for m in members], "mixed").set_tuning(16, 64, 48)
+    tall = [_case("mixed", nx=40, ny=520, N=1)[:4]]
+    with pytest.raises(celeris.CelError):   # 520 rows > 32 chunks x 16 rows: too tall for the cluster solver
+        celeris.Batch([(m[0], m[1]) for m in tall], "mixed").set_tuning(32, 64, 32)
     t = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
     got = t.autotune(2)
     assert got["band_width"] in (1, 8, 16, 32) and got["strip_height"] in (32, 64, 128) and got["ms_per_step"] > 0

@@ -31,3 +31,16 @@ def rel_ok(errs: dict, rtol: float, atol: float = 0.0) -> bool:
 def eta_rms(gpu: np.ndarray, ref: np.ndarray) -> float:
     d = interior(np.asarray(gpu, dtype=np.float64))[..., 0] - interior(np.asarray(ref, dtype=np.float64))[..., 0]
     return float(np.sqrt(np.mean(d * d)))
+
+
+def surface_rms(gpu: np.ndarray, ref: np.ndarray, bed: np.ndarray) -> float:
+    """RMS over interior cells of the free-surface difference, the surface being max(w, B): the water
+    level where a cell holds water and the bed where it is dry.  Below the bed, w is no surface: a
+    sponge over dry land keeps pulling it toward sea level (w = sl + gamma (w - sl)) while the depth
+    stays 0, and single- and double-precision runs of that decay part by centimetres without moving
+    any water."""
+    b = interior(np.asarray(bed, dtype=np.float64))
+    g = np.maximum(interior(np.asarray(gpu, dtype=np.float64))[..., 0], b)
+    r = np.maximum(interior(np.asarray(ref, dtype=np.float64))[..., 0], b)
+    d = g - r
+    return float(np.sqrt(np.mean(d * d)))
