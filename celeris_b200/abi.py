@@ -209,6 +209,7 @@ def _declare(L: C.CDLL) -> None:
         "cel_kernel_times": (i, [vp, i, C.POINTER(C.c_char * 64), C.POINTER(C.c_double),
                                  C.POINTER(C.c_longlong), i, C.POINTER(i)]),
         "cel_byte_model": (i, [i, i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "cel_selftest_reciprocal": (i, [C.POINTER(C.c_float), C.POINTER(C.c_float), i]),
         "cel_stats_noalloc": (i, [vp, vp, C.POINTER(Params), vp, C.POINTER(Stats)]),
     }
     for name, (res, args) in sig.items():
@@ -243,5 +244,5 @@ EXPORTED = [
     "cel_batch_use_graph", "cel_batch_cells", "cel_batch_set_timestep", "cel_batch_launches_per_step", "cel_set_tuning", "cel_batch_set_tuning",
     "cel_batch_get_tuning", "cel_batch_col_chunks", "cel_batch_set_stencil_rows", "cel_batch_set_stencil_width", "cel_batch_stencil_width",
     "cel_batch_autotune",
-    "cel_batch_kernel_timing", "cel_engine_kernel_timing", "cel_kernel_times", "cel_byte_model", "cel_stats_noalloc",
+    "cel_batch_kernel_timing", "cel_engine_kernel_timing", "cel_kernel_times", "cel_byte_model", "cel_selftest_reciprocal", "cel_stats_noalloc",
 ]

@@ -56,6 +56,8 @@ int lane_col_chunks(const cel_lane* b);   // chunks per column of the column sol
 KernelTimer* lane_timer(cel_lane* b);
 int lane_launches_per_step(const cel_lane* b);
 void byte_model(int form, int correction_steps, double& stencil_bytes, double& step_bytes);
+// the fused forms' flux reciprocal (rcp_newton) over n host values, run on the current device
+int selftest_reciprocal(const float* x, float* out, int n, std::string& err);
 
 // ---- a batch of lanes (lanes.cpp); member indices are the caller's ------------------------------
 // lanes <= 0 picks the default: 2 lanes for 2 or more members, else 1.

@@ -447,6 +447,15 @@ int cel_kernel_times(void* handle, int is_batch, char (*names)[64], double* tota
     CEL_GUARD_END
 }
 
+int cel_selftest_reciprocal(const float* x, float* out, int n) {
+    CEL_GUARD_BEGIN
+    std::string err;
+    const int st = cel::selftest_reciprocal(x, out, n, err);
+    if (st) set_error(err);
+    return st;
+    CEL_GUARD_END
+}
+
 int cel_byte_model(int form, int correction_steps, double* stencil, double* step) {
     double s = 0, t = 0;
     cel::byte_model(form, correction_steps, s, t);

@@ -231,11 +231,25 @@ __device__ __forceinline__ float div_by_h_fast(float h, float eps) {
     const float h2 = h * h, h4 = h2 * h2;
     return 1.41421354f * h * rsqrtf(h4 + fmaxf(h4, eps));
 }
+// Reciprocal of the Kurganov-Petrova denominator a+ - a- (> 0 where it is used): the hardware
+// approximation r0 = __fdividef(1, x), refined by one Newton-Raphson iteration for f(r) = 1/r - x,
+//   r1 = r0 + r0 (1 - x r0),
+// with both steps as fused multiply-adds (Newton's method for the reciprocal, as in Markstein,
+// "IA-64 and Elementary Functions", 2000, ch. 8).  The approximation alone errs with a small
+// systematic bias; through the fluxes at an open boundary the compensated form's water volume
+// picked it up as a steady drift from the FP64 oracle (6.5e-9 of the volume after 10,000 steps of
+// the C1 flume, 3.2e-9 and 2.7e-9 on two C4 members).  Refined, the drift is gone (0.3e-9, 0.4e-9,
+// 0.2e-9) at no measurable cost.  The refined values stay within one unit in the last place of the
+// correctly rounded reciprocal (cel_selftest_reciprocal checks it on the device).
+__device__ __forceinline__ float rcp_newton(float x) {
+    const float r = __fdividef(1.0f, x);
+    return fmaf(r, fmaf(-x, r, 1.0f), r);
+}
 // NumericalFlux for the three components of one face, sharing the reciprocal of a+ - a-
 __device__ __forceinline__ void numflux3(float ap, float am, const float Fp[3], const float Fm[3], const float dU[3],
                                          float out[3]) {
     const float den = ap - am;
-    const float inv = den != 0.f ? __fdividef(1.0f, den) : 0.f;
+    const float inv = den != 0.f ? rcp_newton(den) : 0.f;
     const float apam = ap * am;
 #pragma unroll
     for (int k = 0; k < 3; ++k) out[k] = (ap * Fm[k] - am * Fp[k] + apam * dU[k]) * inv;
@@ -828,7 +842,7 @@ __device__ __forceinline__ void face_flux2(f2 hm, f2 um, f2 vm, f2 wm, f2 hp, f2
         dU[2] = sub2(mul2(hp, vp), mul2(hm, vm));
     }
     const f2 den = sub2(ap, am);
-    const f2 inv = P2(den.x != 0.f ? __fdividef(1.0f, den.x) : 0.f, den.y != 0.f ? __fdividef(1.0f, den.y) : 0.f);
+    const f2 inv = P2(den.x != 0.f ? rcp_newton(den.x) : 0.f, den.y != 0.f ? rcp_newton(den.y) : 0.f);
     const f2 apam = mul2(ap, am);
 #pragma unroll
     for (int k = 0; k < 3; ++k) out[k] = mul2(fma2(apam, dU[k], sub2(mul2(ap, Fm[k]), mul2(am, Fp[k]))), inv);
@@ -2420,6 +2434,11 @@ __global__ void k_choose_dt(DtCtl* __restrict__ ctl, float* __restrict__ dt_tabl
 
 // End of a physical step: advance the clocks by the dt of the step's last pass and, in adaptive
 // batches, shift the controller's dt queue (engine.cpp:1507-1518).
+// rcp_newton over a caller's inputs (the device self-test behind cel_selftest_reciprocal)
+__global__ void k_rcp_selftest(const float* __restrict__ x, float* __restrict__ out, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = rcp_newton(x[i]);
+}
+
 __global__ void k_advance_time(const MemberDev* __restrict__ mems, DtCtl* __restrict__ ctl, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -3694,6 +3713,22 @@ EngineIface* make_fused_engine(const cel_params& p, const float* bathy, int bnx,
         return nullptr;
     }
     return e;
+}
+
+int selftest_reciprocal(const float* x, float* out, int n, std::string& err) {
+    if (n < 0 || (n > 0 && (!x || !out))) { err = "selftest_reciprocal: bad arguments"; return CEL_ERR_ARG; }
+    if (n == 0) return CEL_OK;
+    float* d = nullptr;
+    B_TRY(cudaMalloc(&d, 2 * sizeof(float) * size_t(n)));
+    cudaError_t e = cudaMemcpy(d, x, sizeof(float) * size_t(n), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_rcp_selftest<<<std::min((n + 255) / 256, 4096), 256>>>(d, d + n, n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + n, sizeof(float) * size_t(n), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) { err = std::string("selftest_reciprocal: ") + cudaGetErrorString(e); return CEL_ERR_CUDA; }
+    return CEL_OK;
 }
 
 }  // namespace cel

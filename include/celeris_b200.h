@@ -303,6 +303,11 @@ int cel_engine_kernel_timing(cel_engine* h, int enable);
 /* Copies up to cap (name, total ms, launches) records; returns the count in *n. */
 int cel_kernel_times(void* handle, int is_batch, char (*names)[64], double* total_ms, long long* launches,
                      int cap, int* n);
+/* Device self-test of the fused forms' flux reciprocal (no counterpart in the reference): writes
+ * to out[i] what the Kurganov-Petrova flux uses as 1 / x[i] (the hardware approximation refined by
+ * one Newton-Raphson step), computed on the current device; x and out are host arrays of n floats.
+ * It allocates device memory for the call. */
+int cel_selftest_reciprocal(const float* x, float* out, int n);
 /* Algorithmic HBM bytes per cell for one pass of the dominant kernel and for a whole
  * physical step (the roofline byte model recorded in code). */
 int cel_byte_model(int form, int correction_steps, double* stencil_bytes_per_cell_pass,

@@ -1,7 +1,8 @@
 """GPU forms against the fixtures written from the reference's own code (tests/golden/).
 
 The plain FP32 form reproduces the reference's compute.hlsl (compiled as C++, driven with the
-reference's pass schedule) bit for bit; the batched fused forms stay within the eta tolerance.
+reference's pass schedule) bit for bit, state and aux texture; the batched fused forms stay within
+the eta tolerance, with the aux texture's inundation depth and breaking flag checked too.
 """
 from __future__ import annotations
 
@@ -30,6 +31,8 @@ def test_plain_form_reproduces_reference_shader(celeris, name):
     eng = celeris.Engine(p, z, "plain")
     eng.physical_steps(STEPS)
     np.testing.assert_array_equal(eng.state()[..., :3], GOLD[f"{name}/state"][..., :3])
+    # the Pass1/Pass2 aux texture: max inundated depth, atan of the slope indicator, breaking flag
+    np.testing.assert_array_equal(eng.aux(), GOLD[f"{name}/aux"])
     if name == "mixed":
         eng.add_solitary_wave(0.2, 30.0, 15.0, 10.0)
         eng.physical_steps(3)
@@ -62,6 +65,12 @@ def test_batched_forms_within_tolerance_of_reference(celeris, form):
             d = got[2:-2, 2:-2, 0] - ref[2:-2, 2:-2, 0]
             rms = float(np.sqrt(np.mean(d * d)))
             assert rms < 1e-4, (n, rms)
+            # aux: the maximum inundated depth follows the state; the breaking flag (a threshold on
+            # the surface slope, then a decay) may flip only where the slope sits at the threshold
+            ra, ga = GOLD[f"{n}/aux"].astype(np.float64), batch.aux(i).astype(np.float64)
+            assert np.max(np.abs(ga[2:-2, 2:-2, 0] - ra[2:-2, 2:-2, 0])) < 1e-3, n
+            flips = np.abs(ga[2:-2, 2:-2, 3] - ra[2:-2, 2:-2, 3]) > 1e-3
+            assert flips.mean() <= 2e-3, (n, int(flips.sum()))
             # the clock at the start of the last step (the sum of the steps taken before it, adaptive
             # ones included) matches the reference's
             keys = list(GOLD["stat_keys"])
