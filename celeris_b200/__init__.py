@@ -223,6 +223,14 @@ class Batch:
         check(lib().cel_batch_get_state(self.h, i, _fp(out)))
         return out
 
+    def state_parts(self, i: int):
+        """Member i's state as (hi, lo) float textures; hi + lo is the compensated state (lo = 0 in
+        the FP32 forms)."""
+        hi = np.zeros(self.shapes[i] + (4,), dtype=np.float32)
+        lo = np.zeros(self.shapes[i] + (4,), dtype=np.float32)
+        check(lib().cel_batch_get_state_parts(self.h, i, _fp(hi), _fp(lo)))
+        return hi, lo
+
     def set_state(self, i: int, rgba: np.ndarray):
         a = np.ascontiguousarray(rgba, dtype=np.float32)
         check(lib().cel_batch_set_state(self.h, i, _fp(a)))

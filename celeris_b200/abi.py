@@ -196,6 +196,7 @@ def _declare(L: C.CDLL) -> None:
         "cel_batch_stencil_width": (i, [vp]),
         "cel_batch_autotune": (i, [vp, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]),
         "cel_batch_get_state": (i, [vp, i, fp]),
+        "cel_batch_get_state_parts": (i, [vp, i, fp, fp]),
         "cel_batch_set_state": (i, [vp, i, fp]),
         "cel_batch_get_aux": (i, [vp, i, fp]),
         "cel_batch_use_graph": (i, [vp, i]),
@@ -240,7 +241,7 @@ EXPORTED = [
     "cel_batch_set_bathymetry", "cel_batch_add_solitary_wave",
     "cel_batch_create", "cel_batch_create_lanes", "cel_batch_lanes", "cel_batch_destroy", "cel_batch_set_stream",
     "cel_batch_step",
-    "cel_batch_stats", "cel_batch_stats_current", "cel_batch_get_state", "cel_batch_set_state", "cel_batch_get_aux",
+    "cel_batch_stats", "cel_batch_stats_current", "cel_batch_get_state", "cel_batch_get_state_parts", "cel_batch_set_state", "cel_batch_get_aux",
     "cel_batch_use_graph", "cel_batch_cells", "cel_batch_set_timestep", "cel_batch_launches_per_step", "cel_set_tuning", "cel_batch_set_tuning",
     "cel_batch_get_tuning", "cel_batch_col_chunks", "cel_batch_set_stencil_rows", "cel_batch_set_stencil_width", "cel_batch_stencil_width",
     "cel_batch_autotune",

@@ -37,6 +37,7 @@ int lane_stats(cel_lane* b, cel_stats* out, bool current, std::string& err);
 int lane_stats_enqueue(cel_lane* b, bool current, std::string& err);
 int lane_stats_finish(cel_lane* b, cel_stats* out, bool current, std::string& err);
 int lane_get_state(cel_lane* b, int i, float* rgba, std::string& err);
+int lane_get_state_parts(cel_lane* b, int i, float* hi_rgba, float* lo_rgba, std::string& err);
 int lane_set_state(cel_lane* b, int i, const float* rgba, std::string& err);
 int lane_get_aux(cel_lane* b, int i, float* rgba, std::string& err);
 int lane_set_bathymetry(cel_lane* b, int i, const float* z, int bnx, int bny, std::string& err);
@@ -69,6 +70,7 @@ int batch_set_stream(cel_batch* b, cudaStream_t s, std::string& err);
 int batch_step(cel_batch* b, int nsteps, std::string& err);
 int batch_stats(cel_batch* b, cel_stats* out, bool current, std::string& err);
 int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err);
+int batch_get_state_parts(cel_batch* b, int i, float* hi_rgba, float* lo_rgba, std::string& err);
 int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err);
 int batch_get_aux(cel_batch* b, int i, float* rgba, std::string& err);
 int batch_set_bathymetry(cel_batch* b, int i, const float* z, int bnx, int bny, std::string& err);

@@ -366,6 +366,11 @@ int cel_batch_get_state(cel_batch* b, int i, float* rgba) {
     if (!rgba) { set_error("null buffer"); return CEL_ERR_ARG; }
     CEL_GUARD_BEGIN BRET(cel::batch_get_state(b, i, rgba, err)); CEL_GUARD_END
 }
+int cel_batch_get_state_parts(cel_batch* b, int i, float* hi_rgba, float* lo_rgba) {
+    BAT(b);
+    if (!hi_rgba && !lo_rgba) { set_error("null buffer"); return CEL_ERR_ARG; }
+    CEL_GUARD_BEGIN BRET(cel::batch_get_state_parts(b, i, hi_rgba, lo_rgba, err)); CEL_GUARD_END
+}
 int cel_batch_set_state(cel_batch* b, int i, const float* rgba) {
     BAT(b);
     if (!rgba) { set_error("null buffer"); return CEL_ERR_ARG; }

@@ -3428,6 +3428,35 @@ int lane_stats_finish(cel_lane* b, cel_stats* out, bool current, std::string& er
     return CEL_OK;
 }
 
+// The state as two float textures whose sum is the compensated value: hi = the stored state, lo =
+// its low words (zero in the FP32 forms).  Either pointer may be null.
+int lane_get_state_parts(cel_lane* b, int i, float* hi_rgba, float* lo_rgba, std::string& err) {
+    if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
+    Member& m = b->mem[i];
+    const MemberDev& d = b->hdev[i];
+    const int NX = m.hs.NX, NY = m.hs.NY;
+    std::vector<float> pl[3], lo[3];
+    for (int q = 0; q < 3; ++q) {
+        pl[q].resize(m.plane);
+        lo[q].assign(m.plane, 0.f);
+        B_TRY(cudaMemcpyAsync(pl[q].data(), d.S[b->ix.sin][q], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+        if (b->mixed)
+            B_TRY(cudaMemcpyAsync(lo[q].data(), d.L[b->ix.sin][q], m.plane * sizeof(float), cudaMemcpyDeviceToHost, b->stream));
+    }
+    B_TRY(cudaStreamSynchronize(b->stream));
+    for (int y = 0; y < NY; ++y)
+        for (int x = 0; x < NX; ++x) {
+            const size_t k = size_t(y) * m.P + x, o = (size_t(y) * NX + x) * 4;
+            for (int q = 0; q < 3; ++q) {
+                if (hi_rgba) hi_rgba[o + q] = pl[q][k];
+                if (lo_rgba) lo_rgba[o + q] = lo[q][k];
+            }
+            if (hi_rgba) hi_rgba[o + 3] = 0.f;
+            if (lo_rgba) lo_rgba[o + 3] = 0.f;
+        }
+    return CEL_OK;
+}
+
 int lane_get_state(cel_lane* b, int i, float* rgba, std::string& err) {
     if (i < 0 || i >= int(b->mem.size())) { err = "member index out of range"; return CEL_ERR_ARG; }
     Member& m = b->mem[i];

@@ -212,6 +212,10 @@ int batch_get_state(cel_batch* b, int i, float* rgba, std::string& err) {
     return on_member(b, i, err, [&](cel_lane* l, int k) { return lane_get_state(l, k, rgba, err); });
 }
 
+int batch_get_state_parts(cel_batch* b, int i, float* hi_rgba, float* lo_rgba, std::string& err) {
+    return on_member(b, i, err, [&](cel_lane* l, int k) { return lane_get_state_parts(l, k, hi_rgba, lo_rgba, err); });
+}
+
 int batch_set_state(cel_batch* b, int i, const float* rgba, std::string& err) {
     return on_member(b, i, err, [&](cel_lane* l, int k) { return lane_set_state(l, k, rgba, err); });
 }

@@ -253,6 +253,10 @@ int cel_batch_stats(cel_batch* b, cel_stats* out);
 /* n entries: the same totals computed now, from the current state (one extra pass over it). */
 int cel_batch_stats_current(cel_batch* b, cel_stats* out);
 int cel_batch_get_state(cel_batch* b, int i, float* rgba);
+/* Member i's state as two RGBA32F textures whose sum is the compensated state of the mixed form:
+ * hi (the stored state, what the stencils read) and lo (its low words; 0 in the FP32 forms).
+ * cel_batch_get_state returns hi + lo rounded to float.  Either pointer may be NULL.  Library only. */
+int cel_batch_get_state_parts(cel_batch* b, int i, float* hi_rgba, float* lo_rgba);
 int cel_batch_set_state(cel_batch* b, int i, const float* rgba);
 int cel_batch_get_aux(cel_batch* b, int i, float* rgba);
 /* cel_add_solitary_wave for member i */

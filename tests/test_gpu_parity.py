@@ -666,3 +666,20 @@ def test_adaptive_batch_reports_the_uniform_step_before_its_first_pass(celeris):
     assert s["total_time"] == 0.0
     b.step(3)
     assert b.stats()[0]["timestep"] > 0
+
+
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+def test_state_parts_sum_to_the_state(celeris, form):
+    """cel_batch_get_state_parts: hi + lo is the compensated state (lo = 0 in the FP32 form), and
+    cel_batch_get_state returns that sum rounded to float."""
+    members = [_case(k, nx=48, ny=32, N=1)[:4] for k in ["mixed", "sponge"]]
+    b = celeris.Batch([(m[0], m[1]) for m in members], form)
+    b.step(25)
+    for i in range(len(members)):
+        hi, lo = b.state_parts(i)
+        if form == "fused":
+            assert not lo.any()
+        else:
+            assert np.abs(lo[2:-2, 2:-2, :3]).max() > 0      # the low words carry something
+            assert np.all(np.abs(lo) <= np.abs(hi) * 2.0 ** -23 + 1e-30)
+        np.testing.assert_array_equal((hi.astype(np.float64) + lo).astype(np.float32), b.state(i))
