@@ -422,7 +422,10 @@ def main():
     batch.use_graph(not args.no_graph)
     st_ms, st_n = kt.get("fused_stencil", (0.0, 0))
     comp = 8.0 if args.form == "mixed" else 0.0
-    stencil_bytes_cell = ((112 + comp) + N * (136 + comp)) / (1 + N)  # average over pass kinds
+    # the paired-row stencil rebuilds the bottom from the corner grid (4 B); the one-row stencil
+    # reads BA, BX and BY (12 B)
+    bottom = 0.0 if batch.stencil_rows == 2 else 8.0
+    stencil_bytes_cell = ((104 + bottom + comp) + N * (128 + bottom + comp)) / (1 + N)  # average over pass kinds
     avg_launch_s = st_ms / max(st_n, 1) / 1e3
     cells_launch = cells / lanes
     achieved = stencil_bytes_cell * cells_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0

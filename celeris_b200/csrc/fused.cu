@@ -81,6 +81,8 @@ struct MemberDev {
     float* AUX[2];          // {max inundated depth, breaking} as one float2 plane pair (AUX[0])
     const float* FX[3];     // x-systems: c', inv_den, m
     const float* FYF[3];    // y-systems: c', inv_den, m
+    float* CORN;            // bathymetry at cell corners, (NX+1) x (NY+1) with pitch PC (the stencil rebuilds BA, BX, BY)
+    int PC;
     BoundaryDesc bd[4];     // N, E, S, W
     const float4* waves;
     const double* waves64;  // the same components in FP64, 4 per component (compensated form)
@@ -177,6 +179,7 @@ constexpr int MH_DEFAULT = 64;   // rows per strip unless tuned (each work item 
 constexpr int RING = 7;          // state / bottom rows resident in shared memory (PREFETCH + 5)
 constexpr int RBOX = 136;        // TMA box width in floats (covers columns x0-2 .. x0+127)
 constexpr int RSTR = 160;        // ring row stride in floats (640 B, a multiple of 128 B)
+constexpr int CBOX = RBOX + 4;   // corner-grid box: the RBOX cells' corners (one more), rounded to 16 B
 constexpr unsigned ROW_BYTES = 6u * RBOX * 4u;
 constexpr int PREFETCH = 2;      // rows requested ahead of the row being consumed
 
@@ -733,7 +736,12 @@ __global__ void __launch_bounds__(MW, MARCH_MIN_CTAS) k_march(const MemberDev* _
 constexpr int march2_min_ctas(int w) { return w == 128 ? MARCH2_MIN_CTAS : 4; }
 constexpr int RING2 = 9;
 constexpr int FSTR2 = RING2 * RSTR;
-constexpr size_t MARCH2_DYN_SMEM = sizeof(float) * 6 * FSTR2;   // the 9-row TMA ring
+// the 9-row TMA ring of the paired-row stencil: fields w, hu, hv and the corner grid row above
+// each cell row (the bottom BA, BX, BY is rebuilt from the corners)
+constexpr size_t MARCH2_DYN_SMEM = sizeof(float) * 4 * FSTR2;
+constexpr unsigned ROW_BYTES2 = (3u * RBOX + unsigned(CBOX)) * 4u;
+
+
 
 typedef float2 f2;
 __device__ __forceinline__ f2 P2(float a, float b) { return make_float2(a, b); }
@@ -774,6 +782,18 @@ __device__ __forceinline__ f2 div_by_h2(f2 h, float eps) {
     return mul2(mul2(S2(1.41421354f), h), P2(rsqrtf(t.x), rsqrtf(t.y)));
 }
 
+// The bottom of a pair of cells (rows r, r+1 of one column) from the corner grid, exactly as the
+// host's prepare_bottom sums the corners (terrain_heightfield.cpp:213-297): BA = ((z00/4 + z10/4)
+// + z01/4) + z11/4, BX = z10/2 + z11/2 (east edge), BY = z01/2 + z11/2 (north edge).  The
+// products by powers of two are exact, so these sums round as the host's do with or without FMA
+// contraction.  L0/R0: the left/right corners on the south edges of the two cells (corner rows
+// r, r+1), L1/R1: on their north edges (corner rows r+1, r+2).
+__device__ __forceinline__ f2 corner_mean2(f2 a, f2 b) { return fma2(S2(0.5f), b, mul2(S2(0.5f), a)); }
+__device__ __forceinline__ f2 corner_mean4(f2 l0, f2 r0, f2 l1, f2 r1) {
+    const f2 q = S2(0.25f);
+    return fma2(q, r1, fma2(q, l1, fma2(q, r0, mul2(q, l0))));
+}
+
 struct Face2 { f2 hN, hE, hS, hW, uN, uE, uS, uW, vN, vE, vS, vW, wN, wE, wS, wW, msd; };
 // what the next step needs of a pair's faces: north and east faces of both rows, south face of
 // the second row (depth, velocities, water level)
@@ -792,14 +812,16 @@ __device__ __forceinline__ void faces_at2(const float* __restrict__ ring, int om
     const float* W = ring;
     const float* HU = ring + FSTR2;
     const float* HV = ring + 2 * FSTR2;
-    const float* BXr = ring + 4 * FSTR2;
-    const float* BYr = ring + 5 * FSTR2;
+    const float* Cr = ring + 3 * FSTR2;   // slot of row q holds corner row q+1
     const int a0 = o0 + col, a1 = o1 + col;
     const f2 tt = S2(c.two_theta);
     const f2 wc = P2(W[a0], W[a1]), wl = P2(W[a0 - 1], W[a1 - 1]), wr = P2(W[a0 + 1], W[a1 + 1]);
     const f2 wd = P2(W[om1 + col], W[a0]), wu = P2(W[a1], W[o2 + col]);
-    const f2 BN = P2(BYr[a0], BYr[a1]), BE = P2(BXr[a0], BXr[a1]);
-    const f2 BS = P2(BYr[om1 + col], BYr[a0]), BW = P2(BXr[a0 - 1], BXr[a1 - 1]);
+    // corners of cells (r, r+1): south edges in the slots of rows r-1, r; north edges in r, r+1
+    const f2 L0 = P2(Cr[om1 + col], Cr[a0]), L1 = P2(Cr[a0], Cr[a1]);
+    const f2 R0 = P2(Cr[om1 + col + 1], Cr[a0 + 1]), R1 = P2(Cr[a0 + 1], Cr[a1 + 1]);
+    const f2 BN = corner_mean2(L1, R1), BE = corner_mean2(R0, R1);
+    const f2 BS = corner_mean2(L0, R0), BW = corner_mean2(L0, L1);
     f2 wN, wE, wS, wW, huN, huE, huS, huW, hvN, hvE, hvS, hvW, sd1, sd2;
     recon_sd2(tt, wl, wc, wr, wW, wE, sd1);
     recon_sd2(tt, wd, wc, wu, wS, wN, sd2);
@@ -863,7 +885,7 @@ struct Kahan2 {
 template <bool MIXED, bool ADAPT, int TW>
 __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const MemberDev* __restrict__ mems,
                                                                const int4* __restrict__ tiles, int ntiles, PassArgs pa) {
-    extern __shared__ __align__(128) float ring[];   // 6 * FSTR2 floats (dynamic: the total passes 48 KB)
+    extern __shared__ __align__(128) float ring[];   // 4 * FSTR2 floats: w, hu, hv, corner rows
     __shared__ float dring[RING2 * RSTR];   // still-water depth of each ring row (same stride as the ring)
     __shared__ __align__(8) unsigned long long bars[RING2];
     __shared__ float fW[2][2][4][TW];       // [step parity][row of the pair][hW, uW, vW, wW][thread]
@@ -882,9 +904,7 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
     const float* W = ring;
     const float* HU = ring + FSTR2;
     const float* HV = ring + 2 * FSTR2;
-    const float* BAr = ring + 3 * FSTR2;
-    const float* BXr = ring + 4 * FSTR2;
-    const float* BYr = ring + 5 * FSTR2;
+    const float* Cr = ring + 3 * FSTR2;   // slot of row q: corner row q+1
     const bool stats = pa.stats != 0;
     const bool corr = pa.scheme == CEL_SCHEME_CORRECTOR;
     const bool euler = pa.scheme == CEL_SCHEME_EULER;
@@ -930,33 +950,43 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
         const unsigned seq0 = seq;
         auto slot_of = [&](int r) { return int((seq0 + unsigned(r - (y0 - 2))) % RING2); };
         auto par_of = [&](int r) { return ((seq0 + unsigned(r - (y0 - 2))) / RING2) & 1u; };
-        auto issue = [&](int row) {   // one thread: request the 6 fields of a row into its slot
+        auto issue = [&](int row) {   // one thread: request a row's w, hu, hv and the corner row above it
             if (tma_late) return;       // a wait gave up: request nothing more
             requested = seq0 + unsigned(row - (y0 - 2)) + 1u;
             const int sl_ = slot_of(row);
             const int ry = min(row, NYm1);          // rows past the domain are never used; load the last
-            mbar_expect_tx(&bars[sl_], ROW_BYTES);
+            mbar_expect_tx(&bars[sl_], ROW_BYTES2);
             float* dst = ring + sl_ * RSTR;
             tma_row(dst, tm + pa.in * 3 + 0, xs, ry, &bars[sl_]);
             tma_row(dst + FSTR2, tm + pa.in * 3 + 1, xs, ry, &bars[sl_]);
             tma_row(dst + 2 * FSTR2, tm + pa.in * 3 + 2, xs, ry, &bars[sl_]);
-            tma_row(dst + 3 * FSTR2, tm + 9, xs, ry, &bars[sl_]);
-            tma_row(dst + 4 * FSTR2, tm + 10, xs, ry, &bars[sl_]);
-            tma_row(dst + 5 * FSTR2, tm + 11, xs, ry, &bars[sl_]);
+            tma_row(dst + 3 * FSTR2, tm + 12, xs, ry + 1, &bars[sl_]);   // corner rows 0 .. NY
         };
         auto wait_row = [&](int row) {
             if (!mbar_wait_bounded(&bars[slot_of(row)], par_of(row), tma_late ? 1 : (1 << 22))) tma_late = true;
         };
         // still-water depth of a ring row: thread k covers ring column rc0(thread 0) - 1 + k, and
-        // threads 0 and 1 also the two columns past the last thread
+        // threads 0 and 1 also the two columns past the last thread.  BA is rebuilt from the corner
+        // rows in the slots of rows row-1 and row; the strip's first row (whose lower corner row is
+        // not in the ring) reads BA from its plane (zero past the row, as the TMA fill would give).
         const int dcol = rc0 - 1;
+        const int d2c = min(dcol + TW, RBOX - 1);
+        auto depth_at = [&](int row, int k) {
+            float ba;
+            if (row == y0 - 2) {
+                const int gx = xs + k;
+                ba = gx < c.NX ? M.BA[size_t(row) * P + gx] : 0.f;
+            } else {
+                const float* lo = Cr + slot_of(row - 1) * RSTR;
+                const float* up = Cr + slot_of(row) * RSTR;
+                ba = fmaf(0.25f, up[k + 1], fmaf(0.25f, up[k], fmaf(0.25f, lo[k + 1], 0.25f * lo[k])));
+            }
+            return fmaxf(0.f, sl - ba);
+        };
         auto depth_row = [&](int row) {
-            const int off = slot_of(row) * RSTR;
-            const float* ba = BAr + off;
-            float* dr = dring + off;
-            dr[dcol] = fmaxf(0.f, sl - ba[dcol]);
-            const int d2c = min(dcol + TW, RBOX - 1);
-            if (tid < 2) dr[d2c] = fmaxf(0.f, sl - ba[d2c]);
+            float* dr = dring + slot_of(row) * RSTR;
+            dr[dcol] = depth_at(row, dcol);
+            if (tid < 2) dr[d2c] = depth_at(row, d2c);
         };
 
         Kahan2 acc[5];
@@ -1086,8 +1116,11 @@ __global__ void __launch_bounds__(TW, march2_min_ctas(TW)) k_march2(const Member
                 // rows t, t+1 as pairs; "d" = the row below, "u" = the row above
                 const f2 wc = P2(W[a0], W[a1]);
                 const f2 huc = P2(HU[a0], HU[a1]), hvc = P2(HV[a0], HV[a1]);
-                const f2 BAh = P2(BAr[a0], BAr[a1]), BXh = P2(BXr[a0], BXr[a1]), BYh = P2(BYr[a0], BYr[a1]);
-                const f2 BXw = P2(BXr[a0 - 1], BXr[a1 - 1]), BYs = P2(BYr[am1], BYr[a0]);
+                // the bottom of cells (rc, t) and (rc, t+1) from the corner rows t .. t+2
+                const f2 cL0 = P2(Cr[am1], Cr[a0]), cL1 = P2(Cr[a0], Cr[a1]);
+                const f2 cR0 = P2(Cr[am1 + 1], Cr[a0 + 1]), cR1 = P2(Cr[a0 + 1], Cr[a1 + 1]);
+                const f2 BAh = corner_mean4(cL0, cR0, cL1, cR1), BXh = corner_mean2(cR0, cR1);
+                const f2 BYh = corner_mean2(cL1, cR1), BXw = corner_mean2(cL0, cL1), BYs = corner_mean2(cL0, cR0);
                 const f2 h = max2(S2(0.f), sub2(wc, BAh));
                 const f2 dh = P2(dring[a0], dring[a1]), d2 = mul2(dh, dh), d3 = mul2(d2, dh);
                 const f2 dl = P2(dring[a0 - 1], dring[a1 - 1]), dr = P2(dring[a0 + 1], dring[a1 + 1]);
@@ -2556,12 +2589,12 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 
 // Row map of one NX x NY plane with pitch P floats: boxes of RBOX x 1 floats; reads outside
 // the plane return zero, like the reference's out-of-range texture loads.
-int encode_row_map(CUtensorMap* m, const float* plane, int NX, int NY, int P, std::string& err) {
+int encode_row_map(CUtensorMap* m, const float* plane, int NX, int NY, int P, std::string& err, int box_w = RBOX) {
     auto enc = tensor_map_encoder();
     if (!enc) { err = "cuTensorMapEncodeTiled unavailable"; return CEL_ERR_CUDA; }
     cuuint64_t dims[2] = {cuuint64_t(NX), cuuint64_t(NY)};
     cuuint64_t strides[1] = {cuuint64_t(P) * sizeof(float)};
-    cuuint32_t box[2] = {cuuint32_t(RBOX), 1u};
+    cuuint32_t box[2] = {cuuint32_t(box_w), 1u};
     cuuint32_t estr[2] = {1u, 1u};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(plane), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -2586,6 +2619,23 @@ int dalloc(cel_lane* b, void** ptr, size_t bytes, std::string& err) {
         cudaError_t _e = (expr);                                                        \
         if (_e != cudaSuccess) { err = std::string(#expr) + ": " + cudaGetErrorString(_e); return CEL_ERR_CUDA; } \
     } while (0)
+
+// Uploads the member's corner grid (HostSetup::corners) into its pitched corner plane: on the legacy
+// stream and synchronously when `stream` is null (set-up), else ordered on `stream` from `keep`,
+// which the caller holds until the stream has passed the copy.
+int upload_corners(const Member& m, const MemberDev& d, cudaStream_t stream, std::string& err,
+                   std::vector<float>* keep = nullptr) {
+    const int NX = m.hs.NX, NY = m.hs.NY;
+    std::vector<float> local;
+    std::vector<float>& pl = keep ? *keep : local;
+    pl.assign(size_t(d.PC) * (NY + 1), 0.f);
+    for (int y = 0; y <= NY; ++y)
+        std::memcpy(&pl[size_t(y) * d.PC], &m.hs.corners[size_t(y) * (NX + 1)], sizeof(float) * (NX + 1));
+    const cudaError_t e = stream ? cudaMemcpyAsync(d.CORN, pl.data(), pl.size() * sizeof(float), cudaMemcpyHostToDevice, stream)
+                                 : cudaMemcpy(d.CORN, pl.data(), pl.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { err = std::string("corner upload: ") + cudaGetErrorString(e); return CEL_ERR_CUDA; }
+    return CEL_OK;
+}
 
 // Uploads a member's state (RGBA texels); `lo3`, when given, holds the mixed form's low words
 // (3 per texel), else they start at zero.
@@ -2854,14 +2904,16 @@ int build_graphs(cel_lane* b, std::string& err) {
 }  // namespace
 
 void byte_model(int form, int N, double& stencil, double& step) {
-    // Algorithmic HBM bytes per interior cell (compulsory traffic of this design):
-    //  stencil, predictor: read state 12 + bottom 12 + history 40 + aux 8;
-    //                      write w 4 + rhs 8 + history 20 + aux 8  -> 112
-    //  stencil, corrector: + predicted history 20 + CURRENT_STATE w 4  -> 136
+    // Algorithmic HBM bytes per interior cell (compulsory traffic of this design), for the
+    // paired-row stencil (k_march2), which rebuilds the bottom from the corner grid:
+    //  stencil, predictor: read state 12 + corner grid 4 + history 40 + aux 8;
+    //                      write w 4 + rhs 8 + history 20 + aux 8  -> 104
+    //  stencil, corrector: + predicted history 20 + CURRENT_STATE w 4  -> 128
+    //  (the one-row stencil k_march reads BA, BX and BY: 8 more in each pass)
     //  tridiagonal (x and y): read rhs 8 + factors 24 + base 8, write 8 -> 48
     //  mixed form: + compensation words: stencil w lo read/write 8, solves hu/hv lo 16 -> +24
     const double comp = (form == CEL_FORM_MIXED) ? 1.0 : 0.0;
-    const double st_pred = 112 + 8 * comp, st_corr = 136 + 8 * comp;
+    const double st_pred = 104 + 8 * comp, st_corr = 128 + 8 * comp;
     const double tri = 48 + 16 * comp;
     stencil = st_pred;
     step = (st_pred + tri) + N * (st_corr + tri);
@@ -3122,16 +3174,22 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
         for (int k = 0; k < 3; ++k) fy[k] = next();
         for (int k = 0; k < 3; ++k) { d.FX[k] = fx[k]; d.FYF[k] = fy[k]; }
         {   // TMA row maps: the three state buffers (w, hu, hv), then BA, BX, BY
-            std::vector<CUtensorMap> maps(12);
+            std::vector<CUtensorMap> maps(13);
             for (int sb = 0; sb < 3; ++sb)
                 for (int k = 0; k < 3; ++k)
                     if (encode_row_map(&maps[sb * 3 + k], d.S[sb][k], NX, NY, m.P, err)) return nullptr;
             if (encode_row_map(&maps[9], ba, NX, NY, m.P, err) || encode_row_map(&maps[10], bx, NX, NY, m.P, err) ||
                 encode_row_map(&maps[11], by, NX, NY, m.P, err))
                 return nullptr;
+            // the corner grid: rows of CBOX floats, so that a ring row's RBOX cells have both corners
+            d.PC = (NX + 1 + 31) / 32 * 32;
+            void* cp_ = nullptr;
+            if (dalloc(b.get(), &cp_, sizeof(float) * size_t(d.PC) * (NY + 1), err)) return nullptr;
+            d.CORN = static_cast<float*>(cp_);
+            if (encode_row_map(&maps[12], d.CORN, NX + 1, NY + 1, d.PC, err, CBOX)) return nullptr;
             void* mp = nullptr;
-            if (dalloc(b.get(), &mp, sizeof(CUtensorMap) * 12, err)) return nullptr;
-            if (cudaMemcpy(mp, maps.data(), sizeof(CUtensorMap) * 12, cudaMemcpyHostToDevice) != cudaSuccess) {
+            if (dalloc(b.get(), &mp, sizeof(CUtensorMap) * 13, err)) return nullptr;
+            if (cudaMemcpy(mp, maps.data(), sizeof(CUtensorMap) * 13, cudaMemcpyHostToDevice) != cudaSuccess) {
                 err = "tensor map upload failed";
                 return nullptr;
             }
@@ -3150,6 +3208,7 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
             return CEL_OK;
         };
         if (put(by, m.hs.BY) || put(bx, m.hs.BX) || put(ba, m.hs.BA)) return nullptr;
+        if (upload_corners(m, d, nullptr, err)) return nullptr;
         {
             std::vector<float> cpv, inv, mv;
             thomas_factors_x(m.hs, cpv, inv, mv);
@@ -3522,6 +3581,8 @@ int lane_set_bathymetry(cel_lane* b, int i, const float* z, int bnx, int bny, st
     B_TRY(cudaMemcpyAsync(const_cast<float*>(d.BY), by.data(), pb, cudaMemcpyHostToDevice, b->stream));
     B_TRY(cudaMemcpyAsync(const_cast<float*>(d.BX), bx.data(), pb, cudaMemcpyHostToDevice, b->stream));
     B_TRY(cudaMemcpyAsync(const_cast<float*>(d.BA), ba.data(), pb, cudaMemcpyHostToDevice, b->stream));
+    std::vector<float> corners;
+    if (int e = upload_corners(m, d, b->stream, err, &corners)) return e;
     B_TRY(cudaMemcpyAsync(d.S[sin][0], hi.data(), pb, cudaMemcpyHostToDevice, b->stream));
     if (b->mixed) B_TRY(cudaMemcpyAsync(d.L[sin][0], lo.data(), pb, cudaMemcpyHostToDevice, b->stream));
     B_TRY(cudaMemsetAsync(d.AUX[0], 0, 2 * pb, b->stream));
