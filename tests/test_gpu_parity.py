@@ -570,6 +570,25 @@ def test_new_terrain_fused_forms(celeris, form):
     np.testing.assert_array_equal(b.state(1), solo.state(0))
 
 
+@pytest.mark.parametrize("form", ["fused", "mixed"])
+def test_new_terrain_paired_row_stencil(celeris, form):
+    """The paired-row stencil rebuilds BA, BX and BY from the corner grid: a terrain change must
+    reach its corner plane.  A batch member's terrain changes mid-run and the batch follows the FP64
+    oracle through the same change (a stale corner plane would keep the old bed under the new one)."""
+    p, z, bnx, bny, keep = _case("mixed", nx=70, ny=45, N=1)
+    z2 = _terrain_change(z)
+    ref = O.Oracle(p, z, bnx, bny, "f64")
+    ref.physical_steps(40)
+    ref.new_terrain(z2)
+    ref.physical_steps(60)
+    b = celeris.Batch([(p, z)], form)
+    b.set_stencil_rows(2)
+    b.step(40)
+    b.set_bathymetry(0, z2)
+    b.step(60)
+    assert eta_rms(b.state(0), ref.state()) <= 1e-4
+
+
 def _water_height_expected(state, bottom, p, x, y):
     """getWaterHeight (engine.cpp:4994-5012) restated in float32: GetTerrainHeight's bilinear of BA
     (terrain_heightfield.cpp:313-351) plus the 4x4 block's sum of h (GetStats order) / 16."""
