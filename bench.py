@@ -436,10 +436,10 @@ def main():
     except Exception:
         peak, peak_src = 6650.0, "fallback"
     # DRAM bytes per cell of one stencil launch measured by ncu (dram__bytes_read.sum +
-    # dram__bytes_write.sum / cells) on the first 8 members of this ensemble, mixed form, paired-row
-    # stencil at 96 threads per strip: predictor 116.2, corrector 142.3; scaled here to this
-    # launch's cells.
-    ncu_bytes_cell = {"mixed": (116.2, 142.3)}
+    # dram__bytes_write.sum / cells) on the first 8 members of this ensemble in one lane, mixed form,
+    # paired-row stencil at 96 threads per strip (corner-grid bottom): predictor 106.9, corrector
+    # 132.9; scaled here to this launch's cells.
+    ncu_bytes_cell = {"mixed": (106.9, 132.9)}
     traffic = None
     if args.form in ncu_bytes_cell:
         pb, cbytes = ncu_bytes_cell[args.form]
