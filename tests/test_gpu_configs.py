@@ -31,7 +31,7 @@ from util import surface_rms
 
 pytestmark = pytest.mark.gpu
 
-ETA_RMS = 1e-4          # m
+ETA_RMS = 1e-4          # m, the eta RMS bound after the runs
 MASS_REL = 1e-9         # relative difference of the FP64 water volume (compensated form)
 BREAK_FRAC = 2e-3       # fraction of interior cells whose breaking indicator differs by > 1e-3
 
