@@ -503,6 +503,7 @@ def main():
                                       "rows_per_chunk_tallest_member": -(-max(m[0].ny for m in members) // batch.col_chunks),
                                       "cluster_ctas": (batch.col_chunks // 8
                                                        if batch.tuning[0] == 32 and batch.col_chunks >= 32 else 0),
+                                      "tile_transposed": batch.tuning[0] == 16 and batch.col_chunks == 1,
                                       "meaning": "column solver: L and U sweeps split into this many chunks per "
                                                  "column, each swept serially (Thomas) and joined by a scan of "
                                                  "their transfer maps (warp shuffles; with cluster_ctas > 0 "

@@ -1718,6 +1718,157 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
     }
 }
 
+// Column (y) solves through tile-transposed shared memory: a CTA of 16 warps takes a band of 16
+// columns and walks it in tiles of TT_ROWS rows.  The CTA loads a tile of every input it needs as
+// 64-byte row pieces into shared memory laid out by column (a 4-float pad per column row), then
+// warp w sweeps column w of the tile the way k_rows sweeps a row: lane j owns rows 4j .. 4j+3, read
+// as one float4, runs the recurrence over them from zero, and the lanes' affine maps are joined by a
+// warp-shuffle scan, with the tile's carry passed on to the next tile.  The forward values of the
+// whole band stay in shared memory (16 x ny floats) for the backward walk, which loads c' and the
+// base state per tile, sweeps up the same way, and writes hv = base + x back as row pieces.  Every
+// input is read once; no walk re-reads a plane.
+constexpr int TT_ROWS = 128, TT_CW = 16, TT_STR = TT_ROWS + 4;
+
+template <bool MIXED>
+__global__ void __launch_bounds__(512, 2) k_cols_tt(const MemberDev* __restrict__ mems, const int2* __restrict__ bands,
+                                                    int nbands, PassArgs pa) {
+    extern __shared__ __align__(16) float fwd[];          // [TT_CW][ny rounded to 4]: forward values by column
+    __shared__ __align__(16) float stg[3][TT_CW][TT_STR];  // one tile of three inputs, by column
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    for (int it = blockIdx.x; it < nbands; it += gridDim.x) {
+        const int2 bd = bands[it];
+        const MemberDev& M = mems[bd.x];
+        const int n = M.c.ny, P = M.P, x0 = bd.y, nxe = M.c.nx + 2;
+        const int ntile = (n + TT_ROWS - 1) / TT_ROWS;
+        const int base = (pa.scheme == CEL_SCHEME_CORRECTOR) ? pa.cur : pa.in;
+        float* __restrict__ yb = fwd + size_t(w) * ((n + 3) & ~3);   // 16-byte aligned columns
+        // ---- forward: y_i = inv_i r_i + m_i y_{i-1} ----
+        float carry = 0.f;
+        for (int t = 0; t < ntile; ++t) {
+            const int r0 = t * TT_ROWS;
+            __syncthreads();   // the previous tile (or band) is done with the staging buffer
+            for (int e = tid; e < TT_ROWS * TT_CW; e += 512) {
+                const int rr = e / TT_CW, cc = e % TT_CW, i = r0 + rr, gx = x0 + cc;
+                float m = 0.f, iv = 0.f, r = 0.f;
+                if (i < n && gx >= 2 && gx < nxe) {
+                    const size_t o = size_t(i + 2) * P + gx;
+                    m = __ldg(M.FYF[2] + o); iv = __ldg(M.FYF[1] + o); r = __ldg(M.R[1] + o);
+                }
+                stg[0][cc][rr] = m; stg[1][cc][rr] = iv; stg[2][cc][rr] = r;
+            }
+            __syncthreads();
+            const float4 m4 = *reinterpret_cast<const float4*>(&stg[0][w][4 * lane]);
+            const float4 i4 = *reinterpret_cast<const float4*>(&stg[1][w][4 * lane]);
+            const float4 r4 = *reinterpret_cast<const float4*>(&stg[2][w][4 * lane]);
+            const float mv[4] = {m4.x, m4.y, m4.z, m4.w}, iv[4] = {i4.x, i4.y, i4.z, i4.w};
+            const float rv[4] = {r4.x, r4.y, r4.z, r4.w};
+            float yv[4], a = 1.f, b = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                b = iv[k] * rv[k] + mv[k] * b;
+                a *= mv[k];
+                yv[k] = b;
+            }
+            Affine inc{a, b};
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const Affine o = shfl_up_affine(inc, off);
+                if (lane >= off) inc = compose(inc, o);
+            }
+            const Affine before = shfl_up_affine(inc, 1);
+            const float cin = lane > 0 ? before.b + before.a * carry : carry;
+            float pref = 1.f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                pref *= mv[k];
+                yv[k] += pref * cin;
+            }
+            const int i0 = r0 + 4 * lane;
+            if (i0 + 3 < n) {
+                *reinterpret_cast<float4*>(yb + i0) = make_float4(yv[0], yv[1], yv[2], yv[3]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (i0 + k < n) yb[i0 + k] = yv[k];
+            }
+            carry = __shfl_sync(0xffffffffu, inc.b + inc.a * carry, 31);
+        }
+        // ---- backward: x_i = y_i - c'_i x_{i+1}; hv = base + x ----
+        const float* __restrict__ bhi = M.S[base][2];
+        float* __restrict__ ohi = M.S[pa.out][2];
+        const float* __restrict__ blo = MIXED ? M.L[base][2] : nullptr;
+        float* __restrict__ olo = MIXED ? M.L[pa.out][2] : nullptr;
+        float xcarry = 0.f;
+        for (int t = ntile - 1; t >= 0; --t) {
+            const int r0 = t * TT_ROWS;
+            __syncthreads();
+            for (int e = tid; e < TT_ROWS * TT_CW; e += 512) {
+                const int rr = e / TT_CW, cc = e % TT_CW, i = r0 + rr, gx = x0 + cc;
+                float cp = 0.f, bh = 0.f, bl = 0.f;
+                if (i < n && gx >= 2 && gx < nxe) {
+                    const size_t o = size_t(i + 2) * P + gx;
+                    cp = __ldg(M.FYF[0] + o); bh = bhi[o];
+                    if (MIXED) bl = blo[o];
+                }
+                stg[0][cc][rr] = cp; stg[1][cc][rr] = bh; stg[2][cc][rr] = bl;
+            }
+            __syncthreads();
+            const int i0 = r0 + 4 * lane;
+            const float4 c4 = *reinterpret_cast<const float4*>(&stg[0][w][4 * lane]);
+            float cv[4] = {c4.x, c4.y, c4.z, c4.w}, yv[4];
+            if (i0 + 3 < n) {
+                const float4 y4 = *reinterpret_cast<const float4*>(yb + i0);
+                yv[0] = y4.x; yv[1] = y4.y; yv[2] = y4.z; yv[3] = y4.w;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) yv[k] = (i0 + k < n) ? yb[i0 + k] : 0.f;
+            }
+            float z = 0.f, qa = 1.f;
+#pragma unroll
+            for (int k = 3; k >= 0; --k) {
+                const float cn = (i0 + k < n) ? -cv[k] : 0.f;
+                z = yv[k] + cn * z;
+                qa *= cn;
+                yv[k] = z;
+                cv[k] = cn;
+            }
+            Affine inc{qa, z};
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const Affine o = shfl_down_affine(inc, off);
+                if (lane + off < 32) inc = compose(inc, o);
+            }
+            const Affine after = shfl_down_affine(inc, 1);
+            const float cnext = lane < 31 ? after.b + after.a * xcarry : xcarry;
+            float suf = 1.f;
+#pragma unroll
+            for (int k = 3; k >= 0; --k) {
+                suf *= cv[k];
+                yv[k] += suf * cnext;
+            }
+            xcarry = __shfl_sync(0xffffffffu, inc.b + inc.a * xcarry, 0);
+            // lane j alone used its c' entries: overwrite them with x for the write-back
+            *reinterpret_cast<float4*>(&stg[0][w][4 * lane]) = make_float4(yv[0], yv[1], yv[2], yv[3]);
+            __syncthreads();
+            for (int e = tid; e < TT_ROWS * TT_CW; e += 512) {
+                const int rr = e / TT_CW, cc = e % TT_CW, i = r0 + rr, gx = x0 + cc;
+                if (i < n && gx >= 2 && gx < nxe) {
+                    const size_t o = size_t(i + 2) * P + gx;
+                    const float x = stg[0][cc][rr];
+                    if (MIXED) {
+                        float hi = stg[1][cc][rr], lo = stg[2][cc][rr];
+                        two_sum_add(hi, lo, x);
+                        ohi[o] = hi;
+                        olo[o] = lo;
+                    } else {
+                        ohi[o] = stg[1][cc][rr] + x;
+                    }
+                }
+            }
+        }
+    }
+}
+
 // Column (y) solves, one thread per column: the thread runs the forward recurrence down its whole
 // column and the backward one up it.  A warp covers 32 adjacent columns, so every row access is a
 // coalesced 128-byte segment, and each thread issues the loads of CS rows before using them.  The
@@ -2561,6 +2712,7 @@ struct cel_lane {
     int cw = 16;                        // column solver band width (columns per CTA)
     int cnt = 512;                      // column solver threads per CTA (chunks per column = cnt / cw)
     int col_cl = 0;                     // cluster column solver: CTAs per cluster (0: not in use)
+    bool col_tt = false;                // tile-transposed column solver (band width 16, "1 chunk")
     int mh = cel::MH_DEFAULT;           // stencil strip height (rows per CTA work item)
     int rows_per_step = 1;              // stencil rows per thread step: 1 (k_march) or 2 (k_march2)
     int mw = 128;                       // stencil CTA width in threads (k_march2: 128 or 96)
@@ -2710,6 +2862,9 @@ int launch_pass(cel_lane* b, const PassArgs& pa, std::string& err) {
         if (b->cw == 1) {
             if (b->mixed) k_cols_serial<true><<<b->grid_cols, 128, 0, b->side>>>(b->ddev, b->bands, b->nbands, pa);
             else k_cols_serial<false><<<b->grid_cols, 128, 0, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+        } else if (b->col_tt) {
+            if (b->mixed) k_cols_tt<true><<<b->grid_cols, 512, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
+            else k_cols_tt<false><<<b->grid_cols, 512, b->smem_cols, b->side>>>(b->ddev, b->bands, b->nbands, pa);
         } else if (b->col_cl > 0) {
             // one cluster of col_cl CTAs per 32-column band
             cudaLaunchConfig_t cfg{};
@@ -2940,7 +3095,9 @@ int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::st
     // 32-column bands with 32, 64 or 128 chunks per column (nt = chunks x 32 = 1024, 2048, 4096):
     // the cluster solver, 8 chunks per CTA and nt / 256 CTAs per cluster
     const int cl = (cw == 32 && (nt == 1024 || nt == 2048 || nt == 4096)) ? nt / 256 : 0;
-    if (nt != 256 && nt != 512 && cl == 0) {
+    // 16-column bands with "1 chunk per column" (nt = 16): the tile-transposed solver
+    const bool tt = (cw == 16 && nt == 16);
+    if (nt != 256 && nt != 512 && cl == 0 && !tt) {
         err = "column solver chunks x band width must be 256 or 512 threads (or 32 columns x 32, 64 or 128 chunks)";
         return CEL_ERR_ARG;
     }
@@ -2975,7 +3132,8 @@ int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::st
     const int mo = mw - 2;   // output columns per strip
     if (cw != 1 && cw != 8 && cw != 16 && cw != 32) { err = "column band width must be 1, 8, 16 or 32"; return CEL_ERR_ARG; }
     if (mh < 8 || mh > 1024) { err = "strip height must be in [8, 1024]"; return CEL_ERR_ARG; }
-    const size_t smem_cols = (cw == 1 || cl > 0) ? 0 : sizeof(float) * size_t(b->max_ny) * cw;
+    const size_t smem_cols = tt ? sizeof(float) * size_t(TT_CW) * size_t((b->max_ny + 3) & ~3)
+                             : (cw == 1 || cl > 0) ? 0 : sizeof(float) * size_t(b->max_ny) * cw;
     if (smem_cols + COLS_STATIC_SMEM > 227 * 1024) { err = "column band too wide for the tallest member (shared memory)"; return CEL_ERR_ARG; }
     std::vector<int4> mt;
     std::vector<int2> bd;
@@ -3019,9 +3177,16 @@ int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::st
     b->mw = mw;
     b->smem_cols = smem_cols;
     b->col_cl = cl;
+    b->col_tt = tt;
     int occ = 1;
     if (cw == 1) {
         b->grid_cols = (b->nbands + 127) / 128;
+    } else if (tt) {
+        for (auto* kk : {k_cols_tt<true>, k_cols_tt<false>}) B_TRY(allow_max_dynamic_smem(reinterpret_cast<const void*>(kk)));
+        B_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b->mixed ? k_cols_tt<true> : k_cols_tt<false>, 512,
+                                                            smem_cols));
+        if (occ < 1) { err = "column band too tall for the tile-transposed solver (shared memory)"; return CEL_ERR_ARG; }
+        b->grid_cols = std::max(1, std::min(b->nbands, b->sms * occ * 4));
     } else if (cl > 0) {
         b->grid_cols = b->nbands * cl;
     } else {

@@ -340,6 +340,9 @@ int batch_autotune(cel_batch* b, int steps, int* tx, int* ty, double* best_ms, s
         // clusters of 4 or 8 CTAs)
         for (int nt : {1024, 2048})
             if (max_ny <= nt / 2) solver.push_back({32, st.mh, st.rps, st.mw, nt});
+        // the tile-transposed solver (16-column bands, the band's forward values in shared memory)
+        if (sizeof(float) * 16 * size_t((max_ny + 3) & ~3) + 27 * 1024 <= 227 * 1024)
+            solver.push_back({16, st.mh, st.rps, st.mw, 16});
     }
     const int kb = ks >= 0 ? search(solver, ms) : -1;
     cudaEventDestroy(e0);

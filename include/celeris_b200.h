@@ -283,8 +283,9 @@ int cel_batch_launches_per_step(const cel_batch* b);
  * the bidiagonal sweeps).  Chunks x band width must be 256 or 512 threads, or, with tile_x = 32, 32,
  * 64 or 128 chunks: the cluster solver, where a cluster of chunks/8 CTAs holds a 32-column band with
  * every chunk (at most 16 rows, so the tallest member must have at most 16 x chunks rows) in
- * registers and joins the chunks' maps through distributed shared memory; 0 keeps the current
- * value.  Plain engines ignore the call. */
+ * registers and joins the chunks' maps through distributed shared memory; or, with tile_x = 16,
+ * 1 chunk: the tile-transposed solver, where a warp sweeps each column of 128-row tiles staged
+ * through shared memory by the CTA; 0 keeps the current value.  Plain engines ignore the call. */
 int cel_set_tuning(cel_engine* h, int tile_x, int tile_y, int pcr_switch);
 int cel_batch_set_tuning(cel_batch* b, int tile_x, int tile_y, int pcr_switch);
 int cel_batch_get_tuning(const cel_batch* b, int* tile_x, int* tile_y, int* rows_per_step);

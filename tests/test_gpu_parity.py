@@ -313,7 +313,8 @@ def test_tuning_changes_decomposition_not_results(celeris):
     ref = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
     ref.step(30)
     for bw, sh, chunks in [(32, 32, 16), (32, 64, 8), (8, 128, 64), (8, 32, 32), (16, 8, 16), (16, 64, 32), (1, 64, 0),
-                           (32, 64, 32), (32, 32, 64), (32, 64, 128)]:   # the last three: cluster solver
+                           (32, 64, 32), (32, 32, 64), (32, 64, 128),    # cluster solver
+                           (16, 64, 1)]:                                  # tile-transposed solver
         b = celeris.Batch([(m[0], m[1]) for m in members], "mixed")
         b.set_tuning(bw, sh, chunks)
         assert b.tuning == (bw, sh)
