@@ -82,6 +82,8 @@ struct MemberDev {
     const float* FX[3];     // x-systems: c', inv_den, m
     const float* FYF[3];    // y-systems: c', inv_den, m
     float* CORN;            // bathymetry at cell corners, (NX+1) x (NY+1) with pitch PC (the stencil rebuilds BA, BX, BY)
+    float* FYB[3];          // the y factors band-major for the banded column solve: band b, row i, column c at
+                            // (b * ny + i) * band width + c
     int PC;
     BoundaryDesc bd[4];     // N, E, S, W
     const float4* waves;
@@ -1583,10 +1585,13 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
         const int mc = (n + NCH - 1) / NCH;
         const int i0 = min(n, k * mc), i1 = min(n, i0 + mc);
         const float* __restrict__ r = M.R[1] + gx;
-        const float* __restrict__ cp = M.FYF[0] + gx;
-        const float* __restrict__ inv = M.FYF[1] + gx;
-        const float* __restrict__ mm = M.FYF[2] + gx;
+        // factors band-major: a chunk's rows of this band are contiguous (CW floats apart)
+        const size_t fb = size_t(bd.y / CW) * n * CW + c;
+        const float* __restrict__ cp = M.FYB[0] + fb;
+        const float* __restrict__ inv = M.FYB[1] + fb;
+        const float* __restrict__ mm = M.FYB[2] + fb;
         auto at = [&](int i) { return size_t(i + 2) * P; };   // row offset of system element i
+        auto atf = [&](int i) { return size_t(i) * CW; };     // factor offset of system element i
         __syncthreads();
         float yv = 0.f, pa_ = 1.f, q = 1.f, z0 = 0.f, z1 = 0.f;
         if (col_ok)
@@ -1595,10 +1600,10 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
 #pragma unroll
                 for (int u = 0; u < CU; ++u) {
                     const bool ok = i + u < i1;
-                    mv[u] = ok ? __ldg(mm + at(i + u)) : 0.f;
-                    iv[u] = ok ? __ldg(inv + at(i + u)) : 0.f;
+                    mv[u] = ok ? __ldg(mm + atf(i + u)) : 0.f;
+                    iv[u] = ok ? __ldg(inv + atf(i + u)) : 0.f;
                     rv[u] = ok ? __ldg(r + at(i + u)) : 0.f;
-                    cv[u] = ok ? __ldg(cp + at(i + u)) : 0.f;
+                    cv[u] = ok ? __ldg(cp + atf(i + u)) : 0.f;
                 }
 #pragma unroll
                 for (int u = 0; u < CU; ++u)
@@ -1676,7 +1681,7 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
             for (int i = i0; i < i1; i += CU) {
                 float mv[CU];
 #pragma unroll
-                for (int u = 0; u < CU; ++u) mv[u] = (i + u < i1) ? __ldg(mm + at(i + u)) : 0.f;
+                for (int u = 0; u < CU; ++u) mv[u] = (i + u < i1) ? __ldg(mm + atf(i + u)) : 0.f;
 #pragma unroll
                 for (int u = 0; u < CU; ++u)
                     if (i + u < i1) {
@@ -1696,7 +1701,7 @@ __global__ void __launch_bounds__(NT, cols_min_ctas(NT)) k_cols(const MemberDev*
 #pragma unroll
                 for (int u = 0; u < CU; ++u) {
                     const bool ok = i - u >= i0;
-                    cv[u] = ok ? __ldg(cp + at(i - u)) : 0.f;
+                    cv[u] = ok ? __ldg(cp + atf(i - u)) : 0.f;
                     bh[u] = ok ? bhi[at(i - u)] : 0.f;
                     bl[u] = (MIXED && ok) ? blo[at(i - u)] : 0.f;
                 }
@@ -2618,6 +2623,19 @@ __global__ void k_choose_dt(DtCtl* __restrict__ ctl, float* __restrict__ dt_tabl
 
 // End of a physical step: advance the clocks by the dt of the step's last pass and, in adaptive
 // batches, shift the controller's dt queue (engine.cpp:1507-1518).
+// The band-major copy of a member's y factors for band width cw (k_cols reads it).
+__global__ void k_band_major(const MemberDev* __restrict__ mems, int mi, int cw) {
+    const MemberDev& M = mems[mi];
+    const int n = M.c.ny, NX = M.c.NX, nb = (M.c.nx + 2 + cw - 1) / cw;
+    const size_t total = size_t(nb) * n * cw;
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < total; e += size_t(gridDim.x) * blockDim.x) {
+        const int c = int(e % cw), i = int((e / cw) % n), b = int(e / (size_t(cw) * n));
+        const int x = b * cw + c;
+        const size_t o = size_t(i + 2) * M.P + x;
+        for (int q = 0; q < 3; ++q) M.FYB[q][e] = x < NX ? M.FYF[q][o] : 0.f;
+    }
+}
+
 // rcp_newton over a caller's inputs (the device self-test behind cel_selftest_reciprocal)
 __global__ void k_rcp_selftest(const float* __restrict__ x, float* __restrict__ out, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = rcp_newton(x[i]);
@@ -3178,6 +3196,11 @@ int configure_work(cel_lane* b, int cw, int mh, int rps, int mw, int nt, std::st
     b->smem_cols = smem_cols;
     b->col_cl = cl;
     b->col_tt = tt;
+    if (cw == 8 || cw == 16 || cw == 32) {
+        for (int i = 0; i < int(b->mem.size()); ++i) k_band_major<<<b->sms * 4, 256, 0, b->stream>>>(b->ddev, i, cw);
+        B_TRY(cudaGetLastError());
+        B_TRY(cudaStreamSynchronize(b->stream));
+    }
     int occ = 1;
     if (cw == 1) {
         b->grid_cols = (b->nbands + 127) / 128;
@@ -3338,6 +3361,12 @@ cel_lane* lane_create(int n, const cel_params* const* params, const float* const
         for (int k = 0; k < 3; ++k) fx[k] = next();
         for (int k = 0; k < 3; ++k) fy[k] = next();
         for (int k = 0; k < 3; ++k) { d.FX[k] = fx[k]; d.FYF[k] = fy[k]; }
+        {   // band-major y factors, sized for the widest band (32 columns)
+            const size_t nbm = size_t((m.hs.nx + 2 + 31) / 32) * 32 * m.hs.ny;
+            void* fp_ = nullptr;
+            if (dalloc(b.get(), &fp_, 3 * nbm * sizeof(float), err)) return nullptr;
+            for (int k = 0; k < 3; ++k) d.FYB[k] = static_cast<float*>(fp_) + k * nbm;
+        }
         {   // TMA row maps: the three state buffers (w, hu, hv), then BA, BX, BY
             std::vector<CUtensorMap> maps(13);
             for (int sb = 0; sb < 3; ++sb)
