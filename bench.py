@@ -491,7 +491,7 @@ def main():
             "config": {"workload": workload, "form": args.form, "members_per_gpu": len(members),
                        "cells_per_gpu": cells, "correction_steps": N, "adaptive": bool(args.adaptive), "cuda_graph": not args.no_graph,
                        "l2": "working set (%.1f GB) larger than L2 (126 MB); no flush" % (
-                           cells * 4 * (42 + (9 if args.form == "mixed" else 0)) / 1e9),
+                           cells * 4 * (46 + (9 if args.form == "mixed" else 0)) / 1e9),
                        "parallelism": f"ensemble sharded by domain over {world} GPU(s)",
                        "lanes": lanes,
                        "tuning": {"column_band_width": batch.tuning[0], "strip_height": batch.tuning[1],
